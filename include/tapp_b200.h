@@ -1,0 +1,84 @@
+/*
+ * Implementation-defined extensions of the B200 TAPP library.
+ *
+ * Everything here sits in the ranges the TAPP headers leave to
+ * implementations: attribute keys and error codes at or above 0x1000
+ * (api/include/tapp/datatype.h:9-12 of the reference states the rule for
+ * data types; this library applies it to keys and codes as well).
+ * None of it is needed to use the library as a drop-in: a caller that only
+ * uses the reference's API gets synchronous execution on the CUDA legacy
+ * default stream with the precision the product asks for.
+ */
+#ifndef TAPP_B200_H_
+#define TAPP_B200_H_
+
+#include "tapp.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- error codes (returned by TAPP_execute_product and friends) ---- */
+enum {
+    TAPP_B200_ERR_CUDA = 0x1001,        /* a CUDA call failed (no device, launch error) */
+    TAPP_B200_ERR_LIMIT = 0x1002,       /* more modes than the planner supports */
+    TAPP_B200_ERR_UNSUPPORTED = 0x1003, /* storage type or option not supported */
+    TAPP_B200_ERR_NOMEM = 0x1004,       /* device allocation failed */
+    TAPP_B200_ERR_INVALID = 0x1005,     /* invalid object or argument */
+    TAPP_B200_ERR_LABELS = 0x1006,      /* a tensor gained modes after the product was created */
+};
+
+/* ---- attribute keys, set with TAPP_attr_set on a TAPP_executor ---- */
+enum {
+    /* value: cudaStream_t. Work is issued on this stream instead of the
+     * legacy default stream. */
+    TAPP_B200_ATTR_STREAM = 0x1000,
+    /* value: int* (0/1). 1: TAPP_execute_product returns without waiting for
+     * the GPU; all operands must then be device pointers. */
+    TAPP_B200_ATTR_ASYNC = 0x1001,
+    /* value: int*. Arithmetic used for TAPP_F32F32_ACCUM_F32 products (and
+     * TAPP_DEFAULT_PREC on binary32 data):
+     *   0 plain binary32 on CUDA cores (default),
+     *   1 split-bfloat16 on tensor cores: each operand is split into a
+     *     bfloat16 high and low part, three products accumulate in binary32. */
+    TAPP_B200_ATTR_F32_MODE = 0x1002,
+    /* value: int*. Force an execution path: 0 automatic (default),
+     * 1 CUDA-core element kernel, 3 tiled CUDA-core GEMM, 4 tensor cores. */
+    TAPP_B200_ATTR_PATH = 0x1004,
+    /* value: int* (0/1). 1: TAPP_execute_product writes a status object to
+     * *status, to be read with TAPP_attr_get and freed with
+     * TAPP_destroy_status. */
+    TAPP_B200_ATTR_WANT_STATUS = 0x1005,
+};
+
+/* ---- keys readable from a status object with TAPP_attr_get ---- */
+enum {
+    TAPP_B200_STATUS_PATH = 0x1100,      /* int: execution path taken (values above) */
+    TAPP_B200_STATUS_KERNELS = 0x1101,   /* int: kernels launched */
+    TAPP_B200_STATUS_FLOPS = 0x1102,     /* double: algorithmic flops (2|D||K|, 8|D||K| complex) */
+    TAPP_B200_STATUS_DEVICE_US = 0x1103, /* double: device time of the launches, microseconds
+                                          * (synchronous executions only) */
+    TAPP_B200_STATUS_TC_MODE = 0x1104,   /* int: tensor-core operand mode (0 bf16, 1 f16, 2 split bf16) */
+};
+
+/*
+ * Describes, in a NUL-terminated string, how the library would run the
+ * product with the tensor infos' current contents: index classes after
+ * repeated labels are merged, strides, compute type and path. Returns the
+ * string length (like TAPP_explain_error: maxlen == 0 only measures). A
+ * validation failure returns 0 and writes nothing. Host-only; touches no GPU.
+ */
+TAPP_EXPORT size_t tapp_b200_describe_plan(TAPP_tensor_product plan, TAPP_executor exec,
+                                           size_t maxlen, char* out);
+
+/*
+ * Number of kernels this library launched since the process started (all
+ * threads, all devices). For launch counting in benchmarks.
+ */
+TAPP_EXPORT long long tapp_b200_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TAPP_B200_H_ */

@@ -1,0 +1,277 @@
+// CUDA-core product kernels for every shape, storage type and precision.
+//
+//   k_elementwise  one thread per element of D: decodes the free coordinates,
+//                  then walks the contracted coordinates and, inside, the
+//                  unary coordinates of A and of B. This is the reference's
+//                  loop nest (reference_implementation/src/product.c:338-399)
+//                  with the outer loop spread over threads.
+//   k_reduce       one block per element of D for few outputs with a long
+//                  contraction: the contracted range is split over the
+//                  block's threads and combined with warp shuffles.
+//
+// Both evaluate D = op_D(alpha * sum op_A(A) op_B(B) + beta * op_C(C)) in the
+// plan's compute domain (real/complex, binary32/binary64) and honour the
+// plan's operand rounding for the 16-bit precisions.
+#include <cstdio>
+
+#include "tb_common.cuh"
+
+namespace tb {
+
+struct GenParams {
+    int32_t nF, nK, nUA, nUB;
+    int32_t tA, tB, tC, tD;
+    int32_t round_in, conjA, conjB, conjC, conjD, conjD_f32, beta_zero, small_F;
+    int64_t sizeF, sizeK, sizeUA, sizeUB;
+    double alpha_re, alpha_im, beta_re, beta_im;
+    FastDiv fF[TB_MAXMODES];
+    int64_t F_ext[TB_MAXMODES], F_sA[TB_MAXMODES], F_sB[TB_MAXMODES], F_sC[TB_MAXMODES], F_sD[TB_MAXMODES];
+    int64_t K_ext[TB_MAXMODES], K_sA[TB_MAXMODES], K_sB[TB_MAXMODES];
+    FastDiv fK[TB_MAXMODES];
+    int64_t UA_ext[TB_MAXMODES], UA_s[TB_MAXMODES];
+    int64_t UB_ext[TB_MAXMODES], UB_s[TB_MAXMODES];
+};
+
+// complex helpers on (re, im) pairs; CPLX=false keeps only the real part
+template <typename R, bool CPLX>
+__device__ __forceinline__ void cmac(R& sr, R& si, R ar, R ai, R br, R bi)
+{
+    if (CPLX) {
+        sr = fma(ar, br, sr);
+        sr = fma(-ai, bi, sr);
+        si = fma(ar, bi, si);
+        si = fma(ai, br, si);
+    } else {
+        sr = fma(ar, br, sr);
+    }
+}
+
+// sum over the unary coordinates of one operand at base offset `off`
+template <typename R, bool CPLX>
+__device__ __forceinline__ void unary_sum(const void* base, int64_t off, int t, int conj, int rmode, int n,
+                                          int64_t size, const int64_t* ext, const int64_t* str, R& re, R& im)
+{
+    if (n == 0) {
+        load_rounded<R>(base, off, t, rmode, re, im);
+        if (conj) im = -im;
+        return;
+    }
+    re = 0;
+    im = 0;
+    int64_t c[TB_MAXMODES];
+    for (int j = 0; j < n; j++) c[j] = 0;
+    int64_t o = off;
+    for (int64_t u = 0; u < size; u++) {
+        R xr, xi;
+        load_elem<R>(base, o, t, xr, xi);
+        if (conj) xi = -xi;
+        re += xr;
+        im += xi;
+        if (rmode != TB_ROUND_NONE) {  // the 16-bit precisions keep the running sum in 16 bits
+            re = round_in<R>(re, rmode);
+            im = round_in<R>(im, rmode);
+        }
+        for (int j = 0; j < n; j++) {
+            o += str[j];
+            if (++c[j] < ext[j]) break;
+            o -= str[j] * ext[j];
+            c[j] = 0;
+        }
+    }
+}
+
+template <typename R, bool CPLX>
+__device__ __forceinline__ void finish(const GenParams& p, R sr, R si, const void* C, int64_t oC, void* D, int64_t oD)
+{
+    // alpha * sum
+    R ar = (R)p.alpha_re, ai = (R)p.alpha_im;
+    R accr, acci;
+    if (CPLX) {
+        accr = ar * sr - ai * si;
+        acci = ar * si + ai * sr;
+    } else {
+        accr = ar * sr;
+        acci = 0;
+    }
+    if (!p.beta_zero) {
+        R cr, ci;
+        load_rounded<R>(C, oC, p.tC, p.round_in, cr, ci);
+        if (p.conjC) ci = -ci;
+        R br = (R)p.beta_re, bi = (R)p.beta_im;
+        if (CPLX) {
+            accr += br * cr - bi * ci;
+            acci += br * ci + bi * cr;
+        } else {
+            accr += br * cr;
+        }
+    }
+    if (p.conjD) {
+        if (p.conjD_f32) {
+            accr = (R)(float)accr;
+            acci = (R)(float)acci;
+        }
+        acci = -acci;
+    }
+    store_elem<R>(D, oD, p.tD, accr, acci);
+}
+
+template <typename R, bool CPLX>
+__global__ void __launch_bounds__(256) k_elementwise(GenParams p, const void* A, const void* B, const void* C, void* D)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < p.sizeF; i += stride) {
+        int64_t oA = 0, oB = 0, oC = 0, oD = 0;
+        if (p.small_F) {
+            uint32_t r = (uint32_t)i;
+            for (int j = 0; j < p.nF; j++) {
+                uint32_t q = fdiv(r, p.fF[j]);
+                int64_t c = r - q * p.fF[j].d;
+                r = q;
+                oA += c * p.F_sA[j];
+                oB += c * p.F_sB[j];
+                oC += c * p.F_sC[j];
+                oD += c * p.F_sD[j];
+            }
+        } else {
+            int64_t r = i;
+            for (int j = 0; j < p.nF; j++) {
+                int64_t c = r % p.F_ext[j];
+                r /= p.F_ext[j];
+                oA += c * p.F_sA[j];
+                oB += c * p.F_sB[j];
+                oC += c * p.F_sC[j];
+                oD += c * p.F_sD[j];
+            }
+        }
+        R sr = 0, si = 0;
+        int64_t kc[TB_MAXMODES];
+        for (int j = 0; j < p.nK; j++) kc[j] = 0;
+        int64_t kA = oA, kB = oB;
+        for (int64_t k = 0; k < p.sizeK; k++) {
+            R ar, ai, br, bi;
+            unary_sum<R, CPLX>(A, kA, p.tA, p.conjA, p.round_in, p.nUA, p.sizeUA, p.UA_ext, p.UA_s, ar, ai);
+            unary_sum<R, CPLX>(B, kB, p.tB, p.conjB, p.round_in, p.nUB, p.sizeUB, p.UB_ext, p.UB_s, br, bi);
+            cmac<R, CPLX>(sr, si, ar, ai, br, bi);
+            for (int j = 0; j < p.nK; j++) {
+                kA += p.K_sA[j];
+                kB += p.K_sB[j];
+                if (++kc[j] < p.K_ext[j]) break;
+                kA -= p.K_sA[j] * p.K_ext[j];
+                kB -= p.K_sB[j] * p.K_ext[j];
+                kc[j] = 0;
+            }
+        }
+        finish<R, CPLX>(p, sr, si, C, oC, D, oD);
+    }
+}
+
+template <typename R>
+__device__ __forceinline__ R warp_sum(R v)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// one block per output element; the contracted range is split over threads
+template <typename R, bool CPLX>
+__global__ void __launch_bounds__(256) k_reduce(GenParams p, const void* A, const void* B, const void* C, void* D)
+{
+    __shared__ R red[2][8];
+    for (int64_t i = blockIdx.x; i < p.sizeF; i += gridDim.x) {
+        int64_t oA = 0, oB = 0, oC = 0, oD = 0;
+        int64_t r = i;
+        for (int j = 0; j < p.nF; j++) {
+            int64_t c = r % p.F_ext[j];
+            r /= p.F_ext[j];
+            oA += c * p.F_sA[j];
+            oB += c * p.F_sB[j];
+            oC += c * p.F_sC[j];
+            oD += c * p.F_sD[j];
+        }
+        R sr = 0, si = 0;
+        for (int64_t k = threadIdx.x; k < p.sizeK; k += blockDim.x) {
+            uint32_t rk = (uint32_t)k;
+            int64_t kA = oA, kB = oB;
+            for (int j = 0; j < p.nK; j++) {
+                uint32_t q = fdiv(rk, p.fK[j]);
+                int64_t c = rk - q * p.fK[j].d;
+                rk = q;
+                kA += c * p.K_sA[j];
+                kB += c * p.K_sB[j];
+            }
+            R ar, ai, br, bi;
+            unary_sum<R, CPLX>(A, kA, p.tA, p.conjA, p.round_in, p.nUA, p.sizeUA, p.UA_ext, p.UA_s, ar, ai);
+            unary_sum<R, CPLX>(B, kB, p.tB, p.conjB, p.round_in, p.nUB, p.sizeUB, p.UB_ext, p.UB_s, br, bi);
+            cmac<R, CPLX>(sr, si, ar, ai, br, bi);
+        }
+        sr = warp_sum(sr);
+        if (CPLX) si = warp_sum(si);
+        const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+        if (l == 0) { red[0][w] = sr; red[1][w] = si; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            R tr = 0, ti = 0;
+            for (int j = 0; j < (int)(blockDim.x >> 5); j++) { tr += red[0][j]; ti += red[1][j]; }
+            finish<R, CPLX>(p, tr, ti, C, oC, D, oD);
+        }
+        __syncthreads();
+    }
+}
+
+static void fill_params(const tb_plan* P, GenParams& g)
+{
+    memset(&g, 0, sizeof(g));
+    g.nF = P->F.n; g.nK = P->K.n; g.nUA = P->UA.n; g.nUB = P->UB.n;
+    g.tA = P->tA; g.tB = P->tB; g.tC = P->tC; g.tD = P->tD;
+    g.round_in = P->round_in;
+    g.conjA = P->conjA; g.conjB = P->conjB; g.conjC = P->conjC; g.conjD = P->conjD;
+    g.conjD_f32 = P->conjD_round_f32;
+    g.beta_zero = P->beta_zero;
+    g.sizeF = P->F.size; g.sizeK = P->K.size; g.sizeUA = P->UA.size; g.sizeUB = P->UB.size;
+    g.alpha_re = P->alpha_re; g.alpha_im = P->alpha_im;
+    g.beta_re = P->beta_re; g.beta_im = P->beta_im;
+    g.small_F = P->F.size < (1ll << 31);
+    for (int j = 0; j < P->F.n; j++) {
+        g.F_ext[j] = P->F.ext[j];
+        g.fF[j] = make_fastdiv(g.small_F ? (uint32_t)P->F.ext[j] : 1u);
+        g.F_sA[j] = P->F.sA[j]; g.F_sB[j] = P->F.sB[j]; g.F_sC[j] = P->F.sC[j]; g.F_sD[j] = P->F.sD[j];
+    }
+    for (int j = 0; j < P->K.n; j++) {
+        g.K_ext[j] = P->K.ext[j];
+        g.fK[j] = make_fastdiv(P->K.size < (1ll << 31) ? (uint32_t)P->K.ext[j] : 1u);
+        g.K_sA[j] = P->K.sA[j]; g.K_sB[j] = P->K.sB[j];
+    }
+    for (int j = 0; j < P->UA.n; j++) { g.UA_ext[j] = P->UA.ext[j]; g.UA_s[j] = P->UA.sA[j]; }
+    for (int j = 0; j < P->UB.n; j++) { g.UB_ext[j] = P->UB.ext[j]; g.UB_s[j] = P->UB.sB[j]; }
+}
+
+template <typename R, bool CPLX>
+static cudaError_t launch_typed(const GenParams& g, int path, const tb_ptrs* d, cudaStream_t s)
+{
+    if (path == TB_PATH_REDUCE && g.sizeK < (1ll << 31)) {
+        int64_t blocks = g.sizeF < 148 * 16 ? g.sizeF : 148 * 16;
+        k_reduce<R, CPLX><<<(unsigned)blocks, 256, 0, s>>>(g, d->A, d->B, d->C, d->D);
+    } else {
+        int64_t blocks = (g.sizeF + 255) / 256;
+        if (blocks > 148 * 64) blocks = 148 * 64;
+        if (blocks < 1) blocks = 1;
+        k_elementwise<R, CPLX><<<(unsigned)blocks, 256, 0, s>>>(g, d->A, d->B, d->C, d->D);
+    }
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_generic(const tb_plan* P, const tb_ptrs* d, cudaStream_t s)
+{
+    GenParams g;
+    fill_params(P, g);
+    switch (P->compute) {
+    case TB_R32: return launch_typed<float, false>(g, P->path, d, s);
+    case TB_R64: return launch_typed<double, false>(g, P->path, d, s);
+    case TB_C32: return launch_typed<float, true>(g, P->path, d, s);
+    case TB_C64: return launch_typed<double, true>(g, P->path, d, s);
+    }
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace tb

@@ -1,0 +1,114 @@
+/*
+ * Internal objects of the B200 TAPP library (host side, C11).
+ */
+#ifndef TB_INTERNAL_H_
+#define TB_INTERNAL_H_
+
+#include <pthread.h>
+#include <stdint.h>
+
+#include "tapp.h"
+#include "tapp_b200.h"
+#include "../tb_plan.h"
+#include "../tb_cuda.h"
+
+#define TB_MAGIC_INFO 0x54420001
+#define TB_MAGIC_PRODUCT 0x54420002
+#define TB_MAGIC_HANDLE 0x54420003
+#define TB_MAGIC_STATUS 0x54420005
+
+/* tensor info: ref_impl.h:13-19 of the reference holds the same fields */
+struct tb_info {
+    int magic;
+    TAPP_datatype type;
+    int nmode;
+    int64_t* extents;
+    int64_t* strides;
+};
+
+/* executor: the first int is the executor id the reference's product checks
+ * (1 = the reference's own executor, product.c:878-885) */
+struct tb_executor {
+    int id;
+    int reserved;
+    void* stream;          /* cudaStream_t, NULL = legacy default stream */
+    int async;
+    int f32_mode;
+    int force_path;
+    int want_status;
+};
+
+struct tb_handle {
+    int magic;
+    int device;
+};
+
+struct tb_status {
+    int magic;
+    int path;
+    int kernels;
+    int tc_mode;
+    double flops;
+    double device_us;
+};
+
+/* cached launch plan of a product, keyed on the infos' contents */
+struct tb_plan_cache {
+    int valid;
+    int key_len;
+    int64_t* key;
+    int f32_mode, force_path;
+    tb_plan plan;
+};
+
+/* product: ref_impl.h:21-37 of the reference; infos are kept by reference */
+struct tb_product {
+    int magic;
+    TAPP_handle handle;
+    TAPP_element_op op[4];
+    TAPP_tensor_info info[4];
+    int64_t* idx[4];
+    int nidx[4];
+    TAPP_prectype prec;
+    pthread_mutex_t lock;
+    struct tb_plan_cache cache;
+};
+
+/* registry of executors created by this library */
+int tb_executor_is_ours(TAPP_executor e);
+int tb_handle_is_ours(TAPP_handle h);
+
+/* snapshot of one tensor at execute time */
+typedef struct tb_tensor_view {
+    TAPP_datatype type;
+    int nmode;
+    int op;
+    const int64_t* extents;
+    const int64_t* strides;
+    const int64_t* idx;
+} tb_tensor_view;
+
+/* validate.c: the reference's check chain (product.c:199-206) without the
+ * executor check; returns the first failing code or 0 */
+int tb_validate(const tb_tensor_view* A, const tb_tensor_view* B,
+                const tb_tensor_view* C, const tb_tensor_view* D,
+                const void* beta, int C_present);
+int tb_scalar_is_zero(const void* s, TAPP_datatype t);
+
+/* planner.c */
+typedef struct tb_plan_options {
+    int f32_mode;     /* TAPP_B200_ATTR_F32_MODE */
+    int force_path;   /* TAPP_B200_ATTR_PATH */
+} tb_plan_options;
+
+int tb_build_plan(const tb_tensor_view* A, const tb_tensor_view* B,
+                  const tb_tensor_view* C, const tb_tensor_view* D,
+                  TAPP_prectype prec, const void* alpha, const void* beta,
+                  const tb_plan_options* opt, tb_plan* out);
+int tb_plan_set_scalars(tb_plan* P, const void* alpha, const void* beta);
+size_t tb_describe(const tb_plan* p, size_t maxlen, char* out);
+double tb_plan_flops(const tb_plan* p);
+int tb_elem_bytes(TAPP_datatype t);
+int tb_is_complex(TAPP_datatype t);
+
+#endif /* TB_INTERNAL_H_ */

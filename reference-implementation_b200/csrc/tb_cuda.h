@@ -1,0 +1,52 @@
+/*
+ * C ABI of the CUDA layer. The host library (C) calls only these functions;
+ * they are implemented in the .cu translation units. Return values are 0 on
+ * success or a cudaError_t value.
+ */
+#ifndef TB_CUDA_H_
+#define TB_CUDA_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "tb_plan.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { TBK_PTR_HOST = 0, TBK_PTR_HOST_PINNED = 1, TBK_PTR_DEVICE = 2, TBK_PTR_MANAGED = 3 };
+enum { TBK_H2D = 0, TBK_D2H = 1, TBK_D2D = 2 };
+enum { TBK_ERR_NOMEM = 2 };  /* cudaErrorMemoryAllocation */
+
+int tbk_device_count(int* count);
+int tbk_pointer_kind(const void* p, int* kind, int* device);
+int tbk_get_device(int* dev);
+int tbk_set_device(int dev);
+int tbk_malloc(void** p, size_t bytes, void* stream);
+int tbk_free(void* p, void* stream);
+int tbk_memcpy(void* dst, const void* src, size_t bytes, int dir, void* stream);
+int tbk_stream_sync(void* stream);
+
+/* Device time between two points on a stream: begin records an event pair
+ * slot, end records the second event; elapsed waits for it. */
+int tbk_timer_begin(void* stream, void** timer);
+int tbk_timer_end(void* stream, void* timer);
+int tbk_timer_elapsed_us(void* timer, double* us);   /* frees the timer */
+
+/* Runs the plan on device-accessible operands. kernels receives the number
+ * of kernels launched. */
+int tbk_run_plan(const tb_plan* plan, const tb_ptrs* ptrs, void* stream, int* kernels);
+
+/* Runs the plan on num independent operand sets in one grouped launch
+ * where the path allows it. */
+int tbk_run_plan_batched(const tb_plan* plan, const tb_ptrs* ptrs, int num, void* stream, int* kernels);
+
+long long tbk_launch_count(void);
+const char* tbk_error_string(int err);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TB_CUDA_H_ */
