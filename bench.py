@@ -1,0 +1,514 @@
+#!/usr/bin/env python3
+"""Benchmark of the TAPP tensor product on B200 (one JSON line on stdout).
+
+Workload (one step = one TAPP_execute_product): the dense 4-index
+contraction D[a,b,i,j] = sum_{c,d} A[a,c,i,d] B[d,b,c,j] + 0.5 C with every
+extent 64 (M = N = K = 4096), float32 storage, inputs N(0,1) with 1% of the
+entries scaled by 1e3, synthetic and seeded. The headline precision is
+TAPP_BF16BF16_ACCUM_F32 (bfloat16 products, float32 accumulation); the line
+also reports the other precision modes of the same product, among them the
+plain CUDA-core float32 path, each with its error against a binary64
+evaluation.
+
+  value      TFLOP/s with all operands resident in HBM (2*M*N*K flops per
+             step, CUDA events on the launching stream, max over ranks)
+  e2e        the same through the C ABI with pinned HOST buffers: each step
+             copies A, B, C to the device and D back (inside the timed region)
+  roofline   the dominant kernel (the tcgen05 GEMM): algorithmic flops per
+             launch / its measured duration, against the measured bf16 peak
+  cpu_baseline  the reference's own CPU product (built from its sources into
+             oracle/_ref) on this host's cores, on a bounded slab of D
+
+`--impl reference` times only the reference's CPU product (all host threads)
+on the same workload and prints its line. Multi-GPU runs (torchrun) are
+replicas: every rank runs the whole product on its own GPU, no collective on
+the data path; timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+for p in (REPO, os.path.join(REPO, "reference-implementation_b200")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+import numpy as np  # noqa: E402
+
+EXTENT = 64
+FLOPS = 2.0 * (EXTENT ** 2) ** 3          # 2 * M * N * K
+WORKLOAD = "dense_4index_contraction_64^4"
+MODES = {
+    # name: (precision, storage of A and B, f32_mode, forced path)
+    "bf16": (6, 0, 0, 0),
+    "f16": (5, 0, 0, 0),
+    "bf16_storage": (6, 5, 0, 0),
+    "f16_storage": (5, 4, 0, 0),
+    "split_bf16_f32": (0, 0, 1, 0),
+    "plain_f32": (0, 0, 0, 1),
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--no-modes", action="store_true", help="skip the non-headline precision modes")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--only-headline", action="store_true",
+                    help="run only the timed headline steps (for profiling); prints its timing")
+    return ap.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)),
+            int(os.environ.get("WORLD_SIZE", 1)))
+
+
+# --------------------------------------------------------------------------
+# CPU reference product (the reference built from its sources, else the
+# oracle's restatement of it)
+
+def cpu_reference_run(threads: int | None = None, i_slab: int = 16):
+    """Times the reference's CPU product on `threads` disjoint slabs of D
+    (D[:, :, 0:i_slab, t] for thread t, views into the same tensors), in
+    TAPP_F32F32_ACCUM_F32: the reference's BF16 precision does not compile
+    and its default build leaves D untouched for it. Returns a dict."""
+    import oracle
+    from tapp_b200.workloads import large_dense_case
+    from tapp_b200.case import Tensor, Case
+    threads = threads or os.cpu_count() or 1
+    threads = min(threads, EXTENT)
+    ref = oracle.reference_lib()
+    kind = "reference" if ref is not None else "port"
+    case = large_dense_case(np.random.default_rng(0), 0, 0, extent=EXTENT)
+    ora = None if ref is not None else oracle.Oracle()
+
+    def slab(t):
+        D = case.D
+        ext = [EXTENT, EXTENT, i_slab, 1]
+        sub = Tensor(D.dtype, ext, list(D.strides), list(D.idx), 0, D.buf, D.base + t * D.strides[3])
+        Cs = Tensor(case.C.dtype, ext, list(case.C.strides), list(case.C.idx), 0, case.C.buf,
+                    case.C.base + t * case.C.strides[3])
+        B = case.B
+        Bs = Tensor(B.dtype, [EXTENT, EXTENT, EXTENT, 1], list(B.strides), list(B.idx), 0, B.buf,
+                    B.base + t * B.strides[3])
+        A = case.A
+        As = Tensor(A.dtype, [EXTENT, EXTENT, i_slab, EXTENT], list(A.strides), list(A.idx), 0, A.buf, A.base)
+        return Case(As, Bs, Cs, sub, case.alpha, case.beta, 0, False, "slab")
+
+    slabs = [slab(t) for t in range(threads)]
+    errs = [None] * threads
+
+    def work(t):
+        errs[t] = slabs[t].run(ref) if ref is not None else ora.execute(slabs[t])
+
+    ths = [threading.Thread(target=work, args=(t,)) for t in range(threads)]
+    t0 = time.perf_counter()
+    for th in ths:
+        th.start()
+    for th in ths:
+        th.join()
+    wall = time.perf_counter() - t0
+    assert all(e == 0 for e in errs), errs
+    flops = 2.0 * (EXTENT * EXTENT * i_slab) * EXTENT ** 2 * threads
+    return {"value": flops / wall / 1e12, "unit": "TFLOP/s", "cores": threads, "kind": kind,
+            "sample": f"{threads} threads x D[:,:,0:{i_slab},t] slab ({EXTENT * EXTENT * i_slab} outputs x "
+                      f"K={EXTENT ** 2} each), F32F32_ACCUM_F32 (the reference runs no bfloat16 product); "
+                      f"{wall:.1f} s wall",
+            "seconds": wall}
+
+
+def run_reference(args):
+    rank, _, world = dist_env()
+    if rank != 0:
+        return
+    vals = []
+    for _ in range(min(max(args.warmup, 0), 3)):
+        cpu_reference_run(i_slab=1)
+    info = None
+    total = 0.0
+    for _ in range(max(args.steps, 1)):
+        info = cpu_reference_run(i_slab=2)
+        vals.append(info["value"])
+        total += info["seconds"]
+        if total > 90.0:  # keep the whole run within a few minutes
+            break
+    value = statistics.median(vals)
+    line = {"metric": f"TFLOP/s ({WORKLOAD})", "value": value, "unit": "TFLOP/s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": len(vals), "warmup": args.warmup,
+            "ms_per_step": FLOPS / (value * 1e12) * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "extents": EXTENT, "M": EXTENT ** 2, "N": EXTENT ** 2,
+                       "K": EXTENT ** 2, "precision": "F32F32_ACCUM_F32 (reference has no bf16 product)",
+                       "timed": "bounded slab of D per step, extrapolated per flop"},
+            "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": info["cores"], "kind": info["kind"],
+                             "sample": info["sample"]},
+            "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------
+# GPU
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons (read-only)."""
+    FIELDS = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc is None:
+            return
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self, t0=None, t1=None):
+        """Median SM clock and the throttle reasons seen in [t0, t1] (wall
+        clock); all samples when the window holds none."""
+        from datetime import datetime
+        rows = []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                ts = datetime.strptime(f[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                rows.append((ts, float(f[1]), float(f[2]), f[4:8]))
+            except ValueError:
+                continue
+        inside = [r for r in rows if t0 is not None and t0 <= r[0] <= t1]
+        use = inside or rows
+        reasons = set()
+        for r in use:
+            for n, v in zip(names, r[3]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median([r[1] for r in use]) if use else None,
+                "sm_max_mhz": use[-1][2] if use else None, "reasons": sorted(reasons),
+                "samples": len(use), "samples_in_timed_region": len(inside)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return p["bf16_tflops"], "measured"
+    except (OSError, KeyError, ValueError):
+        return 1590.0, "fallback"
+
+
+def profiled_traffic():
+    """dram bytes per GEMM launch from the committed ncu summary, if any."""
+    path = os.path.join(REPO, "profiles", "k_gemm_dense_4index_64.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+class Product:
+    """One TAPP product bound to device (or host) buffers."""
+
+    def __init__(self, lib, case, tensors, executor):
+        self.lib = lib
+        self.case = case
+        self.ex = executor
+        self.infos = [lib.tensor_info(t.dtype, t.extents, t.strides)[1] for t in (case.A, case.B, case.C, case.D)]
+        err, self.plan = lib.create_product(0, [t.op for t in (case.A, case.B, case.C, case.D)], self.infos,
+                                            [case.A.idx, case.B.idx, case.C.idx, case.D.idx], case.prec)
+        assert err == 0
+        self.ptrs = tensors
+
+    def __call__(self, status=None):
+        st = C.c_ssize_t(0)
+        err = self.lib.lib.TAPP_execute_product(self.plan, self.ex, C.byref(st), self.case.alpha.ctypes.data,
+                                                self.ptrs[0], self.ptrs[1], self.case.beta.ctypes.data,
+                                                self.ptrs[2], self.ptrs[3])
+        if err:
+            raise RuntimeError(f"TAPP_execute_product failed: {err} {self.lib.explain(err)}")
+        if status is not None:
+            status.append(st.value)
+
+    def close(self):
+        self.lib.lib.TAPP_destroy_tensor_product(self.plan)
+        for h in self.infos:
+            self.lib.lib.TAPP_destroy_tensor_info(h)
+
+
+def to_device(t, torch):
+    x = torch.from_numpy(t.buf.view(np.uint8)).cuda()
+    return x, x.data_ptr() + t.base * t.itemsize
+
+
+def make_executor(lib, stream, f32_mode=0, path=0, async_=True, status=False):
+    import tapp_b200
+    ex = lib.create_executor()
+    if stream is not None:
+        lib.set_stream(ex, stream)
+    lib.set_int(ex, tapp_b200.ATTR_ASYNC, 1 if async_ else 0)
+    lib.set_int(ex, tapp_b200.ATTR_F32_MODE, f32_mode)
+    lib.set_int(ex, tapp_b200.ATTR_PATH, path)
+    lib.set_int(ex, tapp_b200.ATTR_WANT_STATUS, 1 if status else 0)
+    return ex
+
+
+def time_device(torch, fn, steps, warmup, barrier, window=None):
+    """Mean device time of one step in ms: `warmup` untimed steps, then
+    `steps` steps between CUDA events on the current stream, bracketed by a
+    barrier and a device synchronisation on both sides."""
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    s = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    w0 = time.time()
+    e0.record(s)
+    for _ in range(steps):
+        fn()
+    e1.record(s)
+    torch.cuda.synchronize()
+    w1 = time.time()
+    barrier()
+    if window is not None:
+        window[:] = [w0, w1]
+    return e0.elapsed_time(e1) / steps  # ms
+
+
+def mode_case(name, rng_seed=1):
+    from tapp_b200.workloads import large_dense_case
+    prec, storage, _, _ = MODES[name]
+    return large_dense_case(np.random.default_rng(rng_seed), prec, storage, extent=EXTENT)
+
+
+def f64_slab_reference(lib, torch, case, j_count=2):
+    """Binary64 evaluation, on the GPU through the library's own F64F64
+    path, of D[:, :, :, 0:j_count] for the exact stored inputs of `case`."""
+    from tapp_b200.case import Tensor, Case, alloc, scalar, bf16_to_f32
+    from tapp_b200.abi import TAPP_F64, TAPP_BF16
+
+    def f64(t, ext=None):
+        vals = bf16_to_f32(t.buf) if t.dtype == TAPP_BF16 else t.buf
+        T = Tensor(TAPP_F64, list(ext or t.extents), list(t.strides), list(t.idx), 0,
+                   np.asarray(vals, dtype=np.float64).copy(), t.base)
+        return T
+    e = EXTENT
+    A = f64(case.A)
+    B = f64(case.B, [e, e, e, j_count])
+    Cc = f64(case.C, [e, e, e, j_count])
+    D = f64(case.D, [e, e, e, j_count])
+    c64 = Case(A, B, Cc, D, scalar(TAPP_F64, float(case.alpha[0])), scalar(TAPP_F64, float(case.beta[0])), 1)
+    dev = [to_device(t, torch) for t in (A, B, Cc, D)]
+    ex = make_executor(lib, None, async_=False)
+    prod = Product(lib, c64, [d[1] for d in dev], ex)
+    prod()
+    prod.close()
+    lib.lib.TAPP_destroy_executor(ex)
+    out = dev[3][0].cpu().numpy().view(np.float64)
+    offs = D.offsets()
+    return out[D.base + offs]
+
+
+def slab_values(case_D, dbuf, j_count=2):
+    from tapp_b200.case import Tensor
+    e = EXTENT
+    sub = Tensor(case_D.dtype, [e, e, e, j_count], list(case_D.strides), list(case_D.idx), 0, None, case_D.base)
+    return dbuf[case_D.base + sub.offsets()].astype(np.float64)
+
+
+def run_b200(args):
+    import torch
+    import tapp_b200
+    rank, local_rank, world = dist_env()
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    lib = tapp_b200.load()
+    stream = torch.cuda.current_stream().cuda_stream
+
+    # ---------------- headline: BF16BF16_ACCUM_F32, operands in HBM ----------------
+    case = mode_case("bf16")
+    dev = [to_device(t, torch) for t in (case.A, case.B, case.C, case.D)]
+    ex = make_executor(lib, stream)
+    prod = Product(lib, case, [d[1] for d in dev], ex)
+    n0 = lib.launches()
+    window = [None, None]
+    with ClockSampler(local_rank) as clk:
+        t_ms = time_device(torch, prod, args.steps, args.warmup, barrier, window)
+    launches = lib.launches() - n0
+    gpu_launches = launches * args.steps // (args.steps + args.warmup)
+    clocks = clk.summary(*window)
+    if args.only_headline:
+        if rank == 0:
+            print(json.dumps({"ms_per_step": t_ms, "tflops": FLOPS / (t_ms * 1e-3) / 1e12,
+                              "gpu_launches": gpu_launches}), flush=True)
+        prod.close()
+        lib.lib.TAPP_destroy_executor(ex)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    t_max = t_ms
+    if dist is not None:
+        x = torch.tensor([t_ms], device="cuda")
+        dist.all_reduce(x, op=dist.ReduceOp.MAX)
+        t_max = float(x.item())
+    value = world * FLOPS / (t_max * 1e-3) / 1e12
+
+    # ---------------- dominant kernel: GEMM duration per launch ----------------
+    ex_s = make_executor(lib, stream, async_=False, status=True)
+    prod_s = Product(lib, case, [d[1] for d in dev], ex_s)
+    mains, devs = [], []
+    for i in range(min(max(args.steps, 3), 20)):
+        st = []
+        prod_s(st)
+        mains.append(lib.status_value(st[0], tapp_b200.STATUS_MAIN_US))
+        devs.append(lib.status_value(st[0], tapp_b200.STATUS_DEVICE_US))
+        lib.lib.TAPP_destroy_status(st[0])
+    main_us = statistics.median(mains[1:] if len(mains) > 1 else mains)
+    dev_us = statistics.median(devs[1:] if len(devs) > 1 else devs)
+    peak, peak_kind = measured_peaks()
+    achieved = FLOPS / (main_us * 1e-6) / 1e12
+    traffic = profiled_traffic()
+    roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak, "traffic": traffic, "peak_source": f"{peak_kind} bf16 dense burst",
+                "kernel": "tb::tc::k_gemm", "kernel_us": main_us, "step_device_us": dev_us,
+                "flops_per_launch": FLOPS}
+    prod_s.close()
+    lib.lib.TAPP_destroy_executor(ex_s)
+
+    # ---------------- other precision modes, with binary64 error ----------------
+    modes = {}
+    ref64 = f64_slab_reference(lib, torch, case) if not args.no_modes else None
+    D_head = dev[3][0].cpu().numpy().view(np.float32)
+    if ref64 is not None:
+        err = np.abs(slab_values(case.D, D_head) - ref64)
+        modes["bf16"] = {"tflops": value / world, "max_abs_err_rel_to_max": float(err.max() / np.abs(ref64).max())}
+    if not args.no_modes:
+        for name, (prec, storage, f32_mode, path) in MODES.items():
+            if name == "bf16":
+                continue
+            mc = mode_case(name)
+            mdev = [to_device(t, torch) for t in (mc.A, mc.B, mc.C, mc.D)]
+            mex = make_executor(lib, stream, f32_mode=f32_mode, path=path)
+            mp = Product(lib, mc, [d[1] for d in mdev], mex)
+            steps = max(2, min(args.steps, 20)) if path == 1 else args.steps
+            mt = time_device(torch, mp, steps, 1 if path == 1 else args.warmup, barrier)
+            mref = ref64 if storage == 0 else f64_slab_reference(lib, torch, mc)
+            Dm = mdev[3][0].cpu().numpy().view(np.float32)
+            merr = np.abs(slab_values(mc.D, Dm) - mref)
+            modes[name] = {"tflops": FLOPS / (mt * 1e-3) / 1e12, "ms": mt,
+                           "max_abs_err_rel_to_max": float(merr.max() / np.abs(mref).max())}
+            mp.close()
+            lib.lib.TAPP_destroy_executor(mex)
+            del mdev
+    plain = modes.get("plain_f32", {}).get("tflops")
+
+    # ---------------- end to end through host buffers ----------------
+    pinned = []
+    for t in (case.A, case.B, case.C, case.D):
+        h = torch.from_numpy(t.buf.view(np.uint8)).pin_memory()
+        pinned.append((h, h.data_ptr() + t.base * t.itemsize))
+    ex_h = make_executor(lib, None, async_=False)
+    prod_h = Product(lib, case, [p[1] for p in pinned], ex_h)
+    e2e_steps = max(3, min(args.steps, 20))
+    for _ in range(2):
+        prod_h()
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        prod_h()
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if dist is not None:
+        x = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(x, op=dist.ReduceOp.MAX)
+        e2e_s = float(x.item())
+    h2d = sum(t.buf.nbytes for t in (case.A, case.B, case.C))
+    d2h = case.D.buf.nbytes
+    e2e = {"value": world * FLOPS / e2e_s / 1e12, "unit": "TFLOP/s", "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1e3,
+           "how": "TAPP_execute_product on pinned host buffers, synchronous; wall clock per call"}
+    prod_h.close()
+    lib.lib.TAPP_destroy_executor(ex_h)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_reference_run()
+        cpu.pop("seconds", None)
+
+    if rank == 0:
+        line = {"metric": f"TFLOP/s ({WORKLOAD}, BF16BF16_ACCUM_F32)", "value": value, "unit": "TFLOP/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16",
+                "data": "synthetic",
+                "config": {"workload": WORKLOAD, "extents": EXTENT, "M": EXTENT ** 2, "N": EXTENT ** 2,
+                           "K": EXTENT ** 2, "storage": "f32 A,B,C,D", "precision": "BF16BF16_ACCUM_F32",
+                           "parallelism": f"replicas x{world}",
+                           "l2": "inputs 256 MiB > 126 MB L2 (A,B,C,D 64 MiB each)",
+                           "step": "pack A, pack B, tcgen05 GEMM + fused epilogue"},
+                "vs_plain_gpu": (value / world / plain) if plain else None,
+                "modes": modes, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu,
+                "clocks": clocks, "gpu_launches": gpu_launches}
+        print(json.dumps(line), flush=True)
+    prod.close()
+    lib.lib.TAPP_destroy_executor(ex)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -59,6 +59,8 @@ enum {
     TAPP_B200_STATUS_DEVICE_US = 0x1103, /* double: device time of the launches, microseconds
                                           * (synchronous executions only) */
     TAPP_B200_STATUS_TC_MODE = 0x1104,   /* int: tensor-core operand mode (0 bf16, 1 f16, 2 split bf16) */
+    TAPP_B200_STATUS_MAIN_US = 0x1105,   /* double: device time of the dominant kernel (the tensor-core
+                                          * GEMM, or the CUDA-core kernel), microseconds */
 };
 
 /*

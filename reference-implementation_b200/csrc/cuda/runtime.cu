@@ -3,6 +3,7 @@
 // plan to its kernels.
 #include <atomic>
 #include <cstdio>
+#include <mutex>
 
 #include "../tb_cuda.h"
 #include "tb_common.cuh"
@@ -13,8 +14,58 @@ static std::atomic<long long> g_launches{0};
 
 void count_launch(int n) { g_launches += n; }
 
+// One device word per GPU that kernels set when a bounded wait expires; the
+// host reads and clears it after synchronous executions.
+static int* g_err_word[64];
+static std::mutex g_err_mutex;
+
+int* device_error_word()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lk(g_err_mutex);
+    if (!g_err_word[dev]) {
+        int* p = nullptr;
+        if (cudaMalloc(&p, sizeof(int)) != cudaSuccess) return nullptr;
+        if (cudaMemset(p, 0, sizeof(int)) != cudaSuccess) return nullptr;
+        g_err_word[dev] = p;
+    }
+    return g_err_word[dev];
+}
+
+// The library's own stream-ordered memory pool per GPU. Its release
+// threshold is unlimited, so scratch and staging buffers freed by one call
+// are reused by the next instead of being unmapped at every synchronisation
+// (the device default pool's threshold of 0 would do that).
+static cudaMemPool_t g_pool[64];
+static std::mutex g_pool_mutex;
+
+cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t s)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaMallocAsync(p, bytes, s);
+    {
+        std::lock_guard<std::mutex> lk(g_pool_mutex);
+        if (!g_pool[dev]) {
+            cudaMemPoolProps props = {};
+            props.allocType = cudaMemAllocationTypePinned;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = dev;
+            cudaMemPool_t pool;
+            e = cudaMemPoolCreate(&pool, &props);
+            if (e != cudaSuccess) return e;
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+            g_pool[dev] = pool;
+        }
+    }
+    return cudaMallocFromPoolAsync(p, bytes, g_pool[dev], s);
+}
+
 cudaError_t launch_generic(const tb_plan* P, const tb_ptrs* d, cudaStream_t s);
-cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t s, int* kernels);
+cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t s, int* kernels, void** main_timer);
 
 }  // namespace tb
 
@@ -50,7 +101,7 @@ int tbk_set_device(int dev) { return (int)cudaSetDevice(dev); }
 int tbk_malloc(void** p, size_t bytes, void* stream)
 {
     if (bytes == 0) bytes = 16;
-    cudaError_t e = cudaMallocAsync(p, bytes, (cudaStream_t)stream);
+    cudaError_t e = tb::pool_alloc(p, bytes, (cudaStream_t)stream);
     if (e != cudaSuccess) (void)cudaGetLastError();
     return (int)e;
 }
@@ -103,16 +154,18 @@ int tbk_timer_elapsed_us(void* timer, double* us)
     return (int)e;
 }
 
-int tbk_run_plan(const tb_plan* plan, const tb_ptrs* ptrs, void* stream, int* kernels)
+int tbk_run_plan(const tb_plan* plan, const tb_ptrs* ptrs, void* stream, int* kernels, void** main_timer)
 {
     cudaStream_t s = (cudaStream_t)stream;
     *kernels = 0;
     cudaError_t e = cudaSuccess;
     switch (plan->path) {
     case TB_PATH_NOOP: return 0;
-    case TB_PATH_TC: e = tb::launch_tc(plan, ptrs, 1, s, kernels); break;
+    case TB_PATH_TC: e = tb::launch_tc(plan, ptrs, 1, s, kernels, main_timer); break;
     default:
+        if (main_timer) tbk_timer_begin(stream, main_timer);
         e = tb::launch_generic(plan, ptrs, s);
+        if (main_timer) tbk_timer_end(stream, *main_timer);
         *kernels = 1;
         break;
     }
@@ -123,10 +176,10 @@ int tbk_run_plan_batched(const tb_plan* plan, const tb_ptrs* ptrs, int num, void
 {
     cudaStream_t s = (cudaStream_t)stream;
     *kernels = 0;
-    if (plan->path == TB_PATH_TC) return (int)tb::launch_tc(plan, ptrs, num, s, kernels);
+    if (plan->path == TB_PATH_TC) return (int)tb::launch_tc(plan, ptrs, num, s, kernels, nullptr);
     for (int i = 0; i < num; i++) {
         int k = 0;
-        int e = tbk_run_plan(plan, &ptrs[i], stream, &k);
+        int e = tbk_run_plan(plan, &ptrs[i], stream, &k, nullptr);
         *kernels += k;
         if (e) return e;
     }
@@ -134,6 +187,20 @@ int tbk_run_plan_batched(const tb_plan* plan, const tb_ptrs* ptrs, int num, void
 }
 
 long long tbk_launch_count(void) { return tb::g_launches.load(); }
+
+int tbk_check_device_error(void)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64 || !tb::g_err_word[dev]) return 0;
+    int v = 0;
+    cudaError_t e = cudaMemcpy(&v, tb::g_err_word[dev], sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return (int)e;
+    if (v) {
+        cudaMemset(tb::g_err_word[dev], 0, sizeof(int));
+        return (int)cudaErrorLaunchTimeout;
+    }
+    return 0;
+}
 
 const char* tbk_error_string(int err) { return cudaGetErrorString((cudaError_t)err); }
 

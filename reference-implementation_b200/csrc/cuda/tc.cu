@@ -1,19 +1,923 @@
-// Tensor-core path (pack pre-pass + tcgen05 GEMM). Placeholder until the
-// kernels land: routes to the CUDA-core kernels.
+// Tensor-core path for real- and complex-valued products on sm_100a.
+//
+//   1. k_pack (twice): gathers op_A(A) and op_B(B) from their strided layouts
+//      into K-major 16-bit operand panels A''[l][m][k'] and B''[l][n'][k'],
+//      summing unary modes, conjugating, and rounding to the precision's
+//      operand format on the way (the reference's get_val /
+//      sum_unary_contractions, product.c:1863, :10830). Complex operands
+//      become real panels (4M form): A'' holds (re, im) pairs along k',
+//      B'' holds two rows per n, (re, -im) and (im, re), so one real GEMM
+//      yields the real and imaginary parts in adjacent columns. The split
+//      mode for binary32 stores three segments along k' — A: hi, hi, lo and
+//      B: hi, lo, hi with hi = bf16(x), lo = bf16(x - hi) — so the GEMM sums
+//      hi*hi + hi*lo + lo*hi.
+//   2. k_gemm: persistent warp-specialised GEMM, one 128x256 output tile per
+//      step: warp 0 issues TMA loads (128B-swizzled, 4-stage mbarrier ring),
+//      warp 1 issues tcgen05.mma (kind::f16, fp32 accumulators in TMEM,
+//      two accumulator buffers), warp 2 owns the TMEM allocation, warps 4-7
+//      drain TMEM with tcgen05.ld and apply the fused epilogue
+//      D = op_D(alpha * acc + beta * op_C(C)) with D's and C's own strides.
+// Every wait on an mbarrier is bounded in time; on expiry the kernel records
+// an error word the host reads back, and returns.
+#include <cuda.h>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+
+#include "../tb_cuda.h"
 #include "tb_common.cuh"
 
 namespace tb {
 cudaError_t launch_generic(const tb_plan* P, const tb_ptrs* d, cudaStream_t s);
+int* device_error_word();
+cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t s);
 
-cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t s, int* kernels)
+namespace tc {
+
+constexpr int BM = 128, BN = 256, BK = 64, STAGES = 4;
+constexpr int A_BYTES = BM * BK * 2;
+constexpr int B_BYTES = BN * BK * 2;
+constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+constexpr int TMEM_COLS = 512;
+constexpr int EPI_WARPS = 8;                    // two warps per TMEM lane quarter
+constexpr int EPI_THREADS = EPI_WARPS * 32;
+constexpr int NTHREADS = 128 + EPI_THREADS;
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/ + 2 * BN * 8 /*column offsets*/;
+constexpr unsigned long long WAIT_NS = 4000000000ull;  // 4 s per wait
+
+struct ModeList {
+    int32_t n;
+    int32_t pad;
+    int64_t ext[TB_MAXMODES];
+    int64_t s0[TB_MAXMODES];  // stride in the first tensor (C, or the packed source)
+    int64_t s1[TB_MAXMODES];  // stride in the second tensor (D)
+};
+
+__host__ __device__ inline void decode2(const ModeList& m, int64_t idx, int64_t& o0, int64_t& o1)
 {
-    tb_plan q = *P;
-    q.path = TB_PATH_GENERIC;
-    for (int i = 0; i < num; i++) {
-        cudaError_t e = launch_generic(&q, &d[i], s);
-        if (e != cudaSuccess) return e;
+    o0 = 0;
+    o1 = 0;
+    for (int j = 0; j < m.n; j++) {
+        int64_t c = idx % m.ext[j];
+        idx /= m.ext[j];
+        o0 += c * m.s0[j];
+        o1 += c * m.s1[j];
     }
-    *kernels = num;
-    return cudaSuccess;
 }
+
+// ---------------------------------------------------------------------------
+// pack
+struct PackParams {
+    const void* src;
+    void* dst;
+    int32_t type, conj, round_mode, cplx, is_B, split, fmt, rows_fast;
+    int64_t R, K, Lsz, Kseg, Kld, Rout;
+    ModeList rows, ks, ls, us;  // s0 = stride in the source tensor
+    int64_t usize;
+};
+
+constexpr int PR = 64, PK = 32;
+
+__device__ __forceinline__ void put16(void* dst, int64_t idx, float v, int fmt)
+{
+    if (fmt == 1) ((__half*)dst)[idx] = __float2half_rn(v);
+    else ((__nv_bfloat16*)dst)[idx] = __float2bfloat16_rn(v);
+}
+
+__device__ __forceinline__ float q16(float v, int fmt)
+{
+    return fmt == 1 ? __half2float(__float2half_rn(v)) : __bfloat162float(__float2bfloat16_rn(v));
+}
+
+__global__ void __launch_bounds__(256) k_pack(PackParams p)
+{
+    __shared__ float vr[PR][PK + 1];
+    __shared__ float vi[PR][PK + 1];
+    __shared__ int64_t rowOff[PR];
+    __shared__ int64_t kOff[PK];
+    __shared__ int64_t lOff;
+    const int64_t r0 = (int64_t)blockIdx.x * PR, k0 = (int64_t)blockIdx.y * PK, l = blockIdx.z;
+    const int t = threadIdx.x;
+    if (t < PR) {
+        int64_t o = 0, dummy;
+        if (r0 + t < p.R) decode2(p.rows, r0 + t, o, dummy);
+        rowOff[t] = o;
+    } else if (t < PR + PK) {
+        int64_t o = 0, dummy;
+        if (k0 + t - PR < p.K) decode2(p.ks, k0 + t - PR, o, dummy);
+        kOff[t - PR] = o;
+    } else if (t == PR + PK) {
+        int64_t o, dummy;
+        decode2(p.ls, l, o, dummy);
+        lOff = o;
+    }
+    __syncthreads();
+    // phase 1: gather source values (coalesced along the source's fastest mode)
+    for (int e = t; e < PR * PK; e += blockDim.x) {
+        int r, kk;
+        if (p.rows_fast) { r = e % PR; kk = e / PR; }
+        else { kk = e % PK; r = e / PK; }
+        float re = 0.f, im = 0.f;
+        if (r0 + r < p.R && k0 + kk < p.K) {
+            const int64_t off = lOff + rowOff[r] + kOff[kk];
+            if (p.us.n == 0) {
+                load_rounded<float>(p.src, off, p.type, p.round_mode, re, im);
+                if (p.conj) im = -im;
+            } else {
+                int64_t c[TB_MAXMODES];
+                for (int j = 0; j < p.us.n; j++) c[j] = 0;
+                int64_t o = off;
+                for (int64_t u = 0; u < p.usize; u++) {
+                    float xr, xi;
+                    load_elem<float>(p.src, o, p.type, xr, xi);
+                    if (p.conj) xi = -xi;
+                    re += xr;
+                    im += xi;
+                    if (p.round_mode != TB_ROUND_NONE) {
+                        re = round_in<float>(re, p.round_mode);
+                        im = round_in<float>(im, p.round_mode);
+                    }
+                    for (int j = 0; j < p.us.n; j++) {
+                        o += p.us.s0[j];
+                        if (++c[j] < p.us.ext[j]) break;
+                        o -= p.us.s0[j] * p.us.ext[j];
+                        c[j] = 0;
+                    }
+                }
+            }
+        }
+        vr[r][kk] = re;
+        vi[r][kk] = im;
+    }
+    __syncthreads();
+    // phase 2: write K-major 16-bit panels, two elements per store
+    const int rmul = (p.cplx && p.is_B) ? 2 : 1;
+    const int cmul = p.cplx ? 2 : 1;
+    const int ocols = PK * cmul;           // output columns of this tile per segment
+    const int orows = PR * rmul;
+    for (int e = t; e < orows * (ocols / 2) * p.split; e += blockDim.x) {
+        const int cp = e % (ocols / 2);
+        const int rest = e / (ocols / 2);
+        const int ro = rest % orows;
+        const int seg = rest / orows;
+        const int r = ro / rmul, variant = ro % rmul;
+        const int64_t rg = r0 + r;
+        if (rg >= p.R) continue;
+        const int64_t col = k0 * cmul + 2 * cp;  // output column of the first element
+        if (col >= p.Kseg) continue;
+        float v[2];
+        for (int h = 0; h < 2; h++) {
+            const int oc = 2 * cp + h;                // column inside the tile
+            float x;
+            if (!p.cplx) {
+                x = vr[r][oc];
+            } else {
+                const int kk = oc >> 1, part = oc & 1;
+                const float a = vr[r][kk], b = vi[r][kk];
+                if (!p.is_B) x = part ? b : a;                 // (re, im)
+                else if (variant == 0) x = part ? -b : a;      // row for the real output
+                else x = part ? a : b;                         // row for the imaginary output
+            }
+            if (p.split == 3) {
+                const float hi = q16(x, 0);
+                const float lo = x - hi;
+                // A: hi, hi, lo   B: hi, lo, hi
+                const bool use_lo = p.is_B ? (seg == 1) : (seg == 2);
+                x = use_lo ? lo : hi;
+            }
+            v[h] = x;
+        }
+        const int64_t base = ((int64_t)l * p.Rout + rg * rmul + variant) * p.Kld + seg * p.Kseg + col;
+        if (col + 1 < p.Kseg) {
+            if (p.fmt == 1) *(__half2*)((__half*)p.dst + base) = __floats2half2_rn(v[0], v[1]);
+            else *(__nv_bfloat162*)((__nv_bfloat16*)p.dst + base) = __floats2bfloat162_rn(v[0], v[1]);
+        } else {
+            put16(p.dst, base, v[0], p.fmt);
+        }
+    }
+}
+
+// Fast pack for the common case: real operands, no unary modes. A 64x64
+// (rows x k) tile per block; 16 independent loads per thread in flight, then
+// 16-byte stores of eight 16-bit values along k.
+constexpr int FR = 64, FK = 64;
+
+template <typename T>
+__device__ __forceinline__ float load_as_float(const void* base, int64_t off)
+{
+    return (float)__ldg((const T*)base + off);
+}
+template <>
+__device__ __forceinline__ float load_as_float<__half>(const void* base, int64_t off)
+{
+    return __half2float(((const __half*)base)[off]);
+}
+template <>
+__device__ __forceinline__ float load_as_float<__nv_bfloat16>(const void* base, int64_t off)
+{
+    return __bfloat162float(((const __nv_bfloat16*)base)[off]);
+}
+
+template <typename T, int SPLIT, int FMT>
+__global__ void __launch_bounds__(256) k_pack_real(PackParams p)
+{
+    __shared__ float v[FR][FK + 1];
+    __shared__ int64_t rowOff[FR];
+    __shared__ int64_t kOff[FK];
+    __shared__ int64_t lOff;
+    const int64_t r0 = (int64_t)blockIdx.x * FR, k0 = (int64_t)blockIdx.y * FK, l = blockIdx.z;
+    const int t = threadIdx.x;
+    if (t < FR) {
+        int64_t o = 0, dummy;
+        if (r0 + t < p.R) decode2(p.rows, r0 + t, o, dummy);
+        rowOff[t] = o;
+    } else if (t < FR + FK) {
+        int64_t o = 0, dummy;
+        if (k0 + t - FR < p.K) decode2(p.ks, k0 + t - FR, o, dummy);
+        kOff[t - FR] = o;
+    } else if (t == FR + FK) {
+        int64_t o, dummy;
+        decode2(p.ls, l, o, dummy);
+        lOff = o;
+    }
+    __syncthreads();
+    float x[FR * FK / 256];
+#pragma unroll
+    for (int u = 0; u < FR * FK / 256; u++) {
+        const int e = t + 256 * u;
+        const int r = p.rows_fast ? (e % FR) : (e / FK);
+        const int kk = p.rows_fast ? (e / FR) : (e % FK);
+        x[u] = (r0 + r < p.R && k0 + kk < p.K) ? load_as_float<T>(p.src, lOff + rowOff[r] + kOff[kk]) : 0.f;
+    }
+#pragma unroll
+    for (int u = 0; u < FR * FK / 256; u++) {
+        const int e = t + 256 * u;
+        const int r = p.rows_fast ? (e % FR) : (e / FK);
+        const int kk = p.rows_fast ? (e / FR) : (e % FK);
+        float y = x[u];
+        if (SPLIT == 1 && p.round_mode != TB_ROUND_NONE) y = round_in<float>(y, p.round_mode);
+        v[r][kk] = y;
+    }
+    __syncthreads();
+    // FR rows x FK/8 groups of eight per segment
+    for (int item = t; item < FR * (FK / 8) * SPLIT; item += 256) {
+        const int g = item % (FK / 8);
+        const int r = (item / (FK / 8)) % FR;
+        const int seg = item / (FR * (FK / 8));
+        const int64_t rg = r0 + r;
+        const int64_t col = k0 + g * 8;
+        if (rg >= p.R || col >= p.Kseg) continue;
+        uint32_t w[4];
+#pragma unroll
+        for (int h = 0; h < 4; h++) {
+            float a = v[r][g * 8 + 2 * h], b = v[r][g * 8 + 2 * h + 1];
+            if (SPLIT == 3) {
+                const float ah = __bfloat162float(__float2bfloat16_rn(a));
+                const float bh = __bfloat162float(__float2bfloat16_rn(b));
+                const bool use_lo = p.is_B ? (seg == 1) : (seg == 2);  // A: hi, hi, lo   B: hi, lo, hi
+                if (use_lo) { a -= ah; b -= bh; } else { a = ah; b = bh; }
+            }
+            if (FMT == 1) {
+                __half2 q = __floats2half2_rn(a, b);
+                w[h] = *(uint32_t*)&q;
+            } else {
+                __nv_bfloat162 q = __floats2bfloat162_rn(a, b);
+                w[h] = *(uint32_t*)&q;
+            }
+        }
+        const int64_t idx = ((int64_t)l * p.Rout + rg) * p.Kld + seg * p.Kseg + col;
+        *(uint4*)((uint16_t*)p.dst + idx) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+}
+
+template <typename T>
+static void launch_pack_real(const PackParams& pp, int split, int fmt, cudaStream_t s)
+{
+    dim3 grid((unsigned)((pp.R + FR - 1) / FR), (unsigned)((pp.Kseg + FK - 1) / FK), (unsigned)pp.Lsz);
+    if (split == 3) k_pack_real<T, 3, 0><<<grid, 256, 0, s>>>(pp);
+    else if (fmt == 1) k_pack_real<T, 1, 1><<<grid, 256, 0, s>>>(pp);
+    else k_pack_real<T, 1, 0><<<grid, 256, 0, s>>>(pp);
+}
+
+// ---------------------------------------------------------------------------
+// GEMM
+struct EpiParams {
+    const void* C;
+    void* D;
+    int32_t tC, tD, cplx, beta_zero, conjC, conjD, conjD_f32, round_C;
+    float alpha_re, alpha_im, beta_re, beta_im;
+    int64_t M, N, L;   // output sizes (N counts complex elements when cplx)
+    ModeList mm, nn, ll;  // s0 = stride in C, s1 = stride in D
+};
+
+struct GemmParams {
+    int32_t tiles_m, tiles_n, num_tiles, num_kb;
+    EpiParams e;
+    int* error;       // set to 1 when a wait times out
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ unsigned long long now_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Waits for the phase of `parity` to complete; gives up after WAIT_NS (or at
+// once when another role already gave up) and returns false.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag)
+{
+    if (mbar_try(bar, parity)) return true;
+    const unsigned long long t0 = now_ns();
+    for (uint32_t i = 1;; i++) {
+        if (mbar_try(bar, parity)) return true;
+        if ((i & 255) == 0) {
+            if (*abort_flag) return false;
+            if (now_ns() - t0 > WAIT_NS) {
+                *abort_flag = 1;
+                return false;
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* tm, uint64_t* bar, int c0, int c1, int c2)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
+        ::"r"(smem_u32(dst)), "l"(tm), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
+        : "memory");
+}
+
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+
+// K-major operand tile with 128-byte swizzle: rows of 64 16-bit elements,
+// 8-row groups 1024 bytes apart.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((addr & 0x3FFFF) >> 4);
+    d |= (uint64_t)1 << 16;             // leading byte offset 16 B (unused with 128B swizzle)
+    d |= (uint64_t)(1024 >> 4) << 32;   // stride byte offset between 8-row groups
+    d |= (uint64_t)1 << 46;             // descriptor version (sm100)
+    d |= (uint64_t)2 << 61;             // SWIZZLE_128B
+    return d;
+}
+
+__device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// read-only global load kept as its own instruction, so a run of them stays
+// in flight together before any result is used
+__device__ __forceinline__ float ld_nc_f32(const float* p)
+{
+    float v;
+    asm volatile("ld.global.nc.f32 %0, [%1];" : "=f"(v) : "l"(p));
+    return v;
+}
+
+__device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, %0;" ::"n"(EPI_THREADS) : "memory"); }
+
+// beta * op_C(C) for one output (0 when beta == 0)
+__device__ __forceinline__ void load_beta_c(const EpiParams& e, int64_t offC, float& br, float& bi)
+{
+    br = 0.f;
+    bi = 0.f;
+    if (e.beta_zero) return;
+    float cr, ci;
+    load_rounded<float>(e.C, offC, e.tC, e.round_C, cr, ci);
+    if (e.conjC) ci = -ci;
+    if (e.cplx) {
+        br = e.beta_re * cr - e.beta_im * ci;
+        bi = e.beta_re * ci + e.beta_im * cr;
+    } else {
+        br = e.beta_re * cr;
+    }
+}
+
+__device__ __forceinline__ void finish_out(const EpiParams& e, int64_t offD, float ar, float ai, float br, float bi)
+{
+    float accr, acci;
+    if (e.cplx) {
+        accr = e.alpha_re * ar - e.alpha_im * ai + br;
+        acci = e.alpha_re * ai + e.alpha_im * ar + bi;
+    } else {
+        accr = e.alpha_re * ar + br;
+        acci = 0.f;
+    }
+    if (e.conjD) acci = -acci;
+    store_elem<float>(e.D, offD, e.tD, accr, acci);
+}
+
+// EPI_F32: real product, C and D binary32 (the common case, specialised);
+// EPI_ANY: every storage type, complex outputs, op_C / op_D.
+enum { EPI_ANY = 0, EPI_F32 = 1 };
+
+template <int EPI>
+__global__ void __launch_bounds__(NTHREADS, 1)
+    k_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, GemmParams p,
+           uint32_t idesc)
+{
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t* tiles = smem;
+    uint64_t* full = (uint64_t*)(smem + STAGES * STAGE_BYTES);
+    uint64_t* empty = full + STAGES;
+    uint64_t* tfull = empty + STAGES;
+    uint64_t* tempty = tfull + 2;
+    uint32_t* tmem_slot = (uint32_t*)(tempty + 2);
+    volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
+    volatile int* epi_ok = (volatile int*)(tmem_slot + 2);
+    int64_t* colC = (int64_t*)(smem + STAGES * STAGE_BYTES + 256);
+    int64_t* colD = colC + BN;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int a = 0; a < 2; a++) {
+            mbar_init(&tfull[a], 1);
+            mbar_init(&tempty[a], EPI_THREADS);
+        }
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 2) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+
+    const int my_tiles = p.num_tiles > (int)blockIdx.x ? (p.num_tiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+
+    if (warp == 0) {
+        // ---------------- TMA producer ----------------
+        if (lane == 0) {
+            uint32_t g = 0;
+            int64_t last_issued[STAGES];
+            for (int s = 0; s < STAGES; s++) last_issued[s] = -1;
+            bool ok = true;
+            for (int i = 0; i < my_tiles && ok; i++) {
+                const int tile = blockIdx.x + i * gridDim.x;
+                const int tm = tile % p.tiles_m;
+                const int rest = tile / p.tiles_m;
+                const int tn = rest % p.tiles_n;
+                const int l = rest / p.tiles_n;
+                for (int kb = 0; kb < p.num_kb; kb++, g++) {
+                    const int s = g % STAGES;
+                    const uint32_t ph = (g / STAGES) & 1;
+                    if (!mbar_wait(&empty[s], ph ^ 1, abort_flag)) { ok = false; break; }
+                    mbar_expect_tx(&full[s], STAGE_BYTES);
+                    uint8_t* a = tiles + s * STAGE_BYTES;
+                    tma_load_3d(a, &tmA, &full[s], kb * BK, tm * BM, l);
+                    tma_load_3d(a + A_BYTES, &tmB, &full[s], kb * BK, tn * BN, l);
+                    last_issued[s] = g;
+                }
+            }
+            // every issued load must land before the block exits: the phase of
+            // the last load issued on a stage stays complete once reached
+            int never = 0;
+            for (int s = 0; s < STAGES; s++)
+                if (last_issued[s] >= 0)
+                    mbar_wait(&full[s], (uint32_t)(last_issued[s] / STAGES) & 1, (volatile int*)&never);
+        }
+    } else if (warp == 1) {
+        // ---------------- MMA issuer ----------------
+        if (lane == 0) {
+            uint32_t g = 0;
+            bool ok = true;
+            for (int i = 0; i < my_tiles && ok; i++) {
+                const int acc = i & 1;
+                const uint32_t aph = (i >> 1) & 1;
+                if (!mbar_wait(&tempty[acc], aph ^ 1, abort_flag)) break;
+                fence_after();
+                const uint32_t d_tmem = tmem_base + acc * BN;
+                for (int kb = 0; kb < p.num_kb; kb++, g++) {
+                    const int s = g % STAGES;
+                    const uint32_t ph = (g / STAGES) & 1;
+                    if (!mbar_wait(&full[s], ph, abort_flag)) { ok = false; break; }
+                    fence_after();
+                    const uint32_t a = smem_u32(tiles + s * STAGE_BYTES);
+                    const uint32_t b = a + A_BYTES;
+#pragma unroll
+                    for (int k = 0; k < BK / 16; k++)
+                        mma_f16(d_tmem, smem_desc(a + k * 32), smem_desc(b + k * 32), idesc, (kb | k) != 0);
+                    mma_commit(&empty[s]);
+                }
+                if (ok) mma_commit(&tfull[acc]);
+            }
+            // wait for the last MMAs before the block can release TMEM
+            volatile int never = 0;
+            if (g > 0) {
+                const uint32_t last = g - 1;
+                mbar_wait(&empty[last % STAGES], (last / STAGES) & 1, &never);
+            }
+        }
+    } else if (warp >= 4) {
+        // ---------------- epilogue ----------------
+        // Warp w drains TMEM lanes 32*(w%4)..+31 (its lane quarter); the two
+        // warps of a quarter take alternate 32-column chunks. For each chunk
+        // the beta*C values are fetched first (independent loads in flight
+        // together), then the accumulators, then D is written.
+        const EpiParams& e = p.e;
+        const int q = warp & 3;
+        const int half = (warp - 4) >> 2;        // 0 or 1: which chunks
+        const int et = threadIdx.x - 128;        // 0 .. EPI_THREADS-1
+        const int cols_out = e.cplx ? BN / 2 : BN;
+        for (int i = 0; i < my_tiles; i++) {
+            const int tile = blockIdx.x + i * gridDim.x;
+            const int tm = tile % p.tiles_m;
+            const int rest = tile / p.tiles_m;
+            const int tn = rest % p.tiles_n;
+            const int l = rest / p.tiles_n;
+            for (int c = et; c < cols_out; c += EPI_THREADS) {
+                const int64_t n = (int64_t)tn * cols_out + c;
+                int64_t oc = 0, od = 0;
+                if (n < e.N) decode2(e.nn, n, oc, od);
+                colC[c] = oc;
+                colD[c] = od;
+            }
+            int64_t lC, lD;
+            decode2(e.ll, l, lC, lD);
+            const int64_t m = (int64_t)tm * BM + q * 32 + lane;
+            const bool mok = m < e.M;
+            int64_t rC = 0, rD = 0;
+            if (mok) decode2(e.mm, m, rC, rD);
+            rC += lC;
+            rD += lD;
+            const int acc = i & 1;
+            const uint32_t aph = (i >> 1) & 1;
+            if (EPI == EPI_F32) {
+                // C does not depend on the accumulators: fetch the first chunk
+                // while the MMAs of this tile may still run
+                epi_bar();  // column offsets of this tile are visible
+                float cur[32], nxt[32];
+                const float* Cb = (const float*)e.C + rC;
+                auto fetch = [&](int ch, float (&dst)[32]) {
+#pragma unroll
+                    for (int j = 0; j < 32; j++) {
+                        const int c = ch * 32 + j;
+                        dst[j] = (!e.beta_zero && mok && (int64_t)tn * BN + c < e.N) ? ld_nc_f32(Cb + colC[c]) : 0.f;
+                    }
+                };
+                fetch(half, cur);
+                if (et == 0) *epi_ok = mbar_wait(&tfull[acc], aph, abort_flag) ? 1 : 0;
+                epi_bar();
+                const bool ok = *epi_ok != 0;
+                fence_after();
+                if (ok) {
+#pragma unroll
+                    for (int t = 0; t < BN / 64; t++) {
+                        const int ch = half + 2 * t;
+                        if (t + 1 < BN / 64) fetch(ch + 2, nxt);
+                        uint32_t r[32];
+                        tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + acc * BN + ch * 32, r);
+#pragma unroll
+                        for (int j = 0; j < 32; j++) {
+                            const int c = ch * 32 + j;
+                            if (mok && (int64_t)tn * BN + c < e.N)
+                                ((float*)e.D)[rD + colD[c]] =
+                                    fmaf(e.alpha_re, __uint_as_float(r[j]), e.beta_re * round_in<float>(cur[j], e.round_C));
+                        }
+#pragma unroll
+                        for (int j = 0; j < 32; j++) cur[j] = nxt[j];
+                    }
+                }
+                fence_before();
+                mbar_arrive(&tempty[acc]);
+                epi_bar();  // offsets and *epi_ok may be rewritten after this point
+                if (!ok) break;
+                continue;
+            }
+            if (et == 0) *epi_ok = mbar_wait(&tfull[acc], aph, abort_flag) ? 1 : 0;
+            epi_bar();  // column offsets and the wait's outcome are visible to every epilogue thread
+            const bool ok = *epi_ok != 0;
+            fence_after();
+            if (ok) {
+                for (int ch = half; ch < BN / 32; ch += 2) {
+                    const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + acc * BN + ch * 32;
+                    if (!e.cplx) {
+                        float br[32], bi[32];
+#pragma unroll
+                        for (int j = 0; j < 32; j++) {
+                            const int c = ch * 32 + j;
+                            br[j] = bi[j] = 0.f;
+                            if (mok && (int64_t)tn * BN + c < e.N) load_beta_c(e, rC + colC[c], br[j], bi[j]);
+                        }
+                        uint32_t r[32];
+                        tmem_ld32(taddr, r);
+#pragma unroll
+                        for (int j = 0; j < 32; j++) {
+                            const int c = ch * 32 + j;
+                            if (mok && (int64_t)tn * BN + c < e.N)
+                                finish_out(e, rD + colD[c], __uint_as_float(r[j]), 0.f, br[j], bi[j]);
+                        }
+                    } else {
+                        float br[16], bi[16];
+#pragma unroll
+                        for (int j = 0; j < 16; j++) {
+                            const int c = ch * 16 + j;
+                            br[j] = bi[j] = 0.f;
+                            if (mok && (int64_t)tn * cols_out + c < e.N) load_beta_c(e, rC + colC[c], br[j], bi[j]);
+                        }
+                        uint32_t r[32];
+                        tmem_ld32(taddr, r);
+#pragma unroll
+                        for (int j = 0; j < 16; j++) {
+                            const int c = ch * 16 + j;
+                            if (mok && (int64_t)tn * cols_out + c < e.N)
+                                finish_out(e, rD + colD[c], __uint_as_float(r[2 * j]), __uint_as_float(r[2 * j + 1]),
+                                           br[j], bi[j]);
+                        }
+                    }
+                }
+            }
+            fence_before();
+            mbar_arrive(&tempty[acc]);
+            epi_bar();  // offsets and *epi_ok may be rewritten after this point
+            if (!ok) break;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && *abort_flag) atomicExch(p.error, 1);
+    if (warp == 2) {
+        fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn()
+{
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    });
+    return fn;
+}
+
+static bool make_map(CUtensorMap* tm, void* base, int fmt, uint64_t kld, uint64_t rows, uint64_t L, uint32_t box_rows)
+{
+    EncodeTiledFn enc = encode_fn();
+    if (!enc) return false;
+    cuuint64_t dims[3] = {kld, rows, L};
+    cuuint64_t strides[2] = {kld * 2, kld * rows * 2};
+    cuuint32_t box[3] = {(cuuint32_t)BK, box_rows, 1};
+    cuuint32_t es[3] = {1, 1, 1};
+    CUresult r = enc(tm, fmt == 1 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, base, dims,
+                     strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+static void fill_modes(ModeList& m, const tb_modes& src, int which0, int which1)
+{
+    memset(&m, 0, sizeof(m));
+    m.n = src.n;
+    for (int j = 0; j < src.n; j++) {
+        m.ext[j] = src.ext[j];
+        const int64_t* s[4] = {src.sA, src.sB, src.sC, src.sD};
+        m.s0[j] = which0 >= 0 ? s[which0][j] : 0;
+        m.s1[j] = which1 >= 0 ? s[which1][j] : 0;
+    }
+}
+
+static int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+static int num_sms()
+{
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    }
+    return n;
+}
+
+// smallest |stride| among a mode list's modes (for the load order of the pack)
+static int64_t min_stride(const tb_modes& m, int which)
+{
+    const int64_t* s = which == 0 ? m.sA : m.sB;
+    int64_t best = INT64_MAX;
+    for (int j = 0; j < m.n; j++) {
+        int64_t v = s[j] < 0 ? -s[j] : s[j];
+        if (v != 0 && v < best) best = v;
+    }
+    return best;
+}
+
+struct Workspace {
+    void* buf = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace tc
+
+cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t s, int* kernels, void** main_timer)
+{
+    using namespace tc;
+    *kernels = 0;
+    const int cplx = P->compute == TB_C32;
+    const int split = P->tc_mode == TB_TC_SPLIT_BF16 ? 3 : 1;
+    const int fmt = P->tc_mode == TB_TC_F16 ? 1 : 0;
+    const int64_t M = P->M.size, N = P->N.size, Lsz = P->L.size, K = P->K.size;
+    const int64_t Kreal = K * (cplx ? 2 : 1);
+    const int64_t Kseg = round_up(Kreal, 8);
+    const int64_t Kld = Kseg * split;
+    const int64_t Nout = N * (cplx ? 2 : 1);
+    const size_t bytesA = (size_t)Lsz * M * Kld * 2, bytesB = (size_t)Lsz * Nout * Kld * 2;
+    const size_t scratch = round_up(bytesA, 256) + round_up(bytesB, 256);
+
+    void* ws = nullptr;
+    cudaError_t e = pool_alloc(&ws, scratch, s);  // reused by every group: same stream, in order
+    if (e != cudaSuccess) return e;
+    int* flag = device_error_word();
+    if (!flag) {
+        cudaFreeAsync(ws, s);
+        return cudaErrorMemoryAllocation;
+    }
+    for (int b = 0; b < num; b++) {
+        char* base = (char*)ws;
+        void* pA = base;
+        void* pB = base + round_up(bytesA, 256);
+
+        // pack A and B
+        for (int side = 0; side < 2; side++) {
+            PackParams pp;
+            memset(&pp, 0, sizeof(pp));
+            pp.src = side == 0 ? d[b].A : d[b].B;
+            pp.dst = side == 0 ? pA : pB;
+            pp.type = side == 0 ? P->tA : P->tB;
+            pp.conj = side == 0 ? P->conjA : P->conjB;
+            pp.round_mode = split == 3 ? TB_ROUND_NONE : P->round_in;
+            pp.cplx = cplx;
+            pp.is_B = side;
+            pp.split = split;
+            pp.fmt = fmt;
+            pp.R = side == 0 ? M : N;
+            pp.K = K;
+            pp.Lsz = Lsz;
+            pp.Kseg = Kseg;
+            pp.Kld = Kld;
+            pp.Rout = side == 0 ? M : Nout;
+            const int which = side;  // stride of A or of B
+            fill_modes(pp.rows, side == 0 ? P->M : P->N, which, -1);
+            fill_modes(pp.ks, P->K, which, -1);
+            fill_modes(pp.ls, P->L, which, -1);
+            fill_modes(pp.us, side == 0 ? P->UA : P->UB, which, -1);
+            pp.usize = side == 0 ? P->UA.size : P->UB.size;
+            pp.rows_fast = min_stride(side == 0 ? P->M : P->N, which) < min_stride(P->K, which);
+            if (!cplx && pp.us.n == 0 && (pp.type == T_F32 || pp.type == T_F64 || pp.type == T_F16 ||
+                                           pp.type == T_BF16)) {
+                switch (pp.type) {
+                case T_F32: launch_pack_real<float>(pp, split, fmt, s); break;
+                case T_F64: launch_pack_real<double>(pp, split, fmt, s); break;
+                case T_F16: launch_pack_real<__half>(pp, split, fmt, s); break;
+                default: launch_pack_real<__nv_bfloat16>(pp, split, fmt, s); break;
+                }
+            } else {
+                dim3 grid((unsigned)((pp.R + PR - 1) / PR), (unsigned)((Kseg / (cplx ? 2 : 1) + PK - 1) / PK),
+                          (unsigned)Lsz);
+                k_pack<<<grid, 256, 0, s>>>(pp);
+            }
+            count_launch();
+            (*kernels)++;
+        }
+        e = cudaGetLastError();
+        if (e != cudaSuccess) break;
+
+        CUtensorMap tmA, tmB;
+        if (!make_map(&tmA, pA, fmt, Kld, M, Lsz, BM) || !make_map(&tmB, pB, fmt, Kld, Nout, Lsz, BN)) {
+            e = cudaErrorInvalidValue;
+            break;
+        }
+        GemmParams gp;
+        memset(&gp, 0, sizeof(gp));
+        gp.tiles_m = (int)((M + BM - 1) / BM);
+        gp.tiles_n = (int)((Nout + BN - 1) / BN);
+        gp.num_tiles = gp.tiles_m * gp.tiles_n * (int)Lsz;
+        gp.num_kb = (int)((Kld + BK - 1) / BK);
+        gp.error = flag;
+        EpiParams& ep = gp.e;
+        ep.C = d[b].C;
+        ep.D = d[b].D;
+        ep.tC = P->tC;
+        ep.tD = P->tD;
+        ep.cplx = cplx;
+        ep.beta_zero = P->beta_zero;
+        ep.conjC = P->conjC;
+        ep.conjD = P->conjD;
+        ep.conjD_f32 = P->conjD_round_f32;
+        ep.round_C = P->round_in;
+        ep.alpha_re = (float)P->alpha_re;
+        ep.alpha_im = (float)P->alpha_im;
+        ep.beta_re = (float)P->beta_re;
+        ep.beta_im = (float)P->beta_im;
+        ep.M = M;
+        ep.N = N;
+        ep.L = Lsz;
+        fill_modes(ep.mm, P->M, 2, 3);
+        fill_modes(ep.nn, P->N, 2, 3);
+        fill_modes(ep.ll, P->L, 2, 3);
+        const uint32_t ab = fmt == 1 ? 0u : 1u;  // operand format: 0 f16, 1 bf16
+        const uint32_t idesc = (1u << 4) | (ab << 7) | (ab << 10) | ((uint32_t)(BN >> 3) << 17) |
+                               ((uint32_t)(BM >> 4) << 24);
+        const bool f32_epi = !cplx && P->tD == T_F32 && (P->beta_zero || P->tC == T_F32) && !P->conjD;
+        auto kern = f32_epi ? k_gemm<EPI_F32> : k_gemm<EPI_ANY>;
+        static int attr_done[64][2];
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (dev < 64 && !attr_done[dev][f32_epi]) {
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+            attr_done[dev][f32_epi] = 1;
+        }
+        const int grid = gp.num_tiles < num_sms() ? gp.num_tiles : num_sms();
+        if (main_timer && b == 0) tbk_timer_begin(s, main_timer);
+        kern<<<grid, NTHREADS, SMEM_BYTES, s>>>(tmA, tmB, gp, idesc);
+        if (main_timer && b == 0) tbk_timer_end(s, *main_timer);
+        count_launch();
+        (*kernels)++;
+        e = cudaGetLastError();
+        if (e != cudaSuccess) break;
+    }
+    cudaFreeAsync(ws, s);
+    return e;
+}
+
 }  // namespace tb

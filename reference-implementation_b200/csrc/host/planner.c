@@ -337,11 +337,17 @@ int tb_build_plan(const tb_tensor_view* A, const tb_tensor_view* B,
         path = TB_PATH_REDUCE;
 
     int tc_ok = 0;
-    if (P->compute == TB_R32 && ksz > 0) {
+    if ((P->compute == TB_R32 || P->compute == TB_C32) && ksz > 0) {
         if (prec == TAPP_BF16BF16_ACCUM_F32) { tc_ok = 1; P->tc_mode = TB_TC_BF16; }
         else if (prec == TAPP_F16F16_ACCUM_F32 || prec == TAPP_F16F16_ACCUM_F16) { tc_ok = 1; P->tc_mode = TB_TC_F16; }
         else if (opt && opt->f32_mode == 1) { tc_ok = 1; P->tc_mode = TB_TC_SPLIT_BF16; }
     }
+    /* launch limits of the pack grid (z = batch, y = contraction tiles) and the tile count */
+    const int64_t kcols = ksz * (P->compute == TB_C32 ? 2 : 1);
+    if (P->L.size > 65535 || (kcols + 31) / 32 > 65535 ||
+        (double)((P->M.size + 127) / 128) * (double)((P->N.size * 2 + 255) / 256) * (double)P->L.size > 1e9 ||
+        P->UA.n > TB_MAXMODES || P->UB.n > TB_MAXMODES)
+        tc_ok = 0;
     const int big = P->M.size >= 64 && P->N.size >= 64 && ksz >= 64 && macs >= 16.0 * 1024 * 1024;
     if (tc_ok && big) path = TB_PATH_TC;
     if (opt && opt->force_path) {

@@ -272,7 +272,7 @@ static int run(struct tb_product* p, TAPP_executor exec, TAPP_status* status, co
     if (err) return err;
 
     int kernels = 0;
-    double dev_us = 0.0;
+    double dev_us = 0.0, main_us = 0.0;
     if (P.path != TB_PATH_NOOP) {
         const void* ptr[4] = {A, B, C, D};
         staging st;
@@ -280,9 +280,11 @@ static int run(struct tb_product* p, TAPP_executor exec, TAPP_status* status, co
         int device = -1;
         err = stage_in(&P, v, ptr, &st, &dp, s.stream, &device);
         void* timer = NULL;
-        if (!err && s.want_status && !s.async) tbk_timer_begin(s.stream, &timer);
+        void* main_timer = NULL;
+        const int timed = !err && s.want_status && !s.async;
+        if (timed) tbk_timer_begin(s.stream, &timer);
         if (!err) {
-            int e = tbk_run_plan(&P, &dp, s.stream, &kernels);
+            int e = tbk_run_plan(&P, &dp, s.stream, &kernels, timed ? &main_timer : NULL);
             if (e) err = cuda_err(e);
         }
         if (timer) tbk_timer_end(s.stream, timer);
@@ -291,8 +293,10 @@ static int run(struct tb_product* p, TAPP_executor exec, TAPP_status* status, co
         if (!s.async || st.staged_any) {
             int e = tbk_stream_sync(s.stream);
             if (!err && e) err = cuda_err(e);
+            if (!err && P.path == TB_PATH_TC && (e = tbk_check_device_error())) err = cuda_err(e);
         }
         if (timer) tbk_timer_elapsed_us(timer, &dev_us);
+        if (main_timer) tbk_timer_elapsed_us(main_timer, &main_us);
     }
     if (s.want_status && status) {
         struct tb_status* so = calloc(1, sizeof(*so));
@@ -303,6 +307,7 @@ static int run(struct tb_product* p, TAPP_executor exec, TAPP_status* status, co
             so->tc_mode = P.tc_mode;
             so->flops = tb_plan_flops(&P);
             so->device_us = dev_us;
+            so->main_us = main_us;
             *status = (TAPP_status)so;
         }
     }
@@ -374,6 +379,7 @@ TAPP_error TAPP_execute_batched_product(TAPP_tensor_product plan, TAPP_executor 
         if (!s.async) {
             e = tbk_stream_sync(s.stream);
             if (e) return cuda_err(e);
+            if (P.path == TB_PATH_TC && (e = tbk_check_device_error())) return cuda_err(e);
         }
         if (s.want_status && status) {
             struct tb_status* so = calloc(1, sizeof(*so));

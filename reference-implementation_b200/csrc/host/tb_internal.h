@@ -50,6 +50,7 @@ struct tb_status {
     int tc_mode;
     double flops;
     double device_us;
+    double main_us;
 };
 
 /* cached launch plan of a product, keyed on the infos' contents */

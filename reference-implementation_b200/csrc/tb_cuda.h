@@ -35,14 +35,19 @@ int tbk_timer_end(void* stream, void* timer);
 int tbk_timer_elapsed_us(void* timer, double* us);   /* frees the timer */
 
 /* Runs the plan on device-accessible operands. kernels receives the number
- * of kernels launched. */
-int tbk_run_plan(const tb_plan* plan, const tb_ptrs* ptrs, void* stream, int* kernels);
+ * of kernels launched. When main_timer is not NULL, a timer (see
+ * tbk_timer_*) around the dominant kernel is returned through it. */
+int tbk_run_plan(const tb_plan* plan, const tb_ptrs* ptrs, void* stream, int* kernels, void** main_timer);
 
 /* Runs the plan on num independent operand sets in one grouped launch
  * where the path allows it. */
 int tbk_run_plan_batched(const tb_plan* plan, const tb_ptrs* ptrs, int num, void* stream, int* kernels);
 
 long long tbk_launch_count(void);
+
+/* Reads (and clears) the word kernels set when one of their bounded waits
+ * expired; returns 0 or a cudaError_t value. Synchronises the device. */
+int tbk_check_device_error(void);
 const char* tbk_error_string(int err);
 
 #ifdef __cplusplus

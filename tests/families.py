@@ -60,7 +60,7 @@ def random_case(rng: np.random.Generator, *, dtype=None, types=None, prec=-1,
                 n_isoA=0, n_isoB=0, n_repA=0, n_repB=0, n_repD=0,
                 min_ext=1, max_ext=4, ext_choices=None,
                 subtensor=False, neg=False, mixed=False, zero_stride=None,
-                ops=None, C_null=False, beta_zero=False, name="") -> Case:
+                ops=None, C_null=False, beta_zero=False, name="", max_work=None) -> Case:
     if types is None:
         if dtype is None:
             dtype = int(rng.choice(ALL_TYPES))
@@ -81,8 +81,14 @@ def random_case(rng: np.random.Generator, *, dtype=None, types=None, prec=-1,
     UA = [next(it) for _ in range(n_isoA)]
     UB = [next(it) for _ in range(n_isoB)]
     ext = {}
-    for l in labs:
-        ext[l] = int(rng.choice(ext_choices)) if ext_choices is not None else r(min_ext, max_ext)
+    for attempt in range(1000):
+        for l in labs:
+            ext[l] = int(rng.choice(ext_choices)) if ext_choices is not None else r(min_ext, max_ext)
+        work = float(np.prod([ext[l] for l in labs], dtype=np.float64))
+        if max_work is None or work <= max_work:
+            break
+    else:
+        raise RuntimeError("no extents under the work bound")
 
     def shuffled(x):
         x = list(x)
@@ -159,3 +165,10 @@ def family_cases(seed: int, count_per_family: int = 4, dtypes=ALL_TYPES, max_ext
             kw2 = dict(kw)
             kw2.setdefault("max_ext", max_ext)
             yield name, random_case(rng, dtype=dt, name=f"{name}-{i}", **kw2)
+
+
+def bounded_case(rng, max_work=3e6, **kw):
+    """random_case with extents redrawn until the product of all label
+    extents (|D| * |K| * |UA| * |UB|, the oracle's work) stays below
+    max_work, so that the binary64 oracle finishes in well under a second."""
+    return random_case(rng, max_work=max_work, **kw)
