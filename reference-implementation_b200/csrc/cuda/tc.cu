@@ -42,7 +42,12 @@ constexpr int TMEM_COLS = 512;
 constexpr int EPI_WARPS = 8;                    // two warps per TMEM lane quarter
 constexpr int EPI_THREADS = EPI_WARPS * 32;
 constexpr int NTHREADS = 128 + EPI_THREADS;
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/ + 2 * BN * 8 /*column offsets*/;
+constexpr int STAGE_EPI_BYTES = 32 * 32 * 4;  // one 32x32 fp32 box per epilogue warp
+// tiles | barriers | epilogue staging (the per-thread epilogue keeps its
+// column-offset tables in the staging area instead)
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/ + 8 * STAGE_EPI_BYTES;
+static_assert(2 * BN * 8 <= 8 * STAGE_EPI_BYTES, "column tables fit in the staging area");
+static_assert(SMEM_BYTES <= 232448, "dynamic shared memory limit of sm_100");
 constexpr unsigned long long WAIT_NS = 4000000000ull;  // 4 s per wait
 
 struct ModeList {
@@ -218,8 +223,12 @@ __device__ __forceinline__ float load_as_float<__nv_bfloat16>(const void* base, 
     return __bfloat162float(((const __nv_bfloat16*)base)[off]);
 }
 
-template <typename T, int SPLIT, int FMT>
-__global__ void __launch_bounds__(256) k_pack_real(PackParams p)
+// ROWS_FAST: the source is contiguous along the first row (M or N) mode, else
+// along the first contracted mode. VEC = 4: that mode has stride 1, an extent
+// divisible by 4 and every other stride (and the base) keeps 16-byte
+// alignment, so four neighbours come in one 16-byte load.
+template <typename T, int SPLIT, int FMT, bool ROWS_FAST, int VEC>
+__global__ void __launch_bounds__(256, 4) k_pack_real(PackParams p)
 {
     __shared__ float v[FR][FK + 1];
     __shared__ int64_t rowOff[FR];
@@ -241,22 +250,37 @@ __global__ void __launch_bounds__(256) k_pack_real(PackParams p)
         lOff = o;
     }
     __syncthreads();
-    float x[FR * FK / 256];
+    constexpr int NV = FR * FK / 256 / VEC;  // vector loads per thread
+    constexpr int G = (ROWS_FAST ? FR : FK) / VEC;  // vectors along the fast direction
+    float x[NV][VEC];
 #pragma unroll
-    for (int u = 0; u < FR * FK / 256; u++) {
+    for (int u = 0; u < NV; u++) {
         const int e = t + 256 * u;
-        const int r = p.rows_fast ? (e % FR) : (e / FK);
-        const int kk = p.rows_fast ? (e / FR) : (e % FK);
-        x[u] = (r0 + r < p.R && k0 + kk < p.K) ? load_as_float<T>(p.src, lOff + rowOff[r] + kOff[kk]) : 0.f;
+        const int fg = e % G, sl = e / G;              // fast-direction group, slow index
+        const int r = ROWS_FAST ? fg * VEC : sl;
+        const int kk = ROWS_FAST ? sl : fg * VEC;
+        const bool in = (r0 + r < p.R) && (k0 + kk < p.K);
+        const int64_t off = lOff + rowOff[r] + kOff[kk];
+        if (VEC == 4) {
+            float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (in) q = __ldg((const float4*)((const float*)p.src + off));
+            x[u][0] = q.x; x[u][VEC > 1 ? 1 : 0] = q.y; x[u][VEC > 2 ? 2 : 0] = q.z; x[u][VEC > 3 ? 3 : 0] = q.w;
+        } else {
+            x[u][0] = in ? load_as_float<T>(p.src, off) : 0.f;
+        }
     }
 #pragma unroll
-    for (int u = 0; u < FR * FK / 256; u++) {
+    for (int u = 0; u < NV; u++) {
         const int e = t + 256 * u;
-        const int r = p.rows_fast ? (e % FR) : (e / FK);
-        const int kk = p.rows_fast ? (e / FR) : (e % FK);
-        float y = x[u];
-        if (SPLIT == 1 && p.round_mode != TB_ROUND_NONE) y = round_in<float>(y, p.round_mode);
-        v[r][kk] = y;
+        const int fg = e % G, sl = e / G;
+#pragma unroll
+        for (int h = 0; h < VEC; h++) {
+            const int r = ROWS_FAST ? fg * VEC + h : sl;
+            const int kk = ROWS_FAST ? sl : fg * VEC + h;
+            float y = x[u][h];
+            if (SPLIT == 1 && p.round_mode != TB_ROUND_NONE) y = round_in<float>(y, p.round_mode);
+            v[r][kk] = y;
+        }
     }
     __syncthreads();
     // FR rows x FK/8 groups of eight per segment
@@ -290,13 +314,44 @@ __global__ void __launch_bounds__(256) k_pack_real(PackParams p)
     }
 }
 
+template <typename T, bool RF, int VEC>
+static void launch_pack_real3(const PackParams& pp, int split, int fmt, dim3 grid, cudaStream_t s)
+{
+    if (split == 3) k_pack_real<T, 3, 0, RF, VEC><<<grid, 256, 0, s>>>(pp);
+    else if (fmt == 1) k_pack_real<T, 1, 1, RF, VEC><<<grid, 256, 0, s>>>(pp);
+    else k_pack_real<T, 1, 0, RF, VEC><<<grid, 256, 0, s>>>(pp);
+}
+
+// whether a mode list's first mode has stride 1 and extent % 4 == 0 and all
+// other strides of `others` keep 4-element alignment
+static bool vec4_ok(const ModeList& fast, const ModeList* others[], int nothers, const void* base)
+{
+    if (fast.n < 1 || fast.s0[0] != 1 || fast.ext[0] % 4 != 0 || ((uintptr_t)base & 15) != 0) return false;
+    for (int j = 1; j < fast.n; j++)
+        if (fast.s0[j] % 4 != 0) return false;
+    for (int i = 0; i < nothers; i++)
+        for (int j = 0; j < others[i]->n; j++)
+            if (others[i]->s0[j] % 4 != 0) return false;
+    return true;
+}
+
 template <typename T>
 static void launch_pack_real(const PackParams& pp, int split, int fmt, cudaStream_t s)
 {
     dim3 grid((unsigned)((pp.R + FR - 1) / FR), (unsigned)((pp.Kseg + FK - 1) / FK), (unsigned)pp.Lsz);
-    if (split == 3) k_pack_real<T, 3, 0><<<grid, 256, 0, s>>>(pp);
-    else if (fmt == 1) k_pack_real<T, 1, 1><<<grid, 256, 0, s>>>(pp);
-    else k_pack_real<T, 1, 0><<<grid, 256, 0, s>>>(pp);
+    const bool rf = pp.rows_fast != 0;
+    bool v4 = false;
+    if (sizeof(T) == 4) {
+        const ModeList* others[3] = {rf ? &pp.ks : &pp.rows, &pp.ls, &pp.us};
+        v4 = vec4_ok(rf ? pp.rows : pp.ks, others, 2, pp.src);
+    }
+    if (rf) {
+        if (v4) launch_pack_real3<T, true, 4>(pp, split, fmt, grid, s);
+        else launch_pack_real3<T, true, 1>(pp, split, fmt, grid, s);
+    } else {
+        if (v4) launch_pack_real3<T, false, 4>(pp, split, fmt, grid, s);
+        else launch_pack_real3<T, false, 1>(pp, split, fmt, grid, s);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -315,6 +370,14 @@ struct GemmParams {
     EpiParams e;
     int* error;       // set to 1 when a wait times out
 };
+
+// TMA epilogue: C and D as (up to) 5-d tensor maps whose dims are
+// [first M mode, first N mode, further M modes, further N modes, L modes];
+// every warp moves 32 x 32 boxes (32 consecutive rows of the first M mode,
+// 32 consecutive columns of the first N mode).
+struct TmaEpi {
+    int32_t rank;
+}; 
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -377,6 +440,21 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* tm, ui
         "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
         ::"r"(smem_u32(dst)), "l"(tm), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
         : "memory");
+}
+
+__device__ __forceinline__ void tma_load_5d(void* dst, const CUtensorMap* tm, uint64_t* bar, const int (&c)[5])
+{
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6, %7}], [%2];"
+        ::"r"(smem_u32(dst)), "l"(tm), "r"(smem_u32(bar)), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(c[4])
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_store_5d(const CUtensorMap* tm, const void* src, const int (&c)[5])
+{
+    asm volatile("cp.async.bulk.tensor.5d.global.shared::cta.bulk_group [%0, {%2, %3, %4, %5, %6}], [%1];"
+                 ::"l"(tm), "r"(smem_u32(src)), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(c[4])
+                 : "memory");
 }
 
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -469,12 +547,14 @@ __device__ __forceinline__ void finish_out(const EpiParams& e, int64_t offD, flo
 
 // EPI_F32: real product, C and D binary32 (the common case, specialised);
 // EPI_ANY: every storage type, complex outputs, op_C / op_D.
-enum { EPI_ANY = 0, EPI_F32 = 1 };
+// EPI_TMA: like EPI_F32, with C and D moved by TMA tensor copies through a
+// per-warp shared-memory box (C and D expressible as tensor maps).
+enum { EPI_ANY = 0, EPI_F32 = 1, EPI_TMA = 2 };
 
 template <int EPI>
 __global__ void __launch_bounds__(NTHREADS, 1)
     k_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, GemmParams p,
-           uint32_t idesc)
+           uint32_t idesc, const __grid_constant__ CUtensorMap tmC, const __grid_constant__ CUtensorMap tmD)
 {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -486,7 +566,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     uint32_t* tmem_slot = (uint32_t*)(tempty + 2);
     volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
     volatile int* epi_ok = (volatile int*)(tmem_slot + 2);
-    int64_t* colC = (int64_t*)(smem + STAGES * STAGE_BYTES + 256);
+    uint64_t* cbar = (uint64_t*)(smem + STAGES * STAGE_BYTES + 128);  // one per epilogue warp
+    uint8_t* staging = smem + STAGES * STAGE_BYTES + 256;
+    int64_t* colC = (int64_t*)staging;
     int64_t* colD = colC + BN;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -499,6 +581,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             mbar_init(&tfull[a], 1);
             mbar_init(&tempty[a], EPI_THREADS);
         }
+        for (int w = 0; w < EPI_WARPS; w++) mbar_init(&cbar[w], 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -588,13 +671,16 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         const int half = (warp - 4) >> 2;        // 0 or 1: which chunks
         const int et = threadIdx.x - 128;        // 0 .. EPI_THREADS-1
         const int cols_out = e.cplx ? BN / 2 : BN;
+        uint32_t epi_cphase = 0;  // completed phases of this warp's C-box barrier
         for (int i = 0; i < my_tiles; i++) {
             const int tile = blockIdx.x + i * gridDim.x;
             const int tm = tile % p.tiles_m;
             const int rest = tile / p.tiles_m;
             const int tn = rest % p.tiles_n;
             const int l = rest / p.tiles_n;
-            for (int c = et; c < cols_out; c += EPI_THREADS) {
+            // column offsets of this tile (the TMA epilogue needs none: its
+            // staging boxes share this memory)
+            for (int c = et; EPI != EPI_TMA && c < cols_out; c += EPI_THREADS) {
                 const int64_t n = (int64_t)tn * cols_out + c;
                 int64_t oc = 0, od = 0;
                 if (n < e.N) decode2(e.nn, n, oc, od);
@@ -611,11 +697,104 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             rD += lD;
             const int acc = i & 1;
             const uint32_t aph = (i >> 1) & 1;
+            if (EPI == EPI_TMA) {
+                // Per chunk: TMA-load the 32x32 box of C into this warp's
+                // staging box, combine with the accumulators, write D into the
+                // same box and TMA-store it. The first box of C is requested
+                // before the accumulators are ready.
+                const int ew = warp - 4;
+                float* box = (float*)(staging + ew * STAGE_EPI_BYTES);
+                int mc[5];  // tensor-map coordinates of this warp's rows
+                {
+                    // the last mode keeps the whole quotient: rows past M give a
+                    // coordinate past the tensor map, where TMA clips the box
+                    int64_t r = (int64_t)tm * BM + q * 32;
+                    for (int j = 0; j < e.mm.n; j++) {
+                        const int64_t c = j + 1 < e.mm.n ? r % e.mm.ext[j] : r;
+                        r /= e.mm.ext[j];
+                        mc[j] = (int)c;
+                    }
+                }
+                int lc[5];
+                {
+                    int64_t r = l;
+                    for (int j = 0; j < e.ll.n; j++) {
+                        lc[j] = (int)(r % e.ll.ext[j]);
+                        r /= e.ll.ext[j];
+                    }
+                }
+                auto coords = [&](int ch, int (&cc)[5]) {
+                    int nc[5];
+                    int64_t r = (int64_t)tn * BN + ch * 32;
+                    for (int j = 0; j < e.nn.n; j++) {
+                        nc[j] = (int)(j + 1 < e.nn.n ? r % e.nn.ext[j] : r);
+                        r /= e.nn.ext[j];
+                    }
+                    int k = 0;
+                    cc[k++] = mc[0];
+                    cc[k++] = nc[0];
+                    for (int j = 1; j < e.mm.n; j++) cc[k++] = mc[j];
+                    for (int j = 1; j < e.nn.n; j++) cc[k++] = nc[j];
+                    for (int j = 0; j < e.ll.n; j++) cc[k++] = lc[j];
+                    while (k < 5) cc[k++] = 0;
+                };
+                const int nch = BN / 64;  // chunks per warp
+                bool ok = true;
+                auto issue_c = [&](int ch) {
+                    if (lane == 0 && !e.beta_zero) {
+                        int cc[5];
+                        coords(ch, cc);
+                        mbar_expect_tx(&cbar[ew], STAGE_EPI_BYTES);
+                        tma_load_5d(box, &tmC, &cbar[ew], cc);
+                    }
+                };
+                issue_c(half);
+                if (et == 0) *epi_ok = mbar_wait(&tfull[acc], aph, abort_flag) ? 1 : 0;
+                epi_bar();
+                ok = *epi_ok != 0;
+                fence_after();
+#pragma unroll 1
+                for (int t = 0; t < nch; t++) {
+                    const int ch = half + 2 * t;
+                    uint32_t r[32];
+                    if (ok) tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + acc * BN + ch * 32, r);
+                    bool cok = true;
+                    if (!e.beta_zero) {
+                        cok = mbar_wait(&cbar[ew], epi_cphase & 1, abort_flag);
+                        cok = __all_sync(0xffffffffu, cok);
+                        epi_cphase++;
+                    }
+                    if (ok && cok) {
+#pragma unroll
+                        for (int j = 0; j < 32; j++) {
+                            const float cv = e.beta_zero ? 0.f : e.beta_re * round_in<float>(box[j * 32 + lane], e.round_C);
+                            box[j * 32 + lane] = fmaf(e.alpha_re, __uint_as_float(r[j]), cv);
+                        }
+                        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    }
+                    __syncwarp();
+                    if (lane == 0 && ok && cok) {
+                        int cc[5];
+                        coords(ch, cc);
+                        tma_store_5d(&tmD, box, cc);
+                        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+                        // the box is reused by the next load: wait until the store has read it
+                        asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+                    }
+                    __syncwarp();
+                    if (!cok) ok = false;
+                    if (t + 1 < nch && ok) issue_c(ch + 2);
+                }
+                fence_before();
+                mbar_arrive(&tempty[acc]);
+                epi_bar();
+                continue;
+            }
             if (EPI == EPI_F32) {
                 // C does not depend on the accumulators: fetch the first chunk
                 // while the MMAs of this tile may still run
                 epi_bar();  // column offsets of this tile are visible
-                float cur[32], nxt[32];
+                float buf[2][32];  // ping-pong: chunk t uses buf[t & 1], chunk t+1 loads into the other
                 const float* Cb = (const float*)e.C + rC;
                 auto fetch = [&](int ch, float (&dst)[32]) {
 #pragma unroll
@@ -624,7 +803,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                         dst[j] = (!e.beta_zero && mok && (int64_t)tn * BN + c < e.N) ? ld_nc_f32(Cb + colC[c]) : 0.f;
                     }
                 };
-                fetch(half, cur);
+                fetch(half, buf[0]);
                 if (et == 0) *epi_ok = mbar_wait(&tfull[acc], aph, abort_flag) ? 1 : 0;
                 epi_bar();
                 const bool ok = *epi_ok != 0;
@@ -633,24 +812,21 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 #pragma unroll
                     for (int t = 0; t < BN / 64; t++) {
                         const int ch = half + 2 * t;
-                        if (t + 1 < BN / 64) fetch(ch + 2, nxt);
+                        if (t + 1 < BN / 64) fetch(ch + 2, buf[(t + 1) & 1]);
                         uint32_t r[32];
                         tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + acc * BN + ch * 32, r);
 #pragma unroll
                         for (int j = 0; j < 32; j++) {
                             const int c = ch * 32 + j;
                             if (mok && (int64_t)tn * BN + c < e.N)
-                                ((float*)e.D)[rD + colD[c]] =
-                                    fmaf(e.alpha_re, __uint_as_float(r[j]), e.beta_re * round_in<float>(cur[j], e.round_C));
+                                ((float*)e.D)[rD + colD[c]] = fmaf(e.alpha_re, __uint_as_float(r[j]),
+                                                                   e.beta_re * round_in<float>(buf[t & 1][j], e.round_C));
                         }
-#pragma unroll
-                        for (int j = 0; j < 32; j++) cur[j] = nxt[j];
                     }
                 }
                 fence_before();
                 mbar_arrive(&tempty[acc]);
                 epi_bar();  // offsets and *epi_ok may be rewritten after this point
-                if (!ok) break;
                 continue;
             }
             if (et == 0) *epi_ok = mbar_wait(&tfull[acc], aph, abort_flag) ? 1 : 0;
@@ -699,8 +875,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             fence_before();
             mbar_arrive(&tempty[acc]);
             epi_bar();  // offsets and *epi_ok may be rewritten after this point
-            if (!ok) break;
         }
+        // no early exit above: every epilogue thread takes every tile's barriers,
+        // and after an expired wait the remaining waits give up at once
+        if (EPI == EPI_TMA && lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
     }
     __syncthreads();
     if (threadIdx.x == 0 && *abort_flag) atomicExch(p.error, 1);
@@ -742,6 +920,49 @@ static bool make_map(CUtensorMap* tm, void* base, int fmt, uint64_t kld, uint64_
                      strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;
+}
+
+
+// Tensor map of C (which = 2) or D (which = 3) for the TMA epilogue, or false
+// when the layout does not allow it: binary32, the first M mode contiguous
+// (stride 1) with an extent that is a multiple of 32, the first N mode with an
+// extent that is a multiple of 32, every other stride positive and a multiple
+// of 16 bytes, at most 5 dimensions. Box: 32 x 32 x 1 x 1 x 1.
+static bool make_epi_map(CUtensorMap* tm, void* base, const tb_plan* P, int which)
+{
+    EncodeTiledFn enc = encode_fn();
+    if (!enc || !base) return false;
+    const tb_modes& M = P->M;
+    const tb_modes& N = P->N;
+    const tb_modes& L = P->L;
+    if (M.n < 1 || N.n < 1) return false;
+    const int rank = 2 + (M.n - 1) + (N.n - 1) + L.n;
+    if (rank > 5) return false;
+    auto st = [&](const tb_modes& m, int j) { return which == 2 ? m.sC[j] : m.sD[j]; };
+    if (st(M, 0) != 1 || M.ext[0] % 32 != 0 || N.ext[0] % 32 != 0) return false;
+    if (((uintptr_t)base & 15) != 0) return false;
+    cuuint64_t dims[5], strides[4];
+    int k = 0;
+    int64_t sd[5];
+    dims[k] = (cuuint64_t)M.ext[0]; sd[k++] = 1;
+    dims[k] = (cuuint64_t)N.ext[0]; sd[k++] = st(N, 0);
+    for (int j = 1; j < M.n; j++) { dims[k] = (cuuint64_t)M.ext[j]; sd[k++] = st(M, j); }
+    for (int j = 1; j < N.n; j++) { dims[k] = (cuuint64_t)N.ext[j]; sd[k++] = st(N, j); }
+    for (int j = 0; j < L.n; j++) { dims[k] = (cuuint64_t)L.ext[j]; sd[k++] = st(L, j); }
+    for (int j = 1; j < k; j++) {
+        if (sd[j] <= 0 || (sd[j] * 4) % 16 != 0 || sd[j] * 4 >= (1ll << 40)) return false;
+        strides[j - 1] = (cuuint64_t)(sd[j] * 4);
+    }
+    while (k < 5) {  // unit dimensions up to rank 5
+        dims[k] = 1;
+        strides[k - 1] = strides[k - 2];
+        k++;
+    }
+    cuuint32_t box[5] = {32, 32, 1, 1, 1};
+    cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    return enc(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 static void fill_modes(ModeList& m, const tb_modes& src, int which0, int which1)
@@ -899,17 +1120,21 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
         const uint32_t idesc = (1u << 4) | (ab << 7) | (ab << 10) | ((uint32_t)(BN >> 3) << 17) |
                                ((uint32_t)(BM >> 4) << 24);
         const bool f32_epi = !cplx && P->tD == T_F32 && (P->beta_zero || P->tC == T_F32) && !P->conjD;
-        auto kern = f32_epi ? k_gemm<EPI_F32> : k_gemm<EPI_ANY>;
-        static int attr_done[64][2];
+        CUtensorMap tmC = tmA, tmD = tmA;  // placeholders when the TMA epilogue is not used
+        const bool tma_epi = f32_epi && make_epi_map(&tmD, d[b].D, P, 3) &&
+                             (P->beta_zero || make_epi_map(&tmC, const_cast<void*>(d[b].C), P, 2));
+        const int kind = tma_epi ? EPI_TMA : (f32_epi ? EPI_F32 : EPI_ANY);
+        auto kern = kind == EPI_TMA ? k_gemm<EPI_TMA> : kind == EPI_F32 ? k_gemm<EPI_F32> : k_gemm<EPI_ANY>;
+        static int attr_done[64][3];
         int dev = 0;
         cudaGetDevice(&dev);
-        if (dev < 64 && !attr_done[dev][f32_epi]) {
+        if (dev < 64 && !attr_done[dev][kind]) {
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-            attr_done[dev][f32_epi] = 1;
+            attr_done[dev][kind] = 1;
         }
         const int grid = gp.num_tiles < num_sms() ? gp.num_tiles : num_sms();
         if (main_timer && b == 0) tbk_timer_begin(s, main_timer);
-        kern<<<grid, NTHREADS, SMEM_BYTES, s>>>(tmA, tmB, gp, idesc);
+        kern<<<grid, NTHREADS, SMEM_BYTES, s>>>(tmA, tmB, gp, idesc, tmC, tmD);
         if (main_timer && b == 0) tbk_timer_end(s, *main_timer);
         count_launch();
         (*kernels)++;

@@ -17,6 +17,7 @@
  * free modes are split into the batch/M/N view the GEMM kernels use.
  */
 #include <math.h>
+#include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -304,7 +305,20 @@ int tb_build_plan(const tb_tensor_view* A, const tb_tensor_view* B,
     P->skip_store = prec == TAPP_F16F16_ACCUM_F16 && tb_is_complex(D->type);
 
     simplify(&F, 3);
-    simplify(&K, 0);
+    /* Contracted modes are ordered by the strides of the operand that is
+     * contiguous along a contracted mode (K-major), so that the operand
+     * packing reads it along its fastest mode; an operand contiguous along a
+     * free mode is read along that mode whatever the contracted order. */
+    int64_t minKA = INT64_MAX, minKB = INT64_MAX, minFA = INT64_MAX;
+    for (int i = 0; i < K.n; i++) {
+        if (K.ext[i] == 1) continue;
+        if (K.s[0][i] && iabs64(K.s[0][i]) < minKA) minKA = iabs64(K.s[0][i]);
+        if (K.s[1][i] && iabs64(K.s[1][i]) < minKB) minKB = iabs64(K.s[1][i]);
+    }
+    for (int i = 0; i < F.n; i++)
+        if (F.s[0][i] && F.s[1][i] == 0 && iabs64(F.s[0][i]) < minFA) minFA = iabs64(F.s[0][i]);
+    const int A_kmajor = minKA < minFA;
+    simplify(&K, (!A_kmajor && minKB != INT64_MAX) ? 1 : 0);
     simplify(&UA, 0);
     simplify(&UB, 1);
     if ((err = to_modes(&F, &P->F)) || (err = to_modes(&K, &P->K)) ||

@@ -190,15 +190,16 @@ def test_planner_dense_contraction_modes(tapp):
     """All-16 dense contraction D[a,b,c,d] = sum_{e,f} A[a,e,b,f] B[f,c,e,d]:
     a,b are M (absent from B), c,d are N; no pair is contiguous in every
     tensor that holds it (e sits between a and b in A, and between c and d
-    in B), so nothing merges; K = (e, f) with strides (16, 4096) in A and
-    (256, 1) in B."""
+    in B), so nothing merges. A is contiguous along a free mode (a) and B
+    along a contracted one (f), so the contracted modes follow B's strides:
+    K = (f, e) with strides (4096, 16) in A and (1, 256) in B."""
     from tapp_b200.workloads import dense_contraction_case
     case = dense_contraction_case(np.random.default_rng(0), extent=16, dtype=0)
     plan, infos = _plan(tapp, case)
     d = tapp.describe(plan)
     assert " M=[(16:1,0,1,1),(16:256,0,16,16)]" in d, d
     assert " N=[(16:0,16,256,256),(16:0,4096,4096,4096)]" in d, d
-    assert " K=[(16:16,256,0,0),(16:4096,1,0,0)]" in d, d
+    assert " K=[(16:4096,1,0,0),(16:16,256,0,0)]" in d, d
     assert " L=[]" in d and " UA=[]" in d
 
 

@@ -117,3 +117,52 @@ def test_full_size_dense_sampled(tapp, oracle, gpu):
     n = 4096 + 8
     bound = (n * 2.0 ** -24) * scale + 2 * 2.0 ** -24 * np.abs(D64)
     assert (np.abs(got - D64) <= bound).all()
+
+
+def _matmul_case(rng, a, b, k, h, prec, beta=0.7, permute_C=False):
+    """D[a,b,h] = sum_k A[a,k,h] B[k,b,h] + beta C, dense column-major."""
+    from tapp_b200.case import alloc, fill_uniform, scalar, Case
+    L = {c: ord(c) for c in "abkh"}
+    def t(idx, ext, strides=None):
+        if strides is None:
+            strides, acc = [], 1
+            for e in ext:
+                strides.append(acc)
+                acc *= e
+        T = alloc(0, ext, strides, [L[c] for c in idx])
+        fill_uniform(T, rng)
+        return T
+    A = t("akh", [a, k, h])
+    B = t("kbh", [k, b, h])
+    D = t("abh", [a, b, h])
+    Cc = t("abh", [a, b, h], [h * b, h, 1] if permute_C else None)
+    return Case(A, B, Cc, D, scalar(0, 1.1), scalar(0, beta), prec, beta == 0.0, "matmul")
+
+
+@pytest.mark.parametrize("beta,permute_C", [(0.7, False), (0.0, False), (0.7, True)])
+def test_tma_epilogue_batched(tapp, oracle, gpu, beta, permute_C):
+    """First M and N modes multiple of 32 (the TMA epilogue), a batch mode,
+    ragged tiles; beta = 0 skips C; a permuted C falls back to per-thread
+    epilogue loads."""
+    rng = np.random.default_rng(11)
+    for prec in (6, 5):
+        case = _matmul_case(rng, 64, 96, 80, 3, prec, beta, permute_C)
+        ex = tc_executor(tapp)
+        check_against_f64(tapp, oracle, case, device=True, executor=ex)
+        tapp.lib.TAPP_destroy_executor(ex)
+
+
+def test_tma_epilogue_4index_sampled(tapp, oracle, gpu):
+    """D[a,b,i,j] = sum_{c,d} A[a,c,i,d] B[d,b,c,j] + 0.5 C, extents 32
+    (M = N = K = 1024), split bfloat16: 4096 outputs against binary64."""
+    case = large_dense_case(np.random.default_rng(12), 0, 0, extent=32)
+    ex = tc_executor(tapp, split=True)
+    run = case.copy()
+    assert run_on_device(tapp, run, ex) == 0
+    samples = np.random.default_rng(13).integers(0, 32 ** 4, 4096)
+    err, D64, scale, offs = oracle.execute_f64(case.copy(), samples=samples)
+    got = run.D.buf[run.D.base + offs].astype(np.complex128)
+    n = 1024 * 3 + 8
+    bound = (n * 2.0 ** -24 + SPLIT_REL) * scale + 2 * 2.0 ** -24 * np.abs(D64)
+    assert (np.abs(got - D64) <= bound).all()
+    tapp.lib.TAPP_destroy_executor(ex)
