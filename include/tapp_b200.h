@@ -26,6 +26,8 @@ enum {
     TAPP_B200_ERR_NOMEM = 0x1004,       /* device allocation failed */
     TAPP_B200_ERR_INVALID = 0x1005,     /* invalid object or argument */
     TAPP_B200_ERR_LABELS = 0x1006,      /* a tensor gained modes after the product was created */
+    TAPP_B200_ERR_SCRATCH = 0x1007,     /* the product needs more scratch than the fixed array of
+                                         * tapp_b200_execute_product_noalloc holds */
 };
 
 /* ---- attribute keys, set with TAPP_attr_set on a TAPP_executor ---- */
@@ -78,6 +80,28 @@ TAPP_EXPORT size_t tapp_b200_describe_plan(TAPP_tensor_product plan, TAPP_execut
  * threads, all devices). For launch counting in benchmarks.
  */
 TAPP_EXPORT long long tapp_b200_kernel_launches(void);
+
+/*
+ * TAPP_execute_product for callers that cannot allocate device memory while
+ * they run a product: code running inside an allocator or memory manager,
+ * or a program that has handed the whole device to its own pool. There is no
+ * counterpart in the reference; it exists only in this library.
+ *
+ * Runs the tensor-core path (BF16BF16_ACCUM_F32, F16F16_ACCUM_F32/_F16, or
+ * F32 with TAPP_B200_ATTR_F32_MODE = 1) with its packed-operand scratch in a
+ * fixed 32 MiB device array of the library (held on every GPU that loads the
+ * library until the process exits); it calls no device or host allocator.
+ * A, B, C and D must be device pointers (TAPP_B200_ERR_INVALID otherwise);
+ * other precisions return TAPP_B200_ERR_UNSUPPORTED; products whose operand
+ * panels need more than the array holds return TAPP_B200_ERR_SCRATCH without
+ * launching anything. The first call on a device looks up the array's device
+ * address with that device current: make it before any stream capture.
+ * Every call shares the array, so calls whose work overlaps on the GPU race.
+ * Codes and validation are otherwise those of TAPP_execute_product.
+ */
+TAPP_EXPORT TAPP_error tapp_b200_execute_product_noalloc(TAPP_tensor_product plan, TAPP_executor exec,
+                                                         const void* alpha, const void* A, const void* B,
+                                                         const void* beta, const void* C, void* D);
 
 #ifdef __cplusplus
 }

@@ -1146,3 +1146,210 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
 }
 
 }  // namespace tb
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the tensor-core product.
+//
+// Some callers cannot allocate device memory while they run a product: code
+// that runs inside a host-side allocator callback or a memory manager, code
+// that has reserved the whole device for its own pool, or code that must not
+// touch the allocator at all once its setup is done. For them the packed
+// operand panels and the kernel's error word live in the fixed array below
+// instead of stream-ordered allocations.
+//
+//   - Every GPU that loads this library holds the array (TB_NOALLOC_SCRATCH
+//     bytes) until the process exits.
+//   - The array's device address is looked up once per device, with that
+//     device current, on the first call there (cudaGetSymbolAddress; the name
+//     of a __device__ array is only a host-side stand-in, not an address the
+//     GPU can use). Make that first call before any stream capture.
+//   - All calls share the array and it keeps the last call's contents; calls
+//     whose work overlaps on the GPU (other streams, or several host threads)
+//     race on it. The pack kernels write every panel element the GEMM reads,
+//     padding included; only the error word has to start at zero and is
+//     cleared at set-up and after each reported error.
+namespace tb {
+namespace tc {
+
+constexpr size_t NOALLOC_SCRATCH = (size_t)32 << 20;  // 32 MiB
+constexpr size_t NOALLOC_RESERVED = 256;              // error word + padding at the front
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH];
+
+static void* g_noalloc_ptr[64];
+static std::mutex g_noalloc_mutex;
+
+// device address of the array on the current device (set-up on first use)
+static cudaError_t noalloc_base(void** out)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        e = cudaMemset(p, 0, NOALLOC_RESERVED);  // error word starts at zero
+        if (e != cudaSuccess) return e;
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return cudaSuccess;
+}
+
+}  // namespace tc
+}  // namespace tb
+
+extern "C" {
+
+size_t tbk_noalloc_capacity(void) { return tb::tc::NOALLOC_SCRATCH - tb::tc::NOALLOC_RESERVED; }
+
+// Scratch bytes the tensor-core path needs for this plan.
+size_t tbk_tc_scratch_bytes(const tb_plan* P)
+{
+    using namespace tb::tc;
+    const int cplx = P->compute == TB_C32;
+    const int split = P->tc_mode == TB_TC_SPLIT_BF16 ? 3 : 1;
+    const int64_t Kseg = round_up(P->K.size * (cplx ? 2 : 1), 8);
+    const int64_t Kld = Kseg * split;
+    const int64_t Nout = P->N.size * (cplx ? 2 : 1);
+    return (size_t)round_up((int64_t)P->L.size * P->M.size * Kld * 2, 256) +
+           (size_t)round_up((int64_t)P->L.size * Nout * Kld * 2, 256);
+}
+
+// The tensor-core product of tb::launch_tc with its scratch taken from the
+// fixed array. Returns cudaErrorMemoryAllocation, without launching, when the
+// plan needs more than tbk_noalloc_capacity() bytes.
+int tbk_run_plan_tc_noalloc(const tb_plan* P, const tb_ptrs* d, void* stream, int* kernels)
+{
+    using namespace tb;
+    using namespace tb::tc;
+    cudaStream_t s = (cudaStream_t)stream;
+    *kernels = 0;
+    if (P->path != TB_PATH_TC) return (int)cudaErrorInvalidValue;
+    if (tbk_tc_scratch_bytes(P) > tbk_noalloc_capacity()) return (int)cudaErrorMemoryAllocation;
+    void* base = nullptr;
+    cudaError_t e = noalloc_base(&base);
+    if (e != cudaSuccess) return (int)e;
+    int* flag = (int*)base;
+    char* ws = (char*)base + NOALLOC_RESERVED;
+
+    const int cplx = P->compute == TB_C32;
+    const int split = P->tc_mode == TB_TC_SPLIT_BF16 ? 3 : 1;
+    const int fmt = P->tc_mode == TB_TC_F16 ? 1 : 0;
+    const int64_t M = P->M.size, N = P->N.size, Lsz = P->L.size, K = P->K.size;
+    const int64_t Kseg = round_up(K * (cplx ? 2 : 1), 8);
+    const int64_t Kld = Kseg * split;
+    const int64_t Nout = N * (cplx ? 2 : 1);
+    void* pA = ws;
+    void* pB = ws + round_up(Lsz * M * Kld * 2, 256);
+
+    for (int side = 0; side < 2; side++) {
+        PackParams pp;
+        memset(&pp, 0, sizeof(pp));
+        pp.src = side == 0 ? d->A : d->B;
+        pp.dst = side == 0 ? pA : pB;
+        pp.type = side == 0 ? P->tA : P->tB;
+        pp.conj = side == 0 ? P->conjA : P->conjB;
+        pp.round_mode = split == 3 ? TB_ROUND_NONE : P->round_in;
+        pp.cplx = cplx;
+        pp.is_B = side;
+        pp.split = split;
+        pp.fmt = fmt;
+        pp.R = side == 0 ? M : N;
+        pp.K = K;
+        pp.Lsz = Lsz;
+        pp.Kseg = Kseg;
+        pp.Kld = Kld;
+        pp.Rout = side == 0 ? M : Nout;
+        fill_modes(pp.rows, side == 0 ? P->M : P->N, side, -1);
+        fill_modes(pp.ks, P->K, side, -1);
+        fill_modes(pp.ls, P->L, side, -1);
+        fill_modes(pp.us, side == 0 ? P->UA : P->UB, side, -1);
+        pp.usize = side == 0 ? P->UA.size : P->UB.size;
+        pp.rows_fast = min_stride(side == 0 ? P->M : P->N, side) < min_stride(P->K, side);
+        if (!cplx && pp.us.n == 0 && (pp.type == T_F32 || pp.type == T_F64 || pp.type == T_F16 || pp.type == T_BF16)) {
+            switch (pp.type) {
+            case T_F32: launch_pack_real<float>(pp, split, fmt, s); break;
+            case T_F64: launch_pack_real<double>(pp, split, fmt, s); break;
+            case T_F16: launch_pack_real<__half>(pp, split, fmt, s); break;
+            default: launch_pack_real<__nv_bfloat16>(pp, split, fmt, s); break;
+            }
+        } else {
+            dim3 grid((unsigned)((pp.R + PR - 1) / PR), (unsigned)((Kseg / (cplx ? 2 : 1) + PK - 1) / PK),
+                      (unsigned)Lsz);
+            k_pack<<<grid, 256, 0, s>>>(pp);
+        }
+        count_launch();
+        (*kernels)++;
+    }
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return (int)e;
+
+    CUtensorMap tmA, tmB;
+    if (!make_map(&tmA, pA, fmt, Kld, M, Lsz, BM) || !make_map(&tmB, pB, fmt, Kld, Nout, Lsz, BN))
+        return (int)cudaErrorInvalidValue;
+    GemmParams gp;
+    memset(&gp, 0, sizeof(gp));
+    gp.tiles_m = (int)((M + BM - 1) / BM);
+    gp.tiles_n = (int)((Nout + BN - 1) / BN);
+    gp.num_tiles = gp.tiles_m * gp.tiles_n * (int)Lsz;
+    gp.num_kb = (int)((Kld + BK - 1) / BK);
+    gp.error = flag;
+    EpiParams& ep = gp.e;
+    ep.C = d->C;
+    ep.D = d->D;
+    ep.tC = P->tC;
+    ep.tD = P->tD;
+    ep.cplx = cplx;
+    ep.beta_zero = P->beta_zero;
+    ep.conjC = P->conjC;
+    ep.conjD = P->conjD;
+    ep.conjD_f32 = P->conjD_round_f32;
+    ep.round_C = P->round_in;
+    ep.alpha_re = (float)P->alpha_re;
+    ep.alpha_im = (float)P->alpha_im;
+    ep.beta_re = (float)P->beta_re;
+    ep.beta_im = (float)P->beta_im;
+    ep.M = M;
+    ep.N = N;
+    ep.L = Lsz;
+    fill_modes(ep.mm, P->M, 2, 3);
+    fill_modes(ep.nn, P->N, 2, 3);
+    fill_modes(ep.ll, P->L, 2, 3);
+    const uint32_t ab = fmt == 1 ? 0u : 1u;
+    const uint32_t idesc = (1u << 4) | (ab << 7) | (ab << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+    const bool f32_epi = !cplx && P->tD == T_F32 && (P->beta_zero || P->tC == T_F32) && !P->conjD;
+    CUtensorMap tmC = tmA, tmD = tmA;
+    const bool tma_epi = f32_epi && make_epi_map(&tmD, d->D, P, 3) &&
+                         (P->beta_zero || make_epi_map(&tmC, const_cast<void*>(d->C), P, 2));
+    const int kind = tma_epi ? EPI_TMA : (f32_epi ? EPI_F32 : EPI_ANY);
+    auto kern = kind == EPI_TMA ? k_gemm<EPI_TMA> : kind == EPI_F32 ? k_gemm<EPI_F32> : k_gemm<EPI_ANY>;
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    if (e != cudaSuccess) return (int)e;
+    const int grid = gp.num_tiles < num_sms() ? gp.num_tiles : num_sms();
+    kern<<<grid, NTHREADS, SMEM_BYTES, s>>>(tmA, tmB, gp, idesc, tmC, tmD);
+    count_launch();
+    (*kernels)++;
+    return (int)cudaGetLastError();
+}
+
+// Reads and clears the error word of the allocation-free path (synchronises).
+int tbk_noalloc_check_error(void)
+{
+    void* base = nullptr;
+    cudaError_t e = tb::tc::noalloc_base(&base);
+    if (e != cudaSuccess) return (int)e;
+    int v = 0;
+    e = cudaMemcpy(&v, base, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return (int)e;
+    if (v) {
+        cudaMemset(base, 0, sizeof(int));
+        return (int)cudaErrorLaunchTimeout;
+    }
+    return 0;
+}
+
+}  // extern "C"

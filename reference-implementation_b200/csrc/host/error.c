@@ -46,6 +46,8 @@ static const char* message_of(TAPP_error error)
     case TAPP_B200_ERR_NOMEM: return "Device memory allocation failed.";
     case TAPP_B200_ERR_INVALID: return "Invalid object or argument.";
     case TAPP_B200_ERR_LABELS: return "A tensor has more modes than when the product was created.";
+    case TAPP_B200_ERR_SCRATCH:
+        return "The product needs more scratch memory than the 32 MiB array of the allocation-free entry point.";
     default: return "Unknown error code.";
     }
 }

@@ -50,6 +50,13 @@ long long tbk_launch_count(void);
 int tbk_check_device_error(void);
 const char* tbk_error_string(int err);
 
+/* Allocation-free tensor-core product: scratch from a fixed device array of
+ * the library (tbk_noalloc_capacity() bytes); see tc.cu. */
+size_t tbk_noalloc_capacity(void);
+size_t tbk_tc_scratch_bytes(const tb_plan* plan);
+int tbk_run_plan_tc_noalloc(const tb_plan* plan, const tb_ptrs* ptrs, void* stream, int* kernels);
+int tbk_noalloc_check_error(void);
+
 #ifdef __cplusplus
 }
 #endif
