@@ -38,6 +38,20 @@ constexpr int BM = 128, BN = 256, BK = 64, STAGES = 4;
 constexpr int A_BYTES = BM * BK * 2;
 constexpr int B_BYTES = BN * BK * 2;
 constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+
+// Stage geometry per CTA. One CTA: A 128x64 and B 256x64 per stage, 4
+// stages. CTA pair (cta_group::2, 256x256 tiles): each CTA holds its 128
+// rows of A and 128 of the 256 columns of B, 6 stages. Same 192 KiB.
+template <bool CTA2>
+struct Geo {
+    static constexpr int stages = CTA2 ? 6 : 4;
+    static constexpr int b_rows = CTA2 ? 128 : 256;   // rows of B per CTA per stage
+    static constexpr int a_bytes = BM * BK * 2;
+    static constexpr int b_bytes = b_rows * BK * 2;
+    static constexpr int stage_bytes = a_bytes + b_bytes;
+    static constexpr int tile_m = CTA2 ? 2 * BM : BM;  // output rows per tile
+};
+static_assert(Geo<true>::stages * Geo<true>::stage_bytes == STAGES * STAGE_BYTES, "same ring size");
 constexpr int TMEM_COLS = 512;
 constexpr int EPI_WARPS = 8;                    // two warps per TMEM lane quarter
 constexpr int EPI_THREADS = EPI_WARPS * 32;
@@ -457,6 +471,59 @@ __device__ __forceinline__ void tma_store_5d(const CUtensorMap* tm, const void* 
                  : "memory");
 }
 
+__device__ __forceinline__ void tma_load_3d_pair(void* dst, const CUtensorMap* tm, uint32_t bar_cluster, int c0, int c1,
+                                                 int c2)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
+        ::"r"(smem_u32(dst)), "l"(tm), "r"(bar_cluster), "r"(c0), "r"(c1), "r"(c2)
+        : "memory");
+}
+
+// address of the same shared-memory location in CTA `rank` of the cluster
+__device__ __forceinline__ uint32_t cluster_addr(const void* p, uint32_t rank)
+{
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(p)), "r"(rank));
+    return r;
+}
+
+__device__ __forceinline__ uint32_t cluster_rank()
+{
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+__device__ __forceinline__ void cluster_sync()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t bar_cluster)
+{
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(bar_cluster) : "memory");
+}
+
+__device__ __forceinline__ void mma_f16_pair(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+// commit to the barrier at this offset in both CTAs of the pair
+__device__ __forceinline__ void mma_commit_pair(uint64_t* bar)
+{
+    const uint16_t mask = 3;
+    asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;"
+                 ::"r"(smem_u32(bar)), "h"(mask)
+                 : "memory");
+}
+
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 
@@ -551,86 +618,120 @@ __device__ __forceinline__ void finish_out(const EpiParams& e, int64_t offD, flo
 // per-warp shared-memory box (C and D expressible as tensor maps).
 enum { EPI_ANY = 0, EPI_F32 = 1, EPI_TMA = 2 };
 
-template <int EPI>
+template <int EPI, bool CTA2>
 __global__ void __launch_bounds__(NTHREADS, 1)
     k_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, GemmParams p,
            uint32_t idesc, const __grid_constant__ CUtensorMap tmC, const __grid_constant__ CUtensorMap tmD)
 {
+    using G = Geo<CTA2>;
+    constexpr int NS = G::stages;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
-    uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    // 1024-byte alignment by pointer arithmetic on the shared array (an
+    // integer round trip would turn every access below into a generic one)
+    uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
     uint8_t* tiles = smem;
-    uint64_t* full = (uint64_t*)(smem + STAGES * STAGE_BYTES);
-    uint64_t* empty = full + STAGES;
-    uint64_t* tfull = empty + STAGES;
-    uint64_t* tempty = tfull + 2;
-    uint32_t* tmem_slot = (uint32_t*)(tempty + 2);
-    volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
-    volatile int* epi_ok = (volatile int*)(tmem_slot + 2);
-    uint64_t* cbar = (uint64_t*)(smem + STAGES * STAGE_BYTES + 128);  // one per epilogue warp
+    uint8_t* bars = smem + STAGES * STAGE_BYTES;  // 256 bytes of barriers and flags
+    uint64_t* full = (uint64_t*)bars;             // up to 6
+    uint64_t* empty = (uint64_t*)(bars + 48);     // up to 6
+    uint64_t* tfull = (uint64_t*)(bars + 96);
+    uint64_t* tempty = (uint64_t*)(bars + 112);
+    uint64_t* cbar = (uint64_t*)(bars + 128);     // one per epilogue warp
+    uint32_t* tmem_slot = (uint32_t*)(bars + 192);
+    volatile int* abort_flag = (volatile int*)(bars + 196);
+    volatile int* epi_ok = (volatile int*)(bars + 200);
     uint8_t* staging = smem + STAGES * STAGE_BYTES + 256;
     int64_t* colC = (int64_t*)staging;
     int64_t* colD = colC + BN;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = CTA2 ? cluster_rank() : 0;  // 0 = the pair's leader, which issues the MMAs
     if (threadIdx.x == 0) {
-        for (int s = 0; s < STAGES; s++) {
+        for (int s = 0; s < NS; s++) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
         for (int a = 0; a < 2; a++) {
             mbar_init(&tfull[a], 1);
-            mbar_init(&tempty[a], EPI_THREADS);
+            // one CTA: every epilogue thread arrives; pair: one arrival per
+            // epilogue warp of either CTA, on the leader's barrier
+            mbar_init(&tempty[a], CTA2 ? 2 * EPI_WARPS : EPI_THREADS);
         }
         for (int w = 0; w < EPI_WARPS; w++) mbar_init(&cbar[w], 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 2) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(TMEM_COLS));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+        if (CTA2) {
+            asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                         "r"(TMEM_COLS));
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+        } else {
+            asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                         "r"(TMEM_COLS));
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+        }
     }
     fence_before();
-    __syncthreads();
+    if (CTA2) cluster_sync();  // barriers of both CTAs initialised before any remote signal
+    else __syncthreads();
     fence_after();
     const uint32_t tmem_base = *tmem_slot;
 
-    const int my_tiles = p.num_tiles > (int)blockIdx.x ? (p.num_tiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    // tiles: one CTA walks 128x256 tiles; a pair walks 256x256 tiles together
+    const int unit = CTA2 ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;
+    const int units = CTA2 ? (int)(gridDim.x >> 1) : (int)gridDim.x;
+    const int my_tiles = p.num_tiles > unit ? (p.num_tiles - 1 - unit) / units + 1 : 0;
 
     if (warp == 0) {
         // ---------------- TMA producer ----------------
         if (lane == 0) {
             uint32_t g = 0;
-            int64_t last_issued[STAGES];
-            for (int s = 0; s < STAGES; s++) last_issued[s] = -1;
+            int64_t last_issued[NS];
+            for (int s = 0; s < NS; s++) last_issued[s] = -1;
             bool ok = true;
             for (int i = 0; i < my_tiles && ok; i++) {
-                const int tile = blockIdx.x + i * gridDim.x;
+                const int tile = unit + i * units;
                 const int tm = tile % p.tiles_m;
                 const int rest = tile / p.tiles_m;
                 const int tn = rest % p.tiles_n;
                 const int l = rest / p.tiles_n;
                 for (int kb = 0; kb < p.num_kb; kb++, g++) {
-                    const int s = g % STAGES;
-                    const uint32_t ph = (g / STAGES) & 1;
+                    const int s = g % NS;
+                    const uint32_t ph = (g / NS) & 1;
                     if (!mbar_wait(&empty[s], ph ^ 1, abort_flag)) { ok = false; break; }
-                    mbar_expect_tx(&full[s], STAGE_BYTES);
-                    uint8_t* a = tiles + s * STAGE_BYTES;
-                    tma_load_3d(a, &tmA, &full[s], kb * BK, tm * BM, l);
-                    tma_load_3d(a + A_BYTES, &tmB, &full[s], kb * BK, tn * BN, l);
+                    uint8_t* a = tiles + s * G::stage_bytes;
+                    if (CTA2) {
+                        // both halves land on the leader's barrier, which expects the pair's bytes
+                        const uint32_t fb = cluster_addr(&full[s], 0);
+                        if (rank == 0) mbar_expect_tx(&full[s], 2 * G::stage_bytes);
+                        tma_load_3d_pair(a, &tmA, fb, kb * BK, tm * G::tile_m + (int)rank * BM, l);
+                        tma_load_3d_pair(a + G::a_bytes, &tmB, fb, kb * BK, tn * BN + (int)rank * G::b_rows, l);
+                    } else {
+                        mbar_expect_tx(&full[s], G::stage_bytes);
+                        tma_load_3d(a, &tmA, &full[s], kb * BK, tm * BM, l);
+                        tma_load_3d(a + G::a_bytes, &tmB, &full[s], kb * BK, tn * BN, l);
+                    }
                     last_issued[s] = g;
                 }
             }
-            // every issued load must land before the block exits: the phase of
-            // the last load issued on a stage stays complete once reached
-            int never = 0;
-            for (int s = 0; s < STAGES; s++)
-                if (last_issued[s] >= 0)
-                    mbar_wait(&full[s], (uint32_t)(last_issued[s] / STAGES) & 1, (volatile int*)&never);
+            if (!CTA2 || rank == 0) {
+                // every issued load must land before the block exits: the phase of
+                // the last load issued on a stage stays complete once reached
+                int never = 0;
+                for (int s = 0; s < NS; s++)
+                    if (last_issued[s] >= 0)
+                        mbar_wait(&full[s], (uint32_t)(last_issued[s] / NS) & 1, (volatile int*)&never);
+            } else if (!ok) {
+                // the second CTA's loads signal the leader: after an expired wait,
+                // give loads in flight time to land before this CTA exits
+                const unsigned long long t0 = now_ns();
+                while (now_ns() - t0 < 200000ull) {
+                }
+            }
         }
     } else if (warp == 1) {
-        // ---------------- MMA issuer ----------------
-        if (lane == 0) {
+        // ---------------- MMA issuer (the leader of a pair) ----------------
+        if (lane == 0 && (!CTA2 || rank == 0)) {
             uint32_t g = 0;
             bool ok = true;
             for (int i = 0; i < my_tiles && ok; i++) {
@@ -640,24 +741,30 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                 fence_after();
                 const uint32_t d_tmem = tmem_base + acc * BN;
                 for (int kb = 0; kb < p.num_kb; kb++, g++) {
-                    const int s = g % STAGES;
-                    const uint32_t ph = (g / STAGES) & 1;
+                    const int s = g % NS;
+                    const uint32_t ph = (g / NS) & 1;
                     if (!mbar_wait(&full[s], ph, abort_flag)) { ok = false; break; }
                     fence_after();
-                    const uint32_t a = smem_u32(tiles + s * STAGE_BYTES);
-                    const uint32_t b = a + A_BYTES;
+                    const uint32_t a = smem_u32(tiles + s * G::stage_bytes);
+                    const uint32_t b = a + G::a_bytes;
 #pragma unroll
-                    for (int k = 0; k < BK / 16; k++)
-                        mma_f16(d_tmem, smem_desc(a + k * 32), smem_desc(b + k * 32), idesc, (kb | k) != 0);
-                    mma_commit(&empty[s]);
+                    for (int k = 0; k < BK / 16; k++) {
+                        if (CTA2) mma_f16_pair(d_tmem, smem_desc(a + k * 32), smem_desc(b + k * 32), idesc, (kb | k) != 0);
+                        else mma_f16(d_tmem, smem_desc(a + k * 32), smem_desc(b + k * 32), idesc, (kb | k) != 0);
+                    }
+                    if (CTA2) mma_commit_pair(&empty[s]);
+                    else mma_commit(&empty[s]);
                 }
-                if (ok) mma_commit(&tfull[acc]);
+                if (ok) {
+                    if (CTA2) mma_commit_pair(&tfull[acc]);
+                    else mma_commit(&tfull[acc]);
+                }
             }
-            // wait for the last MMAs before the block can release TMEM
+            // wait for the last MMAs before TMEM can be released
             volatile int never = 0;
             if (g > 0) {
                 const uint32_t last = g - 1;
-                mbar_wait(&empty[last % STAGES], (last / STAGES) & 1, &never);
+                mbar_wait(&empty[last % NS], (last / NS) & 1, &never);
             }
         }
     } else if (warp >= 4) {
@@ -672,12 +779,23 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         const int et = threadIdx.x - 128;        // 0 .. EPI_THREADS-1
         const int cols_out = e.cplx ? BN / 2 : BN;
         uint32_t epi_cphase = 0;  // completed phases of this warp's C-box barrier
+        // the accumulator buffer is free again once every epilogue thread has
+        // read it (pair: once per warp, on the leader's barrier)
+        auto release_acc = [&](int acc) {
+            if (CTA2) {
+                __syncwarp();
+                if (lane == 0) mbar_arrive_cluster(cluster_addr(&tempty[acc], 0));
+            } else {
+                mbar_arrive(&tempty[acc]);
+            }
+        };
         for (int i = 0; i < my_tiles; i++) {
-            const int tile = blockIdx.x + i * gridDim.x;
+            const int tile = unit + i * units;
             const int tm = tile % p.tiles_m;
             const int rest = tile / p.tiles_m;
             const int tn = rest % p.tiles_n;
             const int l = rest / p.tiles_n;
+            const int64_t row0 = (int64_t)tm * G::tile_m + (int64_t)rank * BM;  // this CTA's first row
             // column offsets of this tile (the TMA epilogue needs none: its
             // staging boxes share this memory)
             for (int c = et; EPI != EPI_TMA && c < cols_out; c += EPI_THREADS) {
@@ -689,7 +807,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             }
             int64_t lC, lD;
             decode2(e.ll, l, lC, lD);
-            const int64_t m = (int64_t)tm * BM + q * 32 + lane;
+            const int64_t m = row0 + q * 32 + lane;
             const bool mok = m < e.M;
             int64_t rC = 0, rD = 0;
             if (mok) decode2(e.mm, m, rC, rD);
@@ -708,7 +826,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                 {
                     // the last mode keeps the whole quotient: rows past M give a
                     // coordinate past the tensor map, where TMA clips the box
-                    int64_t r = (int64_t)tm * BM + q * 32;
+                    int64_t r = row0 + q * 32;
                     for (int j = 0; j < e.mm.n; j++) {
                         const int64_t c = j + 1 < e.mm.n ? r % e.mm.ext[j] : r;
                         r /= e.mm.ext[j];
@@ -739,16 +857,20 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                     while (k < 5) cc[k++] = 0;
                 };
                 const int nch = BN / 64;  // chunks per warp
+                int cc[BN / 64][5];       // tensor-map coordinates of this warp's chunks
+#pragma unroll
+                for (int t = 0; t < nch; t++) coords(half + 2 * t, cc[t]);
+                const float alpha = e.alpha_re, beta = e.beta_re;
+                const int rmode = e.round_C;
+                const bool bzero = e.beta_zero != 0;
                 bool ok = true;
-                auto issue_c = [&](int ch) {
-                    if (lane == 0 && !e.beta_zero) {
-                        int cc[5];
-                        coords(ch, cc);
+                auto issue_c = [&](int t) {
+                    if (lane == 0 && !bzero) {
                         mbar_expect_tx(&cbar[ew], STAGE_EPI_BYTES);
-                        tma_load_5d(box, &tmC, &cbar[ew], cc);
+                        tma_load_5d(box, &tmC, &cbar[ew], cc[t]);
                     }
                 };
-                issue_c(half);
+                issue_c(0);
                 if (et == 0) *epi_ok = mbar_wait(&tfull[acc], aph, abort_flag) ? 1 : 0;
                 epi_bar();
                 ok = *epi_ok != 0;
@@ -759,34 +881,33 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                     uint32_t r[32];
                     if (ok) tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + acc * BN + ch * 32, r);
                     bool cok = true;
-                    if (!e.beta_zero) {
+                    if (!bzero) {
                         cok = mbar_wait(&cbar[ew], epi_cphase & 1, abort_flag);
                         cok = __all_sync(0xffffffffu, cok);
                         epi_cphase++;
                     }
                     if (ok && cok) {
+                        float cv[32];
 #pragma unroll
-                        for (int j = 0; j < 32; j++) {
-                            const float cv = e.beta_zero ? 0.f : e.beta_re * round_in<float>(box[j * 32 + lane], e.round_C);
-                            box[j * 32 + lane] = fmaf(e.alpha_re, __uint_as_float(r[j]), cv);
-                        }
+                        for (int j = 0; j < 32; j++) cv[j] = bzero ? 0.f : box[j * 32 + lane];
+#pragma unroll
+                        for (int j = 0; j < 32; j++)
+                            box[j * 32 + lane] = fmaf(alpha, __uint_as_float(r[j]), beta * round_in<float>(cv[j], rmode));
                         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                     }
                     __syncwarp();
                     if (lane == 0 && ok && cok) {
-                        int cc[5];
-                        coords(ch, cc);
-                        tma_store_5d(&tmD, box, cc);
+                        tma_store_5d(&tmD, box, cc[t]);
                         asm volatile("cp.async.bulk.commit_group;" ::: "memory");
                         // the box is reused by the next load: wait until the store has read it
                         asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
                     }
                     __syncwarp();
                     if (!cok) ok = false;
-                    if (t + 1 < nch && ok) issue_c(ch + 2);
+                    if (t + 1 < nch && ok) issue_c(t + 1);
                 }
                 fence_before();
-                mbar_arrive(&tempty[acc]);
+                release_acc(acc);
                 epi_bar();
                 continue;
             }
@@ -825,7 +946,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                     }
                 }
                 fence_before();
-                mbar_arrive(&tempty[acc]);
+                release_acc(acc);
                 epi_bar();  // offsets and *epi_ok may be rewritten after this point
                 continue;
             }
@@ -873,18 +994,21 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                 }
             }
             fence_before();
-            mbar_arrive(&tempty[acc]);
+            release_acc(acc);
             epi_bar();  // offsets and *epi_ok may be rewritten after this point
         }
         // no early exit above: every epilogue thread takes every tile's barriers,
         // and after an expired wait the remaining waits give up at once
         if (EPI == EPI_TMA && lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
     }
-    __syncthreads();
+    fence_before();
+    if (CTA2) cluster_sync();  // the leader's MMAs into this CTA's TMEM, and remote signals, are done
+    else __syncthreads();
     if (threadIdx.x == 0 && *abort_flag) atomicExch(p.error, 1);
     if (warp == 2) {
         fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS));
+        if (CTA2) asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS));
+        else asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS));
     }
 }
 
@@ -1008,6 +1132,39 @@ struct Workspace {
     size_t bytes = 0;
 };
 
+
+// Launches the GEMM: 1-CTA (128x256 tiles) or CTA pairs (256x256 tiles,
+// cluster of 2, cta_group::2) when M spans at least two 128-row halves.
+static cudaError_t launch_gemm(int kind, bool cta2, int grid, const CUtensorMap& tmA, const CUtensorMap& tmB,
+                               const GemmParams& gp, uint32_t idesc, const CUtensorMap& tmC, const CUtensorMap& tmD,
+                               cudaStream_t s)
+{
+    void (*kern)(CUtensorMap, CUtensorMap, GemmParams, uint32_t, CUtensorMap, CUtensorMap);
+    if (cta2) kern = kind == EPI_TMA ? k_gemm<EPI_TMA, true> : kind == EPI_F32 ? k_gemm<EPI_F32, true> : k_gemm<EPI_ANY, true>;
+    else kern = kind == EPI_TMA ? k_gemm<EPI_TMA, false> : kind == EPI_F32 ? k_gemm<EPI_F32, false> : k_gemm<EPI_ANY, false>;
+    static int attr_done[64][3][2];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64 || !attr_done[dev][kind][cta2]) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+        if (e != cudaSuccess) return e;
+        if (dev >= 0 && dev < 64) attr_done[dev][kind][cta2] = 1;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid, 1, 1);
+    cfg.blockDim = dim3(NTHREADS, 1, 1);
+    cfg.dynamicSmemBytes = SMEM_BYTES;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cta2 ? 2 : 1;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, tmA, tmB, gp, idesc, tmC, tmD);
+}
+
 }  // namespace tc
 
 cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t s, int* kernels, void** main_timer)
@@ -1083,14 +1240,16 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
         e = cudaGetLastError();
         if (e != cudaSuccess) break;
 
+        const bool cta2 = M >= 2 * BM && num_sms() % 2 == 0;
         CUtensorMap tmA, tmB;
-        if (!make_map(&tmA, pA, fmt, Kld, M, Lsz, BM) || !make_map(&tmB, pB, fmt, Kld, Nout, Lsz, BN)) {
+        if (!make_map(&tmA, pA, fmt, Kld, M, Lsz, BM) ||
+            !make_map(&tmB, pB, fmt, Kld, Nout, Lsz, cta2 ? Geo<true>::b_rows : BN)) {
             e = cudaErrorInvalidValue;
             break;
         }
         GemmParams gp;
         memset(&gp, 0, sizeof(gp));
-        gp.tiles_m = (int)((M + BM - 1) / BM);
+        gp.tiles_m = (int)((M + (cta2 ? 2 * BM : BM) - 1) / (cta2 ? 2 * BM : BM));
         gp.tiles_n = (int)((Nout + BN - 1) / BN);
         gp.num_tiles = gp.tiles_m * gp.tiles_n * (int)Lsz;
         gp.num_kb = (int)((Kld + BK - 1) / BK);
@@ -1117,28 +1276,21 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
         fill_modes(ep.nn, P->N, 2, 3);
         fill_modes(ep.ll, P->L, 2, 3);
         const uint32_t ab = fmt == 1 ? 0u : 1u;  // operand format: 0 f16, 1 bf16
+        const uint32_t mma_m = cta2 ? 2 * BM : BM;
         const uint32_t idesc = (1u << 4) | (ab << 7) | (ab << 10) | ((uint32_t)(BN >> 3) << 17) |
-                               ((uint32_t)(BM >> 4) << 24);
+                               ((mma_m >> 4) << 24);
         const bool f32_epi = !cplx && P->tD == T_F32 && (P->beta_zero || P->tC == T_F32) && !P->conjD;
         CUtensorMap tmC = tmA, tmD = tmA;  // placeholders when the TMA epilogue is not used
         const bool tma_epi = f32_epi && make_epi_map(&tmD, d[b].D, P, 3) &&
                              (P->beta_zero || make_epi_map(&tmC, const_cast<void*>(d[b].C), P, 2));
         const int kind = tma_epi ? EPI_TMA : (f32_epi ? EPI_F32 : EPI_ANY);
-        auto kern = kind == EPI_TMA ? k_gemm<EPI_TMA> : kind == EPI_F32 ? k_gemm<EPI_F32> : k_gemm<EPI_ANY>;
-        static int attr_done[64][3];
-        int dev = 0;
-        cudaGetDevice(&dev);
-        if (dev < 64 && !attr_done[dev][kind]) {
-            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-            attr_done[dev][kind] = 1;
-        }
-        const int grid = gp.num_tiles < num_sms() ? gp.num_tiles : num_sms();
+        const int units = cta2 ? num_sms() / 2 : num_sms();
+        const int grid = (gp.num_tiles < units ? gp.num_tiles : units) * (cta2 ? 2 : 1);
         if (main_timer && b == 0) tbk_timer_begin(s, main_timer);
-        kern<<<grid, NTHREADS, SMEM_BYTES, s>>>(tmA, tmB, gp, idesc, tmC, tmD);
+        e = launch_gemm(kind, cta2, grid, tmA, tmB, gp, idesc, tmC, tmD, s);
         if (main_timer && b == 0) tbk_timer_end(s, *main_timer);
         count_launch();
         (*kernels)++;
-        e = cudaGetLastError();
         if (e != cudaSuccess) break;
     }
     cudaFreeAsync(ws, s);
@@ -1326,14 +1478,11 @@ int tbk_run_plan_tc_noalloc(const tb_plan* P, const tb_ptrs* d, void* stream, in
     const bool tma_epi = f32_epi && make_epi_map(&tmD, d->D, P, 3) &&
                          (P->beta_zero || make_epi_map(&tmC, const_cast<void*>(d->C), P, 2));
     const int kind = tma_epi ? EPI_TMA : (f32_epi ? EPI_F32 : EPI_ANY);
-    auto kern = kind == EPI_TMA ? k_gemm<EPI_TMA> : kind == EPI_F32 ? k_gemm<EPI_F32> : k_gemm<EPI_ANY>;
-    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-    if (e != cudaSuccess) return (int)e;
     const int grid = gp.num_tiles < num_sms() ? gp.num_tiles : num_sms();
-    kern<<<grid, NTHREADS, SMEM_BYTES, s>>>(tmA, tmB, gp, idesc, tmC, tmD);
+    e = launch_gemm(kind, false, grid, tmA, tmB, gp, idesc, tmC, tmD, s);
     count_launch();
     (*kernels)++;
-    return (int)cudaGetLastError();
+    return (int)e;
 }
 
 // Reads and clears the error word of the allocation-free path (synchronises).
