@@ -53,7 +53,7 @@ MODES = {
     "bf16_storage": (6, 5, 0, 0),
     "f16_storage": (5, 4, 0, 0),
     "split_bf16_f32": (0, 0, 1, 0),
-    "plain_f32": (0, 0, 0, 1),
+    "plain_f32": (0, 0, 0, 3),
 }
 
 
@@ -436,8 +436,8 @@ def run_b200(args):
             mdev = [to_device(t, torch) for t in (mc.A, mc.B, mc.C, mc.D)]
             mex = make_executor(lib, stream, f32_mode=f32_mode, path=path)
             mp = Product(lib, mc, [d[1] for d in mdev], mex)
-            steps = max(2, min(args.steps, 20)) if path == 1 else args.steps
-            mt = time_device(torch, mp, steps, 1 if path == 1 else args.warmup, barrier)
+            steps = max(3, min(args.steps, 50)) if path == 3 else args.steps
+            mt = time_device(torch, mp, steps, 3 if path == 3 else args.warmup, barrier)
             mref = ref64 if storage == 0 else f64_slab_reference(lib, torch, mc)
             Dm = mdev[3][0].cpu().numpy().view(np.float32)
             merr = np.abs(slab_values(mc.D, Dm) - mref)

@@ -65,6 +65,7 @@ cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t s)
 }
 
 cudaError_t launch_generic(const tb_plan* P, const tb_ptrs* d, cudaStream_t s);
+cudaError_t launch_simt(const tb_plan* P, const tb_ptrs* d, cudaStream_t s);
 cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t s, int* kernels, void** main_timer);
 
 }  // namespace tb
@@ -162,6 +163,12 @@ int tbk_run_plan(const tb_plan* plan, const tb_ptrs* ptrs, void* stream, int* ke
     switch (plan->path) {
     case TB_PATH_NOOP: return 0;
     case TB_PATH_TC: e = tb::launch_tc(plan, ptrs, 1, s, kernels, main_timer); break;
+    case TB_PATH_SIMT:
+        if (main_timer) tbk_timer_begin(stream, main_timer);
+        e = tb::launch_simt(plan, ptrs, s);
+        if (main_timer) tbk_timer_end(stream, *main_timer);
+        *kernels = 1;
+        break;
     default:
         if (main_timer) tbk_timer_begin(stream, main_timer);
         e = tb::launch_generic(plan, ptrs, s);

@@ -363,12 +363,17 @@ int tb_build_plan(const tb_tensor_view* A, const tb_tensor_view* B,
         P->UA.n > TB_MAXMODES || P->UB.n > TB_MAXMODES)
         tc_ok = 0;
     const int big = P->M.size >= 64 && P->N.size >= 64 && ksz >= 64 && macs >= 16.0 * 1024 * 1024;
+    /* tiled CUDA-core GEMM: real products without unary modes */
+    const int simt_ok = (P->compute == TB_R32 || P->compute == TB_R64) && P->UA.n == 0 && P->UB.n == 0 &&
+                        ksz > 0 && P->UA.size == 1 && P->UB.size == 1;
+    const int simt_big = P->M.size >= 32 && P->N.size >= 32 && ksz >= 16 && macs >= 4.0 * 1024 * 1024;
+    if (simt_ok && simt_big) path = TB_PATH_SIMT;
     if (tc_ok && big) path = TB_PATH_TC;
     if (opt && opt->force_path) {
         int f = opt->force_path;
         if (f == TB_PATH_TC && tc_ok) path = TB_PATH_TC;
+        else if (f == TB_PATH_SIMT && simt_ok) path = TB_PATH_SIMT;
         else if (f == TB_PATH_GENERIC || f == TB_PATH_REDUCE) path = f;
-        else if (f == TB_PATH_SIMT) path = TB_PATH_GENERIC;
     }
     P->path = path;
     return 0;

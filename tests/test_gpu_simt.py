@@ -1,0 +1,81 @@
+"""GPU parity of the tiled CUDA-core GEMM (the plain path for large real
+products: binary32 and binary64, one launch per product).
+
+Products are forced onto it with TAPP_B200_ATTR_PATH = 3 where the planner
+would choose another path; the bound is helpers.error_bound (binary32 or
+binary64 summation, 16-bit operand rounding identical to the oracle's).
+"""
+import numpy as np
+import pytest
+
+import tapp_b200
+from tapp_b200.workloads import dense_contraction_case, large_dense_case
+from families import bounded_case
+from test_gpu_parity import check_against_f64
+
+pytestmark = pytest.mark.gpu
+
+
+def simt_executor(tapp):
+    ex = tapp.create_executor()
+    tapp.set_int(ex, tapp_b200.ATTR_PATH, tapp_b200.PATH_SIMT)
+    return ex
+
+
+def describe(tapp, case, ex):
+    infos = [tapp.tensor_info(t.dtype, t.extents, t.strides)[1] for t in (case.A, case.B, case.C, case.D)]
+    _, plan = tapp.create_product(0, [t.op for t in (case.A, case.B, case.C, case.D)], infos,
+                                  [case.A.idx, case.B.idx, case.C.idx, case.D.idx], case.prec)
+    d = tapp.describe(plan, ex)
+    tapp.lib.TAPP_destroy_tensor_product(plan)
+    return d
+
+
+def test_dense_contraction_float32_chooses_simt(tapp, oracle, gpu):
+    """D[a,b,c,d] = 1.3 sum_{e,f} A[a,e,b,f] B[f,c,e,d] + 0.7 C, extents 16, F32F32_ACCUM_F32."""
+    case = dense_contraction_case(np.random.default_rng(31), extent=16)
+    ex = tapp.create_executor()
+    assert "path=simt" in describe(tapp, case, ex)
+    check_against_f64(tapp, oracle, case, device=True, executor=ex)
+    tapp.lib.TAPP_destroy_executor(ex)
+
+
+@pytest.mark.parametrize("dtype,prec", [(0, -1), (0, 0), (1, -1), (1, 1), (0, 1), (1, 0), (0, 6), (0, 5)])
+def test_random_real_products(tapp, oracle, gpu, dtype, prec):
+    rng = np.random.default_rng(40 + dtype * 10 + prec)
+    for i in range(4):
+        case = bounded_case(rng, dtype=dtype, prec=prec, n_contracted=1 + i % 2, n_freeA=1 + (i % 2),
+                            n_freeB=1 + (i // 2), n_hadamard=i % 2, ext_choices=[3, 17, 40, 129],
+                            subtensor=bool(i % 2), mixed=(i == 3), n_repA=int(i == 2), max_work=2e6)
+        ex = simt_executor(tapp)
+        check_against_f64(tapp, oracle, case, device=bool(i % 2), executor=ex)
+        tapp.lib.TAPP_destroy_executor(ex)
+
+
+def test_mixed_storage_types(tapp, oracle, gpu):
+    rng = np.random.default_rng(50)
+    for types in [(0, 1, 0, 1), (1, 0, 1, 0), (4, 4, 0, 0), (5, 0, 0, 4)]:
+        case = bounded_case(rng, types=types, prec=-1, n_contracted=2, n_freeA=1, n_freeB=1, n_hadamard=0,
+                            ext_choices=[33, 70], max_work=2e6)
+        ex = simt_executor(tapp)
+        check_against_f64(tapp, oracle, case, device=True, executor=ex)
+        tapp.lib.TAPP_destroy_executor(ex)
+
+
+def test_double_4index_sampled(tapp, oracle, gpu):
+    """D[a,b,i,j] = sum_{e,f} A[a,b,e,f] B[e,f,i,j] + C in binary64 at extents 40/12
+    (M = 1600, N = 144, K = 1600), log-uniform magnitudes: sampled outputs."""
+    from tapp_b200.workloads import double_case
+    from helpers import run_on_device
+    case = double_case(np.random.default_rng(51), cplx=False, ab=40, ij=12)
+    ex = tapp.create_executor()
+    assert "path=simt" in describe(tapp, case, ex)
+    run = case.copy()
+    assert run_on_device(tapp, run, ex) == 0
+    samples = np.random.default_rng(52).integers(0, 40 * 40 * 12 * 12, 2048)
+    err, D64, scale, offs = oracle.execute_f64(case.copy(), samples=samples)
+    got = run.D.buf[run.D.base + offs].astype(np.complex128)
+    n = 1600 + 8
+    bound = n * 2.0 ** -53 * scale * 4 + 2 * 2.0 ** -53 * np.abs(D64)
+    assert (np.abs(got - D64) <= bound).all()
+    tapp.lib.TAPP_destroy_executor(ex)
