@@ -1,6 +1,9 @@
-// Tiled CUDA-core GEMM for real products (binary32 and binary64): the plain
-// GPU path for large contractions that the tensor cores do not take (F32F32
-// without split mode, F64F64, DEFAULT on binary32/binary64 data).
+// Tiled CUDA-core GEMM (binary32 / binary64, real or complex): the plain GPU
+// path for large contractions that the tensor cores do not take (F32F32
+// without split mode, F64F64, DEFAULT on float/double/complex data).
+// Complex operands keep real and imaginary planes in shared memory and
+// accumulate with four FMAs per product; op_A/op_B conjugation is applied at
+// load, op_C and op_D in the epilogue.
 //
 // One launch per product, operands gathered in place from their strided
 // layouts: each block owns a BM x BN tile of the L/M/N view
@@ -44,19 +47,21 @@ struct Params {
     void* D;
     int32_t tA, tB, tC, tD, round_in, beta_zero, a_rows_fast, b_rows_fast;
     int64_t M, N, K, L;
-    double alpha, beta;
+    double alpha, beta, alpha_im, beta_im;
+    int32_t conjA, conjB, conjC, conjD, conjD_f32, pad2;
     Modes am, ak, al;  // A: rows (M), contraction, batch (s0 = stride in A)
     Modes bn, bk, bl;  // B: rows (N), contraction, batch (s0 = stride in B)
     Modes cm, cn, cl;  // C (s0) and D (s1) strides of M, N, L modes
     int32_t tiles_m, tiles_n;
 };
 
-template <typename T, int BM, int BN, int BK, int TM, int TN>
+template <typename T, bool CPLX, int BM, int BN, int BK, int TM, int TN>
 __global__ void __launch_bounds__((BM / TM) * (BN / TN)) k_simt(Params p)
 {
     constexpr int NT = (BM / TM) * (BN / TN);
-    __shared__ T As[2][BK][BM + 1];
-    __shared__ T Bs[2][BK][BN + 1];
+    constexpr int NP = CPLX ? 2 : 1;  // real and imaginary planes
+    __shared__ T As[2][NP][BK][BM + 1];
+    __shared__ T Bs[2][NP][BK][BN + 1];
     __shared__ int64_t aRow[BM], bRow[BN];
     __shared__ int64_t aK[2][BK], bK[2][BK];
     __shared__ int64_t dRow[BM], cRow[BM], dCol[BN], cCol[BN];
@@ -106,7 +111,7 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN)) k_simt(Params p)
         }
     };
     constexpr int A_PER = BM * BK / NT, B_PER = BN * BK / NT;
-    T ra[A_PER], rb[B_PER];
+    T ra[A_PER][NP], rb[B_PER][NP];
     auto load_slice = [&](int64_t k0, int buf) {
 #pragma unroll
         for (int u = 0; u < A_PER; u++) {
@@ -116,7 +121,8 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN)) k_simt(Params p)
             T x = 0, xi = 0;
             if (m0 + r < p.M && k0 + kk < p.K)
                 load_rounded<T>(p.A, aRow[r] + aK[buf][kk], p.tA, p.round_in, x, xi);
-            ra[u] = x;
+            ra[u][0] = x;
+            if (CPLX) ra[u][NP - 1] = p.conjA ? -xi : xi;
         }
 #pragma unroll
         for (int u = 0; u < B_PER; u++) {
@@ -126,7 +132,8 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN)) k_simt(Params p)
             T x = 0, xi = 0;
             if (n0 + r < p.N && k0 + kk < p.K)
                 load_rounded<T>(p.B, bRow[r] + bK[buf][kk], p.tB, p.round_in, x, xi);
-            rb[u] = x;
+            rb[u][0] = x;
+            if (CPLX) rb[u][NP - 1] = p.conjB ? -xi : xi;
         }
     };
     auto store_slice = [&](int buf) {
@@ -135,22 +142,26 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN)) k_simt(Params p)
             const int e = t + NT * u;
             const int r = p.a_rows_fast ? e % BM : e / BK;
             const int kk = p.a_rows_fast ? e / BM : e % BK;
-            As[buf][kk][r] = ra[u];
+#pragma unroll
+            for (int c = 0; c < NP; c++) As[buf][c][kk][r] = ra[u][c];
         }
 #pragma unroll
         for (int u = 0; u < B_PER; u++) {
             const int e = t + NT * u;
             const int r = p.b_rows_fast ? e % BN : e / BK;
             const int kk = p.b_rows_fast ? e / BN : e % BK;
-            Bs[buf][kk][r] = rb[u];
+#pragma unroll
+            for (int c = 0; c < NP; c++) Bs[buf][c][kk][r] = rb[u][c];
         }
     };
 
-    T acc[TM][TN];
+    T acc[TM][TN][NP];
 #pragma unroll
     for (int i = 0; i < TM; i++)
 #pragma unroll
-        for (int j = 0; j < TN; j++) acc[i][j] = 0;
+        for (int j = 0; j < TN; j++)
+#pragma unroll
+            for (int c = 0; c < NP; c++) acc[i][j][c] = 0;
     const int tr = t / (BN / TN), tc = t % (BN / TN);  // thread's rows tr*TM.., columns tc + j*(BN/TN)
 
     slice_offsets(0, 0);
@@ -165,15 +176,26 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN)) k_simt(Params p)
         if (s + 1 < nslices) load_slice((s + 1) * BK, buf ^ 1);  // global loads in flight during the FMAs
 #pragma unroll
         for (int kk = 0; kk < BK; kk++) {
-            T a[TM], b[TN];
-#pragma unroll
-            for (int i = 0; i < TM; i++) a[i] = As[buf][kk][tr * TM + i];
-#pragma unroll
-            for (int j = 0; j < TN; j++) b[j] = Bs[buf][kk][tc + j * (BN / TN)];
+            T a[TM][NP], b[TN][NP];
 #pragma unroll
             for (int i = 0; i < TM; i++)
 #pragma unroll
-                for (int j = 0; j < TN; j++) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+                for (int c = 0; c < NP; c++) a[i][c] = As[buf][c][kk][tr * TM + i];
+#pragma unroll
+            for (int j = 0; j < TN; j++)
+#pragma unroll
+                for (int c = 0; c < NP; c++) b[j][c] = Bs[buf][c][kk][tc + j * (BN / TN)];
+#pragma unroll
+            for (int i = 0; i < TM; i++)
+#pragma unroll
+                for (int j = 0; j < TN; j++) {
+                    acc[i][j][0] = fma(a[i][0], b[j][0], acc[i][j][0]);
+                    if (CPLX) {
+                        acc[i][j][0] = fma(-a[i][NP - 1], b[j][NP - 1], acc[i][j][0]);
+                        acc[i][j][NP - 1] = fma(a[i][0], b[j][NP - 1], acc[i][j][NP - 1]);
+                        acc[i][j][NP - 1] = fma(a[i][NP - 1], b[j][0], acc[i][j][NP - 1]);
+                    }
+                }
         }
         if (s + 1 < nslices) {
             store_slice(buf ^ 1);
@@ -182,8 +204,8 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN)) k_simt(Params p)
             __syncthreads();
         }
     }
-    // epilogue
-    const T alpha = (T)p.alpha, beta = (T)p.beta;
+    // epilogue: D = op_D(alpha * acc + beta * op_C(C))
+    const T ar = (T)p.alpha, ai = (T)p.alpha_im, br = (T)p.beta, bi = (T)p.beta_im;
 #pragma unroll
     for (int i = 0; i < TM; i++) {
         const int r = tr * TM + i;
@@ -192,13 +214,27 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN)) k_simt(Params p)
         for (int j = 0; j < TN; j++) {
             const int c = tc + j * (BN / TN);
             if (n0 + c >= p.N) continue;
-            T v = alpha * acc[i][j];
+            const T xr = acc[i][j][0], xi = CPLX ? acc[i][j][NP - 1] : (T)0;
+            T vr = ar * xr - (CPLX ? ai * xi : (T)0);
+            T vi = CPLX ? ar * xi + ai * xr : (T)0;
             if (!p.beta_zero) {
                 T cr, ci;
                 load_rounded<T>(p.C, cRow[r] + cCol[c], p.tC, p.round_in, cr, ci);
-                v = fma(beta, cr, v);
+                if (p.conjC) ci = -ci;
+                vr = fma(br, cr, vr);
+                if (CPLX) {
+                    vr = fma(-bi, ci, vr);
+                    vi = fma(br, ci, fma(bi, cr, vi));
+                }
             }
-            store_elem<T>(p.D, dRow[r] + dCol[c], p.tD, v, (T)0);
+            if (p.conjD) {
+                if (p.conjD_f32) {
+                    vr = (T)(float)vr;
+                    vi = (T)(float)vi;
+                }
+                vi = -vi;
+            }
+            store_elem<T>(p.D, dRow[r] + dCol[c], p.tD, vr, vi);
         }
     }
 }
@@ -226,14 +262,14 @@ static int64_t min_abs(const tb_modes& m, int w)
     return best;
 }
 
-template <typename T, int BM, int BN, int BK, int TM, int TN>
+template <typename T, bool CPLX, int BM, int BN, int BK, int TM, int TN>
 static cudaError_t launch(Params& p, cudaStream_t s)
 {
     p.tiles_m = (int)((p.M + BM - 1) / BM);
     p.tiles_n = (int)((p.N + BN - 1) / BN);
     const int64_t blocks = (int64_t)p.tiles_m * p.tiles_n * p.L;
     if (blocks <= 0 || blocks > 0x7fffffff) return cudaErrorInvalidConfiguration;
-    k_simt<T, BM, BN, BK, TM, TN><<<(unsigned)blocks, (BM / TM) * (BN / TN), 0, s>>>(p);
+    k_simt<T, CPLX, BM, BN, BK, TM, TN><<<(unsigned)blocks, (BM / TM) * (BN / TN), 0, s>>>(p);
     count_launch();
     return cudaGetLastError();
 }
@@ -261,6 +297,13 @@ cudaError_t launch_simt(const tb_plan* P, const tb_ptrs* d, cudaStream_t s)
     p.L = P->L.size;
     p.alpha = P->alpha_re;
     p.beta = P->beta_re;
+    p.alpha_im = P->alpha_im;
+    p.beta_im = P->beta_im;
+    p.conjA = P->conjA;
+    p.conjB = P->conjB;
+    p.conjC = P->conjC;
+    p.conjD = P->conjD;
+    p.conjD_f32 = P->conjD_round_f32;
     fill(p.am, P->M, 0, -1);
     fill(p.ak, P->K, 0, -1);
     fill(p.al, P->L, 0, -1);
@@ -272,8 +315,12 @@ cudaError_t launch_simt(const tb_plan* P, const tb_ptrs* d, cudaStream_t s)
     fill(p.cl, P->L, 2, 3);
     p.a_rows_fast = min_abs(P->M, 0) < min_abs(P->K, 0);
     p.b_rows_fast = min_abs(P->N, 1) < min_abs(P->K, 1);
-    if (P->compute == TB_R64) return launch<double, 64, 64, 16, 4, 4>(p, s);
-    return launch<float, 128, 128, 16, 8, 8>(p, s);
+    switch (P->compute) {
+    case TB_R64: return launch<double, false, 64, 64, 16, 4, 4>(p, s);
+    case TB_C32: return launch<float, true, 64, 64, 8, 4, 4>(p, s);
+    case TB_C64: return launch<double, true, 64, 64, 8, 4, 4>(p, s);
+    default: return launch<float, false, 128, 128, 16, 8, 8>(p, s);
+    }
 }
 
 }  // namespace tb

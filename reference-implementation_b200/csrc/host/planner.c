@@ -363,9 +363,8 @@ int tb_build_plan(const tb_tensor_view* A, const tb_tensor_view* B,
         P->UA.n > TB_MAXMODES || P->UB.n > TB_MAXMODES)
         tc_ok = 0;
     const int big = P->M.size >= 64 && P->N.size >= 64 && ksz >= 64 && macs >= 16.0 * 1024 * 1024;
-    /* tiled CUDA-core GEMM: real products without unary modes */
-    const int simt_ok = (P->compute == TB_R32 || P->compute == TB_R64) && P->UA.n == 0 && P->UB.n == 0 &&
-                        ksz > 0 && P->UA.size == 1 && P->UB.size == 1;
+    /* tiled CUDA-core GEMM: products without unary modes */
+    const int simt_ok = P->UA.n == 0 && P->UB.n == 0 && ksz > 0 && P->UA.size == 1 && P->UB.size == 1;
     const int simt_big = P->M.size >= 32 && P->N.size >= 32 && ksz >= 16 && macs >= 4.0 * 1024 * 1024;
     if (simt_ok && simt_big) path = TB_PATH_SIMT;
     if (tc_ok && big) path = TB_PATH_TC;

@@ -79,3 +79,36 @@ def test_double_4index_sampled(tapp, oracle, gpu):
     bound = n * 2.0 ** -53 * scale * 4 + 2 * 2.0 ** -53 * np.abs(D64)
     assert (np.abs(got - D64) <= bound).all()
     tapp.lib.TAPP_destroy_executor(ex)
+
+
+@pytest.mark.parametrize("dtype,prec", [(2, -1), (3, -1), (2, 0), (3, 1), (3, 0), (2, 1)])
+def test_complex_products(tapp, oracle, gpu, dtype, prec):
+    """Complex float and double with every element op (op_C only under DEFAULT,
+    op_D under F64 rounding through binary32, as the reference does)."""
+    rng = np.random.default_rng(60 + dtype * 10 + prec)
+    for i in range(4):
+        case = bounded_case(rng, dtype=dtype, prec=prec, n_contracted=1 + i % 2, n_freeA=1, n_freeB=1 + i % 2,
+                            n_hadamard=i % 2, ext_choices=[5, 33, 70], ops=[i & 1, (i >> 1) & 1, 1, int(i == 3)],
+                            subtensor=bool(i % 2), mixed=(i == 2), max_work=1e6)
+        ex = simt_executor(tapp)
+        check_against_f64(tapp, oracle, case, device=bool(i % 2), executor=ex)
+        tapp.lib.TAPP_destroy_executor(ex)
+
+
+def test_complex_double_4index_sampled(tapp, oracle, gpu):
+    """The complex-double form of the 4-index contraction with conj(A), extents
+    40/12, random phases, log-uniform magnitudes: sampled outputs."""
+    from tapp_b200.workloads import double_case
+    from helpers import run_on_device
+    case = double_case(np.random.default_rng(61), cplx=True, ab=40, ij=12)
+    ex = tapp.create_executor()
+    assert "path=simt" in describe(tapp, case, ex) and "compute=c64" in describe(tapp, case, ex)
+    run = case.copy()
+    assert run_on_device(tapp, run, ex) == 0
+    samples = np.random.default_rng(62).integers(0, 40 * 40 * 12 * 12, 2048)
+    err, D64, scale, offs = oracle.execute_f64(case.copy(), samples=samples)
+    got = run.D.buf[run.D.base + offs].astype(np.complex128)
+    n = 1600 + 8
+    bound = n * 2.0 ** -53 * scale * 4 + 2 * 2.0 ** -53 * np.abs(D64)
+    assert (np.abs(got - D64) <= bound).all()
+    tapp.lib.TAPP_destroy_executor(ex)
