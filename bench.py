@@ -65,6 +65,9 @@ def parse():
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-modes", action="store_true", help="skip the non-headline precision modes")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--served", type=int, default=1000,
+                    help="requests in the served-stream measurement (0 skips it)")
+    ap.add_argument("--only-served", action="store_true", help="print only the served-stream measurement")
     ap.add_argument("--only-headline", action="store_true",
                     help="run only the timed headline steps (for profiling); prints its timing")
     return ap.parse_args()
@@ -353,6 +356,60 @@ def slab_values(case_D, dbuf, j_count=2):
     return dbuf[case_D.base + sub.offsets()].astype(np.float64)
 
 
+def served_measure(lib, torch, n, seed=5, max_tensor_bytes=1 << 30):
+    """The served configuration on a reduced stream: n requests of the served
+    mix (every tensor at most max_tensor_bytes), operands resident in HBM.
+    Plain: one synchronous TAPP_execute_product per request, in order; its
+    per-request service times set the Poisson arrival rate (the rate that
+    saturates the plain path) and give its FIFO latencies at those arrivals.
+    Served: the same requests through a server, at those Poisson arrivals and
+    all at once (capacity)."""
+    from tapp_b200.workloads import served_stream
+    from tapp_b200.served import StreamRunner, fifo_latencies
+    from tapp_b200.server import Server
+    rng = np.random.default_rng(seed)
+    specs = served_stream(rng, n, max_tensor_bytes=max_tensor_bytes)
+    run = StreamRunner(lib, specs, torch, seed=seed)
+    ex = make_executor(lib, None, async_=False)
+    run.run_plain(ex, order=range(min(n, 64)))      # warm-up: module loads, pool growth
+    service = run.run_plain(ex)
+    lib.lib.TAPP_destroy_executor(ex)
+    t_plain = float(service.sum())
+    rate = n / t_plain
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
+    flops = float(run.flops.sum())
+    with Server(lib, 64 << 30, n_streams=4, max_in_flight=64) as srv:
+        run.run_served(srv, arrivals=None)               # warm-up of the served path
+        burst = run.run_served(srv, arrivals=None)
+        poisson = run.run_served(srv, arrivals=arrivals)
+    run.close()
+    lat = fifo_latencies(arrivals, service)
+    def served_summary(st):
+        return {"req_per_s": st["requests_per_s"], "tflops": flops / st["span_s"] / 1e12,
+                "p50_ms": st["p50_us"] / 1e3, "p99_ms": st["p99_us"] / 1e3, "span_s": st["span_s"],
+                "units": st["units"], "grouped_requests": st["grouped"], "peak_in_flight": st["peak_in_flight"],
+                "failed": st["failed"]}
+    kinds = {}
+    for s_ in specs:
+        kinds[s_.kind] = kinds.get(s_.kind, 0) + 1
+    return {
+        "workload": "served stream: 50% Tucker mode-n, 30% binary, 20% Hadamard+contraction; "
+                    "40% f32, 30% bf16-accum-f32, 20% f64, 10% c32; HBM budget 64 GB",
+        "requests": n, "requests_by_kind": kinds, "max_tensor_bytes": max_tensor_bytes,
+        "total_gflop": flops / 1e9,
+        "reduction": f"{n} of 20000 requests; every tensor <= {max_tensor_bytes >> 20} MiB",
+        "arrival_rate_per_s": rate,
+        "plain": {"req_per_s": n / t_plain, "tflops": flops / t_plain / 1e12,
+                  "service_mean_ms": 1e3 * t_plain / n,
+                  "p50_ms": 1e3 * float(np.percentile(lat, 50)), "p99_ms": 1e3 * float(np.percentile(lat, 99)),
+                  "how": "synchronous TAPP_execute_product per request; latency = FIFO queue of the measured "
+                         "service times at the Poisson arrivals"},
+        "served_poisson": served_summary(poisson),
+        "served_burst": served_summary(burst),
+        "burst_vs_plain": burst["requests_per_s"] * t_plain / n,
+    }
+
+
 def run_b200(args):
     import torch
     import tapp_b200
@@ -370,6 +427,10 @@ def run_b200(args):
 
     lib = tapp_b200.load()
     stream = torch.cuda.current_stream().cuda_stream
+    if args.only_served:
+        if rank == 0:
+            print(json.dumps(served_measure(lib, torch, max(args.served, 1))), flush=True)
+        return
 
     # ---------------- headline: BF16BF16_ACCUM_F32, operands in HBM ----------------
     case = mode_case("bf16")
@@ -477,6 +538,10 @@ def run_b200(args):
     prod_h.close()
     lib.lib.TAPP_destroy_executor(ex_h)
 
+    served = None
+    if world == 1 and args.served > 0:
+        served = served_measure(lib, torch, args.served)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_reference_run()
@@ -493,7 +558,7 @@ def run_b200(args):
                            "l2": "inputs 256 MiB > 126 MB L2 (A,B,C,D 64 MiB each)",
                            "step": "pack A, pack B, tcgen05 GEMM + fused epilogue"},
                 "vs_plain_gpu": (value / world / plain) if plain else None,
-                "modes": modes, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu,
+                "modes": modes, "served": served, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu,
                 "clocks": clocks, "gpu_launches": gpu_launches}
         print(json.dumps(line), flush=True)
     prod.close()

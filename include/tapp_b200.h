@@ -28,6 +28,8 @@ enum {
     TAPP_B200_ERR_LABELS = 0x1006,      /* a tensor gained modes after the product was created */
     TAPP_B200_ERR_SCRATCH = 0x1007,     /* the product needs more scratch than the fixed array of
                                          * tapp_b200_execute_product_noalloc holds */
+    TAPP_B200_ERR_BUDGET = 0x1008,      /* a served product needs more device memory than the
+                                         * server's whole HBM budget */
 };
 
 /* ---- attribute keys, set with TAPP_attr_set on a TAPP_executor ---- */
@@ -51,6 +53,11 @@ enum {
      * *status, to be read with TAPP_attr_get and freed with
      * TAPP_destroy_status. */
     TAPP_B200_ATTR_WANT_STATUS = 0x1005,
+    /* value: TAPP_b200_server (cast to void*), NULL to detach. Products
+     * executed with this executor are queued on the server and the call
+     * returns when the product has completed; concurrent callers (threads)
+     * are batched together. Detach before destroying the server. */
+    TAPP_B200_ATTR_SERVER = 0x1006,
 };
 
 /* ---- keys readable from a status object with TAPP_attr_get ---- */
@@ -102,6 +109,69 @@ TAPP_EXPORT long long tapp_b200_kernel_launches(void);
 TAPP_EXPORT TAPP_error tapp_b200_execute_product_noalloc(TAPP_tensor_product plan, TAPP_executor exec,
                                                          const void* alpha, const void* A, const void* B,
                                                          const void* beta, const void* C, void* D);
+
+/*
+ * Serving: a request loop that runs products as they arrive on one GPU.
+ * There is no counterpart in the reference (its handle and executor are
+ * placeholders).
+ *
+ * tapp_b200_server_submit validates and plans a product on the calling
+ * thread (returning the same codes TAPP_execute_product would) and queues
+ * it; a scheduler thread admits queued products in arrival order while the
+ * device memory they need fits the HBM budget and fewer than max_in_flight
+ * are running, issues them over n_streams CUDA streams so that their work
+ * overlaps on the GPU, and packs the small products of the CUDA-core element
+ * path that it admits together into one grouped launch per compute domain.
+ * Products that arrive while others run join at the next admission
+ * (continuous batching); each product's memory and slot are released when its
+ * own work has completed.
+ *
+ * Device memory charged against the budget: the staging copies of host
+ * operands (as TAPP_execute_product stages them) and the tensor-core path's
+ * packed panels. Device-resident operands are used in place and not charged.
+ * A product that needs more than the whole budget is refused at submission
+ * with TAPP_B200_ERR_BUDGET. alpha and beta are read at submission; the
+ * operands must stay valid, and D untouched, until the product completes. Results are those TAPP_execute_product gives for the same product:
+ * each runs the same kernels with the same arguments.
+ */
+typedef intptr_t TAPP_b200_server;
+
+typedef struct tapp_b200_server_counters {
+    int64_t submitted;        /* products queued (refused ones excluded) */
+    int64_t completed;        /* products finished, including failed ones */
+    int64_t failed;           /* products whose launch failed */
+    int64_t units;            /* launch units issued: grouped launches plus single products */
+    int64_t grouped;          /* products that ran inside a grouped launch */
+    int64_t budget_waits;     /* products that waited in the queue for budget to free up */
+    int64_t peak_in_flight;   /* most products in flight at once */
+    int64_t budget_bytes;     /* the budget */
+    int64_t peak_reserved;    /* most bytes charged at once */
+    double p50_us, p99_us, mean_us, max_us; /* latency, submission to completion */
+    double span_s;            /* first submission to last completion, seconds */
+    double requests_per_s;    /* completed / span_s */
+    double flops;             /* algorithmic flops of the completed products */
+} tapp_b200_server_counters;
+
+/* Creates a server on the current CUDA device. exec (may be 0) supplies the
+ * precision options (TAPP_B200_ATTR_F32_MODE, _PATH) of submitted products;
+ * n_streams 1..16, max_in_flight >= 1. */
+TAPP_EXPORT TAPP_error tapp_b200_server_create(TAPP_b200_server* server, TAPP_executor exec,
+                                               int64_t hbm_budget_bytes, int n_streams, int max_in_flight);
+/* Queues a product; *ticket identifies it for tapp_b200_server_wait. */
+TAPP_EXPORT TAPP_error tapp_b200_server_submit(TAPP_b200_server server, TAPP_tensor_product plan,
+                                               const void* alpha, const void* A, const void* B,
+                                               const void* beta, const void* C, void* D, int64_t* ticket);
+/* Waits for one product; returns its code (0, or the CUDA error of its launch). */
+TAPP_EXPORT TAPP_error tapp_b200_server_wait(TAPP_b200_server server, int64_t ticket);
+/* Waits for every product submitted so far; returns the first failure's code or 0. */
+TAPP_EXPORT TAPP_error tapp_b200_server_drain(TAPP_b200_server server);
+/* Counters and latency percentiles of the products completed so far. */
+TAPP_EXPORT TAPP_error tapp_b200_server_stats(TAPP_b200_server server, tapp_b200_server_counters* out);
+/* Forgets completed products (their tickets become invalid) and restarts the
+ * counters; products in flight are kept. */
+TAPP_EXPORT TAPP_error tapp_b200_server_reset_stats(TAPP_b200_server server);
+/* Drains, stops the scheduler and frees the server. */
+TAPP_EXPORT TAPP_error tapp_b200_server_destroy(TAPP_b200_server server);
 
 #ifdef __cplusplus
 }

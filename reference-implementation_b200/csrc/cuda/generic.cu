@@ -115,54 +115,83 @@ __device__ __forceinline__ void finish(const GenParams& p, R sr, R si, const voi
     store_elem<R>(D, oD, p.tD, accr, acci);
 }
 
+// one element of D: the reference's loop nest for output index i
+template <typename R, bool CPLX>
+__device__ __forceinline__ void element(const GenParams& p, const void* A, const void* B, const void* C, void* D,
+                                        int64_t i)
+{
+    int64_t oA = 0, oB = 0, oC = 0, oD = 0;
+    if (p.small_F) {
+        uint32_t r = (uint32_t)i;
+        for (int j = 0; j < p.nF; j++) {
+            uint32_t q = fdiv(r, p.fF[j]);
+            int64_t c = r - q * p.fF[j].d;
+            r = q;
+            oA += c * p.F_sA[j];
+            oB += c * p.F_sB[j];
+            oC += c * p.F_sC[j];
+            oD += c * p.F_sD[j];
+        }
+    } else {
+        int64_t r = i;
+        for (int j = 0; j < p.nF; j++) {
+            int64_t c = r % p.F_ext[j];
+            r /= p.F_ext[j];
+            oA += c * p.F_sA[j];
+            oB += c * p.F_sB[j];
+            oC += c * p.F_sC[j];
+            oD += c * p.F_sD[j];
+        }
+    }
+    R sr = 0, si = 0;
+    int64_t kc[TB_MAXMODES];
+    for (int j = 0; j < p.nK; j++) kc[j] = 0;
+    int64_t kA = oA, kB = oB;
+    for (int64_t k = 0; k < p.sizeK; k++) {
+        R ar, ai, br, bi;
+        unary_sum<R, CPLX>(A, kA, p.tA, p.conjA, p.round_in, p.nUA, p.sizeUA, p.UA_ext, p.UA_s, ar, ai);
+        unary_sum<R, CPLX>(B, kB, p.tB, p.conjB, p.round_in, p.nUB, p.sizeUB, p.UB_ext, p.UB_s, br, bi);
+        cmac<R, CPLX>(sr, si, ar, ai, br, bi);
+        for (int j = 0; j < p.nK; j++) {
+            kA += p.K_sA[j];
+            kB += p.K_sB[j];
+            if (++kc[j] < p.K_ext[j]) break;
+            kA -= p.K_sA[j] * p.K_ext[j];
+            kB -= p.K_sB[j] * p.K_ext[j];
+            kc[j] = 0;
+        }
+    }
+    finish<R, CPLX>(p, sr, si, C, oC, D, oD);
+}
+
 template <typename R, bool CPLX>
 __global__ void __launch_bounds__(256) k_elementwise(GenParams p, const void* A, const void* B, const void* C, void* D)
 {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < p.sizeF; i += stride) {
-        int64_t oA = 0, oB = 0, oC = 0, oD = 0;
-        if (p.small_F) {
-            uint32_t r = (uint32_t)i;
-            for (int j = 0; j < p.nF; j++) {
-                uint32_t q = fdiv(r, p.fF[j]);
-                int64_t c = r - q * p.fF[j].d;
-                r = q;
-                oA += c * p.F_sA[j];
-                oB += c * p.F_sB[j];
-                oC += c * p.F_sC[j];
-                oD += c * p.F_sD[j];
-            }
-        } else {
-            int64_t r = i;
-            for (int j = 0; j < p.nF; j++) {
-                int64_t c = r % p.F_ext[j];
-                r /= p.F_ext[j];
-                oA += c * p.F_sA[j];
-                oB += c * p.F_sB[j];
-                oC += c * p.F_sC[j];
-                oD += c * p.F_sD[j];
-            }
-        }
-        R sr = 0, si = 0;
-        int64_t kc[TB_MAXMODES];
-        for (int j = 0; j < p.nK; j++) kc[j] = 0;
-        int64_t kA = oA, kB = oB;
-        for (int64_t k = 0; k < p.sizeK; k++) {
-            R ar, ai, br, bi;
-            unary_sum<R, CPLX>(A, kA, p.tA, p.conjA, p.round_in, p.nUA, p.sizeUA, p.UA_ext, p.UA_s, ar, ai);
-            unary_sum<R, CPLX>(B, kB, p.tB, p.conjB, p.round_in, p.nUB, p.sizeUB, p.UB_ext, p.UB_s, br, bi);
-            cmac<R, CPLX>(sr, si, ar, ai, br, bi);
-            for (int j = 0; j < p.nK; j++) {
-                kA += p.K_sA[j];
-                kB += p.K_sB[j];
-                if (++kc[j] < p.K_ext[j]) break;
-                kA -= p.K_sA[j] * p.K_ext[j];
-                kB -= p.K_sB[j] * p.K_ext[j];
-                kc[j] = 0;
-            }
-        }
-        finish<R, CPLX>(p, sr, si, C, oC, D, oD);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < p.sizeF; i += stride)
+        element<R, CPLX>(p, A, B, C, D, i);
+}
+
+// Many independent products of the same compute domain in one launch:
+// product j owns blocks [first[j], first[j+1]) and walks its elements with
+// them. Descriptors and operand pointers live in device memory.
+template <typename R, bool CPLX>
+__global__ void __launch_bounds__(256) k_elementwise_group(const GenParams* __restrict__ params,
+                                                           const tb_ptrs* __restrict__ ptrs,
+                                                           const int64_t* __restrict__ first, int n)
+{
+    int lo = 0, hi = n - 1;  // last j with first[j] <= blockIdx.x
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (first[mid] <= (int64_t)blockIdx.x) lo = mid;
+        else hi = mid - 1;
     }
+    const GenParams& p = params[lo];
+    const tb_ptrs q = ptrs[lo];
+    const int64_t nb = first[lo + 1] - first[lo];
+    const int64_t stride = nb * blockDim.x;
+    for (int64_t i = ((int64_t)blockIdx.x - first[lo]) * blockDim.x + threadIdx.x; i < p.sizeF; i += stride)
+        element<R, CPLX>(p, q.A, q.B, q.C, q.D, i);
 }
 
 template <typename R>
@@ -256,6 +285,51 @@ static cudaError_t launch_typed(const GenParams& g, int path, const tb_ptrs* d, 
         if (blocks > 148 * 64) blocks = 148 * 64;
         if (blocks < 1) blocks = 1;
         k_elementwise<R, CPLX><<<(unsigned)blocks, 256, 0, s>>>(g, d->A, d->B, d->C, d->D);
+    }
+    count_launch();
+    return cudaGetLastError();
+}
+
+size_t group_descriptor_bytes(int n)
+{
+    return (size_t)n * sizeof(GenParams) + (size_t)n * sizeof(tb_ptrs) + (size_t)(n + 1) * sizeof(int64_t) + 64;
+}
+
+// Fills `host` (pinned, group_descriptor_bytes(n)) with the descriptors of n
+// products of one compute domain, copies it to `dev` and launches one grouped
+// kernel. The host buffer must stay untouched until the copy has run.
+cudaError_t launch_generic_group(const tb_plan* const* P, const tb_ptrs* d, int n, void* host, void* dev,
+                                 cudaStream_t s)
+{
+    if (n <= 0) return cudaSuccess;
+    char* h = (char*)host;
+    GenParams* hp = (GenParams*)h;
+    tb_ptrs* hq = (tb_ptrs*)(h + (size_t)n * sizeof(GenParams));
+    int64_t* hf = (int64_t*)(h + (size_t)n * (sizeof(GenParams) + sizeof(tb_ptrs)));
+    int64_t blocks = 0;
+    for (int j = 0; j < n; j++) {
+        fill_params(P[j], hp[j]);
+        hq[j] = d[j];
+        hf[j] = blocks;
+        int64_t b = (P[j]->F.size + 255) / 256;
+        if (b > 148 * 8) b = 148 * 8;
+        if (b < 1) b = 1;
+        blocks += b;
+    }
+    hf[n] = blocks;
+    const size_t bytes = group_descriptor_bytes(n);
+    cudaError_t e = cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return e;
+    char* dv = (char*)dev;
+    const GenParams* dp = (const GenParams*)dv;
+    const tb_ptrs* dq = (const tb_ptrs*)(dv + (size_t)n * sizeof(GenParams));
+    const int64_t* df = (const int64_t*)(dv + (size_t)n * (sizeof(GenParams) + sizeof(tb_ptrs)));
+    if (blocks > 0x7fffffff) return cudaErrorInvalidConfiguration;
+    switch (P[0]->compute) {
+    case TB_R32: k_elementwise_group<float, false><<<(unsigned)blocks, 256, 0, s>>>(dp, dq, df, n); break;
+    case TB_R64: k_elementwise_group<double, false><<<(unsigned)blocks, 256, 0, s>>>(dp, dq, df, n); break;
+    case TB_C32: k_elementwise_group<float, true><<<(unsigned)blocks, 256, 0, s>>>(dp, dq, df, n); break;
+    default: k_elementwise_group<double, true><<<(unsigned)blocks, 256, 0, s>>>(dp, dq, df, n); break;
     }
     count_launch();
     return cudaGetLastError();

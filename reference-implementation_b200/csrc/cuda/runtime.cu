@@ -67,6 +67,11 @@ cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t s)
 cudaError_t launch_generic(const tb_plan* P, const tb_ptrs* d, cudaStream_t s);
 cudaError_t launch_simt(const tb_plan* P, const tb_ptrs* d, cudaStream_t s);
 cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t s, int* kernels, void** main_timer);
+size_t group_descriptor_bytes(int n);
+cudaError_t launch_generic_group(const tb_plan* const* P, const tb_ptrs* d, int n, void* host, void* dev,
+                                 cudaStream_t s);
+
+static void CUDART_CB free_host_buffer(void* p) { free(p); }
 
 }  // namespace tb
 
@@ -184,6 +189,33 @@ int tbk_run_plan_batched(const tb_plan* plan, const tb_ptrs* ptrs, int num, void
     cudaStream_t s = (cudaStream_t)stream;
     *kernels = 0;
     if (plan->path == TB_PATH_TC) return (int)tb::launch_tc(plan, ptrs, num, s, kernels, nullptr);
+    if (plan->path == TB_PATH_GENERIC && num > 1) {
+        // one grouped launch; the descriptors go through a host buffer that a
+        // stream callback frees once the copy has run
+        const size_t bytes = tb::group_descriptor_bytes(num);
+        void* host = malloc(bytes);
+        const tb_plan** plans = (const tb_plan**)malloc(sizeof(tb_plan*) * (size_t)num);
+        if (!host || !plans) {
+            free(host);
+            free(plans);
+            return (int)cudaErrorMemoryAllocation;
+        }
+        for (int i = 0; i < num; i++) plans[i] = plan;
+        void* dev = nullptr;
+        cudaError_t e = tb::pool_alloc(&dev, bytes, s);
+        if (e == cudaSuccess) {
+            e = tb::launch_generic_group(plans, ptrs, num, host, dev, s);
+            cudaFreeAsync(dev, s);
+        }
+        free(plans);
+        if (e == cudaSuccess) e = cudaLaunchHostFunc(s, tb::free_host_buffer, host);
+        else {
+            cudaStreamSynchronize(s);
+            free(host);
+        }
+        *kernels = 1;
+        return (int)e;
+    }
     for (int i = 0; i < num; i++) {
         int k = 0;
         int e = tbk_run_plan(plan, &ptrs[i], stream, &k, nullptr);
@@ -191,6 +223,35 @@ int tbk_run_plan_batched(const tb_plan* plan, const tb_ptrs* ptrs, int num, void
         if (e) return e;
     }
     return 0;
+}
+
+int tbk_stream_create(void** stream)
+{
+    cudaStream_t s = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    *stream = s;
+    return (int)e;
+}
+
+int tbk_stream_destroy(void* stream) { return (int)cudaStreamDestroy((cudaStream_t)stream); }
+
+int tbk_host_func(void* stream, void (*fn)(void*), void* arg)
+{
+    return (int)cudaLaunchHostFunc((cudaStream_t)stream, fn, arg);
+}
+
+int tbk_host_alloc(void** p, size_t bytes) { return (int)cudaMallocHost(p, bytes); }
+int tbk_host_free(void* p) { return (int)cudaFreeHost(p); }
+
+size_t tbk_group_bytes(int n) { return tb::group_descriptor_bytes(n); }
+
+int tbk_run_group(const tb_plan* const* plans, const tb_ptrs* ptrs, int n, void* host_desc, void* dev_desc,
+                  void* stream)
+{
+    for (int i = 0; i < n; i++)
+        if (plans[i]->path != TB_PATH_GENERIC || plans[i]->compute != plans[0]->compute)
+            return (int)cudaErrorInvalidValue;
+    return (int)tb::launch_generic_group(plans, ptrs, n, host_desc, dev_desc, (cudaStream_t)stream);
 }
 
 long long tbk_launch_count(void) { return tb::g_launches.load(); }

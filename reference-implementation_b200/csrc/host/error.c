@@ -48,6 +48,7 @@ static const char* message_of(TAPP_error error)
     case TAPP_B200_ERR_LABELS: return "A tensor has more modes than when the product was created.";
     case TAPP_B200_ERR_SCRATCH:
         return "The product needs more scratch memory than the 32 MiB array of the allocation-free entry point.";
+    case TAPP_B200_ERR_BUDGET: return "The product needs more device memory than the server's whole HBM budget.";
     default: return "Unknown error code.";
     }
 }

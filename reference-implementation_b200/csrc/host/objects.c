@@ -139,6 +139,10 @@ TAPP_error TAPP_attr_set(TAPP_attr attr, TAPP_key key, void* value)
     case TAPP_B200_ATTR_F32_MODE: e->f32_mode = value ? *(int*)value : 0; return 0;
     case TAPP_B200_ATTR_PATH: e->force_path = value ? *(int*)value : 0; return 0;
     case TAPP_B200_ATTR_WANT_STATUS: e->want_status = value ? *(int*)value : 0; return 0;
+    case TAPP_B200_ATTR_SERVER:
+        if (value && !tb_server_is_live((const struct tb_server*)value)) return TAPP_B200_ERR_INVALID;
+        e->server = (struct tb_server*)value;
+        return 0;
     default: return TAPP_B200_ERR_INVALID;
     }
 }
@@ -157,6 +161,7 @@ TAPP_error TAPP_attr_get(TAPP_attr attr, TAPP_key key, void** value)
         case TAPP_B200_ATTR_F32_MODE: *(int*)*value = e->f32_mode; return 0;
         case TAPP_B200_ATTR_PATH: *(int*)*value = e->force_path; return 0;
         case TAPP_B200_ATTR_WANT_STATUS: *(int*)*value = e->want_status; return 0;
+        case TAPP_B200_ATTR_SERVER: *value = e->server; return 0;
         default: return TAPP_B200_ERR_INVALID;
         }
     }
@@ -184,6 +189,7 @@ TAPP_error TAPP_attr_clear(TAPP_attr attr, TAPP_key key)
     case TAPP_B200_ATTR_F32_MODE: e->f32_mode = 0; return 0;
     case TAPP_B200_ATTR_PATH: e->force_path = 0; return 0;
     case TAPP_B200_ATTR_WANT_STATUS: e->want_status = 0; return 0;
+    case TAPP_B200_ATTR_SERVER: e->server = NULL; return 0;
     default: return TAPP_B200_ERR_INVALID;
     }
 }

@@ -64,14 +64,8 @@ TAPP_error TAPP_destroy_tensor_product(TAPP_tensor_product plan)
     return 0;
 }
 
-/* settings an execution runs with */
-typedef struct {
-    void* stream;
-    int async, f32_mode, force_path, want_status;
-} exec_settings;
-
 /* check_executor_existence, product.c:878-885 (code 33) */
-static int resolve_executor(TAPP_executor exec, exec_settings* s)
+static int resolve_executor(TAPP_executor exec, tb_exec_settings* s)
 {
     memset(s, 0, sizeof(*s));
     if (!exec) return 33;
@@ -82,13 +76,14 @@ static int resolve_executor(TAPP_executor exec, exec_settings* s)
         s->f32_mode = e->f32_mode;
         s->force_path = e->force_path;
         s->want_status = e->want_status;
+        s->server = e->server;
         return 0;
     }
     int id = *(const int*)exec;
     return (id == 1 || id == 2 || id == 12) ? 0 : 33;
 }
 
-static int views(struct tb_product* p, tb_tensor_view v[4])
+int tb_product_views(struct tb_product* p, tb_tensor_view v[4])
 {
     for (int k = 0; k < 4; k++) {
         const struct tb_info* t = (const struct tb_info*)p->info[k];
@@ -106,8 +101,8 @@ static int views(struct tb_product* p, tb_tensor_view v[4])
 /* Launch plans depend on the infos' contents, the scalars (rounded per
  * precision) and the executor's options; a cached plan is reused when all
  * of them match. */
-static int plan_for(struct tb_product* p, const tb_tensor_view v[4], const void* alpha, const void* beta,
-                    const exec_settings* s, tb_plan* out)
+int tb_product_plan(struct tb_product* p, const tb_tensor_view v[4], const void* alpha, const void* beta,
+                    const tb_exec_settings* s, tb_plan* out)
 {
     int64_t key[4 * (3 * 64 + 2) + 8];
     int n = 0, fits = 1;
@@ -154,7 +149,7 @@ static int plan_for(struct tb_product* p, const tb_tensor_view v[4], const void*
 }
 
 /* lowest and highest element offset a layout addresses; 0 if it addresses none */
-static int span_of(const tb_tensor_view* t, int64_t* lo, int64_t* hi)
+int tb_span_of(const tb_tensor_view* t, int64_t* lo, int64_t* hi)
 {
     *lo = *hi = 0;
     for (int i = 0; i < t->nmode; i++) {
@@ -166,7 +161,7 @@ static int span_of(const tb_tensor_view* t, int64_t* lo, int64_t* hi)
 }
 
 /* whether every element of the span is addressed (no holes) */
-static int span_dense(const tb_tensor_view* t, int64_t lo, int64_t hi)
+int tb_span_dense(const tb_tensor_view* t, int64_t lo, int64_t hi)
 {
     int64_t count = 1;
     for (int i = 0; i < t->nmode; i++) count *= t->extents[i];
@@ -216,7 +211,7 @@ static int stage_in(const tb_plan* P, const tb_tensor_view v[4], const void* ptr
             continue;
         }
         int64_t lo, hi;
-        if (!span_of(&v[k], &lo, &hi)) { outp[k] = (void*)ptr[k]; continue; }
+        if (!tb_span_of(&v[k], &lo, &hi)) { outp[k] = (void*)ptr[k]; continue; }
         const int eb = tb_elem_bytes(v[k].type);
         const size_t bytes = (size_t)(hi - lo + 1) * (size_t)eb;
         void* d = NULL;
@@ -228,7 +223,7 @@ static int stage_in(const tb_plan* P, const tb_tensor_view v[4], const void* ptr
         st->host[k] = ptr[k];
         st->staged_any = 1;
         const char* hsrc = (const char*)ptr[k] + lo * eb;
-        if (k < 3 || !span_dense(&v[k], lo, hi)) {
+        if (k < 3 || !tb_span_dense(&v[k], lo, hi)) {
             e = tbk_memcpy(d, hsrc, bytes, TBK_H2D, stream);
             if (e) return cuda_err(e);
         }
@@ -259,16 +254,25 @@ static int run(struct tb_product* p, TAPP_executor exec, TAPP_status* status, co
                const void* A, const void* B, const void* beta, const void* C, void* D)
 {
     tb_tensor_view v[4];
-    int err = views(p, v);
+    int err = tb_product_views(p, v);
     if (err) return err;
     err = tb_validate(&v[0], &v[1], &v[2], &v[3], beta, C != NULL);
     if (err) return err;
-    exec_settings s;
+    tb_exec_settings s;
     err = resolve_executor(exec, &s);
     if (err) return err;
+    if (s.server) {
+        if (!tb_server_is_live(s.server)) return TAPP_B200_ERR_INVALID;
+        /* the executor routes its products through a server: queue, then
+         * wait for this product's completion */
+        int64_t ticket = -1;
+        err = tb_server_enqueue(s.server, p, v, &s, alpha, A, B, beta, C, D, &ticket);
+        if (!err && ticket >= 0) err = tapp_b200_server_wait((TAPP_b200_server)s.server, ticket);
+        return err;
+    }
 
     tb_plan P;
-    err = plan_for(p, v, alpha, beta, &s, &P);
+    err = tb_product_plan(p, v, alpha, beta, &s, &P);
     if (err) return err;
 
     int kernels = 0;
@@ -336,17 +340,17 @@ TAPP_error TAPP_execute_batched_product(TAPP_tensor_product plan, TAPP_executor 
     if (num_batches < 0 || (num_batches > 0 && (!A || !B || !D))) return TAPP_B200_ERR_INVALID;
     if (num_batches == 0) return 0;
     tb_tensor_view v[4];
-    int err = views(p, v);
+    int err = tb_product_views(p, v);
     if (err) return err;
     for (int i = 0; i < num_batches; i++) {
         err = tb_validate(&v[0], &v[1], &v[2], &v[3], beta, C && C[i] != NULL);
         if (err) return err;
     }
-    exec_settings s;
+    tb_exec_settings s;
     err = resolve_executor(exec, &s);
     if (err) return err;
     tb_plan P;
-    err = plan_for(p, v, alpha, beta, &s, &P);
+    err = tb_product_plan(p, v, alpha, beta, &s, &P);
     if (err) return err;
     if (P.path == TB_PATH_NOOP) return 0;
 
@@ -406,8 +410,8 @@ size_t tapp_b200_describe_plan(TAPP_tensor_product plan, TAPP_executor exec, siz
     struct tb_product* p = (struct tb_product*)plan;
     if (!p || p->magic != TB_MAGIC_PRODUCT) return 0;
     tb_tensor_view v[4];
-    if (views(p, v)) return 0;
-    exec_settings s;
+    if (tb_product_views(p, v)) return 0;
+    tb_exec_settings s;
     memset(&s, 0, sizeof(s));
     if (exec) resolve_executor(exec, &s);
     /* beta = 1 in D's type so that C counts as read */

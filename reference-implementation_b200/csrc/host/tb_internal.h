@@ -36,6 +36,7 @@ struct tb_executor {
     int f32_mode;
     int force_path;
     int want_status;
+    struct tb_server* server;   /* TAPP_B200_ATTR_SERVER */
 };
 
 struct tb_handle {
@@ -111,5 +112,28 @@ size_t tb_describe(const tb_plan* p, size_t maxlen, char* out);
 double tb_plan_flops(const tb_plan* p);
 int tb_elem_bytes(TAPP_datatype t);
 int tb_is_complex(TAPP_datatype t);
+
+/* product.c: settings an execution runs with, and the steps of an
+ * execution that the server shares */
+typedef struct tb_exec_settings {
+    void* stream;
+    int async, f32_mode, force_path, want_status;
+    struct tb_server* server;
+} tb_exec_settings;
+
+int tb_product_views(struct tb_product* p, tb_tensor_view v[4]);
+int tb_product_plan(struct tb_product* p, const tb_tensor_view v[4], const void* alpha, const void* beta,
+                    const tb_exec_settings* s, tb_plan* out);
+/* lowest and highest element offset a layout addresses (0 if none), and
+ * whether every element in between is addressed */
+int tb_span_of(const tb_tensor_view* t, int64_t* lo, int64_t* hi);
+int tb_span_dense(const tb_tensor_view* t, int64_t lo, int64_t hi);
+
+/* server.c */
+struct tb_server;
+int tb_server_is_live(const struct tb_server* srv);
+int tb_server_enqueue(struct tb_server* srv, struct tb_product* p, const tb_tensor_view v[4],
+                      const tb_exec_settings* s, const void* alpha, const void* A, const void* B,
+                      const void* beta, const void* C, void* D, int64_t* ticket);
 
 #endif /* TB_INTERNAL_H_ */

@@ -43,6 +43,22 @@ int tbk_run_plan(const tb_plan* plan, const tb_ptrs* ptrs, void* stream, int* ke
  * where the path allows it. */
 int tbk_run_plan_batched(const tb_plan* plan, const tb_ptrs* ptrs, int num, void* stream, int* kernels);
 
+/* Streams (non-blocking) and host callbacks ordered on a stream; fn runs on
+ * a driver thread once the work before it has completed and must not call
+ * CUDA. */
+int tbk_stream_create(void** stream);
+int tbk_stream_destroy(void* stream);
+int tbk_host_func(void* stream, void (*fn)(void*), void* arg);
+int tbk_host_alloc(void** p, size_t bytes);   /* page-locked host memory */
+int tbk_host_free(void* p);
+
+/* One launch for n products of the CUDA-core element path that share a
+ * compute domain (tb_plan.compute). host_desc (page-locked) and dev_desc hold
+ * tbk_group_bytes(n) bytes each and must stay valid until the launch has run. */
+size_t tbk_group_bytes(int n);
+int tbk_run_group(const tb_plan* const* plans, const tb_ptrs* ptrs, int n, void* host_desc, void* dev_desc,
+                  void* stream);
+
 long long tbk_launch_count(void);
 
 /* Reads (and clears) the word kernels set when one of their bounded waits

@@ -12,6 +12,13 @@
   double_case             D[a,b,i,j] = sum_{e,f} A[a,b,e,f] B[e,f,i,j] + C,
                           a=b=e=f=160, i=j=40; |x| log-uniform in [1e-8, 1], random
                           sign (float64) or phase (complex double, conj(A))
+  served_stream           the request mix of the served configuration: 50% Tucker
+                          mode-n products (order-3/4 core, extents 8..256, factor
+                          rank 4..64, random mode), 30% binary contractions with
+                          2..6 indices of extent 4..96, 20% Hadamard plus
+                          contraction; 40% f32, 30% bf16-accum-f32, 20% f64, 10%
+                          complex float; specifications only (shapes, labels,
+                          scalars), the data come from the runner
 The data are synthetic stand-ins with the shapes and value distributions the
 benchmark configurations specify; nothing is read from disk.
 """
@@ -19,7 +26,10 @@ from __future__ import annotations
 
 import numpy as np
 
-from .abi import TAPP_F32, TAPP_F64, TAPP_C32, TAPP_C64, TAPP_F16, TAPP_BF16, TAPP_CONJUGATE
+from dataclasses import dataclass
+
+from .abi import (TAPP_F32, TAPP_F64, TAPP_C32, TAPP_C64, TAPP_F16, TAPP_BF16, TAPP_CONJUGATE, ELEM_BYTES,
+                  TAPP_DEFAULT_PREC, TAPP_F32F32_ACCUM_F32, TAPP_BF16BF16_ACCUM_F32)
 from .case import Case, Tensor, alloc, scalar, bf16_from_f32, NP_DTYPE
 
 L = {ch: ord(ch) for ch in "abcdefhijkuv"}
@@ -117,3 +127,104 @@ def double_case(rng, cplx=False, ab=160, ij=40, beta=1.0) -> Case:
     C = t("abij", [ab, ab, ij, ij])
     D = alloc(ty, [ab, ab, ij, ij], colmajor([ab, ab, ij, ij]), [L[c] for c in "abij"])
     return Case(A, B, C, D, scalar(ty, 1.0), scalar(ty, beta), -1, False, "double_" + ("c64" if cplx else "f64"))
+
+
+@dataclass
+class RequestSpec:
+    """One served product: storage type of all four tensors, precision,
+    extents and labels of A, B, C, D (dense column-major), scalars."""
+    kind: str
+    storage: int
+    prec: int
+    extents: tuple
+    idx: tuple
+    alpha: complex
+    beta: complex
+
+    def elems(self, k: int) -> int:
+        return int(np.prod(self.extents[k], dtype=np.int64))
+
+    def nbytes(self, k: int) -> int:
+        return self.elems(k) * ELEM_BYTES[self.storage]
+
+    def flops(self) -> float:
+        """2 |D| |K| (8 |D| |K| complex): the algorithmic count of the product."""
+        ext = {}
+        for e_list, i_list in zip(self.extents, self.idx):
+            for e, l in zip(e_list, i_list):
+                ext[l] = e
+        K = [l for l in set(self.idx[0]) & set(self.idx[1]) if l not in self.idx[3]]
+        k = float(np.prod([ext[l] for l in K])) if K else 1.0
+        f = 2.0 * self.elems(3) * k
+        return 4.0 * f if self.storage in (TAPP_C32, TAPP_C64) else f
+
+
+# (storage, precision) of the served mix, with its shares
+SERVED_TYPES = ((0.4, TAPP_F32, TAPP_F32F32_ACCUM_F32), (0.3, TAPP_F32, TAPP_BF16BF16_ACCUM_F32),
+                (0.2, TAPP_F64, TAPP_DEFAULT_PREC), (0.1, TAPP_C32, TAPP_DEFAULT_PREC))
+
+
+def _tucker(rng):
+    o = int(rng.integers(3, 5))
+    ext = [int(x) for x in rng.integers(8, 257, o)]
+    R = int(rng.integers(4, 65))
+    n = int(rng.integers(0, o))
+    core = list(range(o))
+    d_idx = list(core)
+    d_idx[n] = o
+    d_ext = list(ext)
+    d_ext[n] = R
+    return (ext, [R, ext[n]], d_ext, d_ext), (core, [o, n], d_idx, d_idx)
+
+
+def _three_way(rng, labels, nK, nH):
+    """Splits labels into contracted, Hadamard and free-in-A/B classes and
+    orders every tensor's labels at random."""
+    labels = list(labels)
+    rng.shuffle(labels)
+    K, H, rest = labels[:nK], labels[nK:nK + nH], labels[nK + nH:]
+    FA = [l for l in rest if rng.random() < 0.5]
+    FB = [l for l in rest if l not in FA]
+    A, B, D = K + H + FA, K + H + FB, H + FA + FB
+    for x in (A, B, D):
+        rng.shuffle(x)
+    return A, B, D
+
+
+def _binary(rng, hadamard: bool):
+    if hadamard:
+        nl = int(rng.integers(3, 7))
+        nH = int(rng.integers(1, nl - 1))
+        nK = int(rng.integers(1, nl - nH))
+    else:
+        nl = int(rng.integers(2, 7))
+        nH = 0
+        nK = int(rng.integers(1, nl))
+    ext = {l: int(rng.integers(4, 97)) for l in range(nl)}
+    A, B, D = _three_way(rng, range(nl), nK, nH)
+    e = lambda idx: [ext[l] for l in idx]
+    return (e(A), e(B), e(D), e(D)), (A, B, D, D)
+
+
+def served_stream(rng, n: int = 20000, max_tensor_bytes: int = 64 << 30) -> list:
+    """n request specifications of the served mix; shapes are redrawn until
+    every tensor of the request fits max_tensor_bytes."""
+    out = []
+    shares = np.cumsum([t[0] for t in SERVED_TYPES])
+    for _ in range(n):
+        u = rng.random()
+        kind = "tucker" if u < 0.5 else ("binary" if u < 0.8 else "hadamard")
+        v = rng.random()
+        _, storage, prec = SERVED_TYPES[int(np.searchsorted(shares, v, side="right"))]
+        eb = ELEM_BYTES[storage]
+        for _attempt in range(10000):
+            ext, idx = _tucker(rng) if kind == "tucker" else _binary(rng, kind == "hadamard")
+            if max(int(np.prod(e, dtype=np.int64)) for e in ext) * eb <= max_tensor_bytes:
+                break
+        if storage in (TAPP_C32, TAPP_C64):
+            a = complex(rng.uniform(-1, 1), rng.uniform(-1, 1))
+            b = complex(rng.uniform(-1, 1), rng.uniform(-1, 1))
+        else:
+            a, b = float(rng.uniform(-1, 1)), float(rng.uniform(-1, 1))
+        out.append(RequestSpec(kind, storage, prec, tuple(list(e) for e in ext), tuple(list(i) for i in idx), a, b))
+    return out
