@@ -127,8 +127,8 @@ TAPP_EXPORT TAPP_error tapp_b200_execute_product_noalloc(TAPP_tensor_product pla
  * own work has completed.
  *
  * Device memory charged against the budget: the staging copies of host
- * operands (as TAPP_execute_product stages them) and the tensor-core path's
- * packed panels. Device-resident operands are used in place and not charged.
+ * operands (as TAPP_execute_product stages them) and the scratch of the
+ * product's kernels (tensor-core panels, split-contraction sums). Device-resident operands are used in place and not charged.
  * A product that needs more than the whole budget is refused at submission
  * with TAPP_B200_ERR_BUDGET. alpha and beta are read at submission; the
  * operands must stay valid, and D untouched, until the product completes. Results are those TAPP_execute_product gives for the same product:

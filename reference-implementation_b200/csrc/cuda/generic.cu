@@ -201,11 +201,18 @@ __device__ __forceinline__ R warp_sum(R v)
     return v;
 }
 
-// one block per output element; the contracted range is split over threads
+// Few outputs, long contraction: block (x, y) sums the y-th chunk of the
+// contracted range of output x with all its threads (combined by warp
+// shuffles). With one chunk the block finishes the output itself; with
+// several, each chunk's sum goes to a workspace and k_reduce_final adds the
+// chunks in order and finishes, so the result does not depend on scheduling.
 template <typename R, bool CPLX>
-__global__ void __launch_bounds__(256) k_reduce(GenParams p, const void* A, const void* B, const void* C, void* D)
+__global__ void __launch_bounds__(256) k_reduce(GenParams p, const void* A, const void* B, const void* C, void* D,
+                                                int64_t chunk, R* ws)
 {
     __shared__ R red[2][8];
+    const int64_t kbeg = (int64_t)blockIdx.y * chunk;
+    const int64_t kend = kbeg + chunk < p.sizeK ? kbeg + chunk : p.sizeK;
     for (int64_t i = blockIdx.x; i < p.sizeF; i += gridDim.x) {
         int64_t oA = 0, oB = 0, oC = 0, oD = 0;
         int64_t r = i;
@@ -218,7 +225,7 @@ __global__ void __launch_bounds__(256) k_reduce(GenParams p, const void* A, cons
             oD += c * p.F_sD[j];
         }
         R sr = 0, si = 0;
-        for (int64_t k = threadIdx.x; k < p.sizeK; k += blockDim.x) {
+        for (int64_t k = kbeg + threadIdx.x; k < kend; k += blockDim.x) {
             uint32_t rk = (uint32_t)k;
             int64_t kA = oA, kB = oB;
             for (int j = 0; j < p.nK; j++) {
@@ -241,10 +248,53 @@ __global__ void __launch_bounds__(256) k_reduce(GenParams p, const void* A, cons
         if (threadIdx.x == 0) {
             R tr = 0, ti = 0;
             for (int j = 0; j < (int)(blockDim.x >> 5); j++) { tr += red[0][j]; ti += red[1][j]; }
-            finish<R, CPLX>(p, tr, ti, C, oC, D, oD);
+            if (ws) {
+                ws[(blockIdx.y * p.sizeF + i) * 2] = tr;
+                ws[(blockIdx.y * p.sizeF + i) * 2 + 1] = ti;
+            } else {
+                finish<R, CPLX>(p, tr, ti, C, oC, D, oD);
+            }
         }
         __syncthreads();
     }
+}
+
+template <typename R, bool CPLX>
+__global__ void __launch_bounds__(256) k_reduce_final(GenParams p, const void* C, void* D, int chunks, const R* ws)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < p.sizeF; i += (int64_t)gridDim.x * blockDim.x) {
+        int64_t oC = 0, oD = 0, r = i;
+        for (int j = 0; j < p.nF; j++) {
+            int64_t c = r % p.F_ext[j];
+            r /= p.F_ext[j];
+            oC += c * p.F_sC[j];
+            oD += c * p.F_sD[j];
+        }
+        R tr = 0, ti = 0;
+        for (int z = 0; z < chunks; z++) {
+            tr += ws[(z * p.sizeF + i) * 2];
+            ti += ws[(z * p.sizeF + i) * 2 + 1];
+        }
+        finish<R, CPLX>(p, tr, ti, C, oC, D, oD);
+    }
+}
+
+// chunks of the contraction for the reduction path: about 8 blocks per SM in
+// all, every chunk at least 2048 terms long
+static int reduce_chunks(int64_t outs, int64_t K)
+{
+    if (outs <= 0) return 1;
+    int64_t S = (148 * 8 + outs - 1) / outs;
+    const int64_t by_len = K / 2048;
+    if (S > by_len) S = by_len;
+    if (S > 4096) S = 4096;
+    return S < 1 ? 1 : (int)S;
+}
+
+size_t reduce_scratch_bytes(const tb_plan* P, size_t real_bytes)
+{
+    const int S = reduce_chunks(P->F.size, P->K.size);
+    return S > 1 ? (size_t)S * (size_t)P->F.size * 2 * real_bytes : 0;
 }
 
 static void fill_params(const tb_plan* P, GenParams& g)
@@ -278,8 +328,31 @@ template <typename R, bool CPLX>
 static cudaError_t launch_typed(const GenParams& g, int path, const tb_ptrs* d, cudaStream_t s)
 {
     if (path == TB_PATH_REDUCE && g.sizeK < (1ll << 31)) {
-        int64_t blocks = g.sizeF < 148 * 16 ? g.sizeF : 148 * 16;
-        k_reduce<R, CPLX><<<(unsigned)blocks, 256, 0, s>>>(g, d->A, d->B, d->C, d->D);
+        const int S = reduce_chunks(g.sizeF, g.sizeK);
+        int64_t bx = g.sizeF < 148 * 16 ? g.sizeF : 148 * 16;
+        if (bx < 1) bx = 1;
+        if (S == 1) {
+            k_reduce<R, CPLX><<<(unsigned)bx, 256, 0, s>>>(g, d->A, d->B, d->C, d->D, g.sizeK, (R*)nullptr);
+            count_launch();
+            return cudaGetLastError();
+        }
+        const int64_t chunk = (g.sizeK + S - 1) / S;
+        const int chunks = (int)((g.sizeK + chunk - 1) / chunk);
+        void* ws = nullptr;
+        cudaError_t e = pool_alloc(&ws, (size_t)chunks * (size_t)g.sizeF * 2 * sizeof(R), s);
+        if (e != cudaSuccess) return e;
+        k_reduce<R, CPLX><<<dim3((unsigned)bx, (unsigned)chunks), 256, 0, s>>>(g, d->A, d->B, d->C, d->D, chunk,
+                                                                            (R*)ws);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) {
+            int64_t b2 = (g.sizeF + 255) / 256;
+            if (b2 > 148 * 8) b2 = 148 * 8;
+            k_reduce_final<R, CPLX><<<(unsigned)b2, 256, 0, s>>>(g, d->C, d->D, chunks, (const R*)ws);
+            e = cudaGetLastError();
+        }
+        count_launch(2);
+        cudaFreeAsync(ws, s);
+        return e;
     } else {
         int64_t blocks = (g.sizeF + 255) / 256;
         if (blocks > 148 * 64) blocks = 148 * 64;

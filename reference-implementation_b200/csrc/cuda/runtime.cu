@@ -68,6 +68,8 @@ cudaError_t launch_generic(const tb_plan* P, const tb_ptrs* d, cudaStream_t s);
 cudaError_t launch_simt(const tb_plan* P, const tb_ptrs* d, cudaStream_t s);
 cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t s, int* kernels, void** main_timer);
 size_t group_descriptor_bytes(int n);
+size_t simt_scratch_bytes(const tb_plan* P);
+size_t reduce_scratch_bytes(const tb_plan* P, size_t real_bytes);
 cudaError_t launch_generic_group(const tb_plan* const* P, const tb_ptrs* d, int n, void* host, void* dev,
                                  cudaStream_t s);
 
@@ -244,6 +246,17 @@ int tbk_host_alloc(void** p, size_t bytes) { return (int)cudaMallocHost(p, bytes
 int tbk_host_free(void* p) { return (int)cudaFreeHost(p); }
 
 size_t tbk_group_bytes(int n) { return tb::group_descriptor_bytes(n); }
+
+size_t tbk_scratch_bytes(const tb_plan* plan)
+{
+    switch (plan->path) {
+    case TB_PATH_TC: return tbk_tc_scratch_bytes(plan);
+    case TB_PATH_SIMT: return tb::simt_scratch_bytes(plan);
+    case TB_PATH_REDUCE:
+        return tb::reduce_scratch_bytes(plan, plan->compute == TB_R32 || plan->compute == TB_C32 ? 4 : 8);
+    default: return 0;
+    }
+}
 
 int tbk_run_group(const tb_plan* const* plans, const tb_ptrs* ptrs, int n, void* host_desc, void* dev_desc,
                   void* stream)

@@ -347,7 +347,7 @@ int tb_build_plan(const tb_tensor_view* A, const tb_tensor_view* B,
     const int64_t outs = P->F.size, ksz = P->K.size;
     const double macs = (double)outs * (double)(ksz > 0 ? ksz : 1) * (double)P->UA.size * (double)P->UB.size;
     int path = TB_PATH_GENERIC;
-    if (outs < 4096 && ksz >= 512 && outs * 64 < ksz * 4)
+    if (outs < 4096 && ksz >= 512 && outs * 16 < ksz)
         path = TB_PATH_REDUCE;
 
     int tc_ok = 0;
@@ -365,7 +365,14 @@ int tb_build_plan(const tb_tensor_view* A, const tb_tensor_view* B,
     const int big = P->M.size >= 64 && P->N.size >= 64 && ksz >= 64 && macs >= 16.0 * 1024 * 1024;
     /* tiled CUDA-core GEMM: products without unary modes */
     const int simt_ok = P->UA.n == 0 && P->UB.n == 0 && ksz > 0 && P->UA.size == 1 && P->UB.size == 1;
-    const int simt_big = P->M.size >= 32 && P->N.size >= 32 && ksz >= 16 && macs >= 4.0 * 1024 * 1024;
+    /* the GEMM is turned so that its rows are the longer side; a long side of
+     * 16 fills its narrowest tile, a short side of 1 (matrix-vector) is fine */
+    const int64_t long_side = P->M.size > P->N.size ? P->M.size : P->N.size;
+    const int64_t short_side = P->M.size > P->N.size ? P->N.size : P->M.size;
+    /* many small batches of matrix-vector products fill tiles poorly: those
+     * stay on the element kernel */
+    const int simt_big = long_side >= 16 && ksz >= 8 && macs >= 1024.0 * 1024 &&
+                         (short_side >= 4 || P->L.size == 1);
     if (simt_ok && simt_big) path = TB_PATH_SIMT;
     if (tc_ok && big) path = TB_PATH_TC;
     if (opt && opt->force_path) {

@@ -437,7 +437,7 @@ int tb_server_enqueue(struct tb_server* s, struct tb_product* p, const tb_tensor
         r->eb[k] = tb_elem_bytes(v[k].type);
         r->need += round512((hi - lo + 1) * r->eb[k]);
     }
-    if (r->P.path == TB_PATH_TC) r->need += round512((int64_t)tbk_tc_scratch_bytes(&r->P));
+    r->need += round512((int64_t)tbk_scratch_bytes(&r->P));
     if (r->need > s->budget) {
         free(r);
         return TAPP_B200_ERR_BUDGET;

@@ -56,6 +56,8 @@ int tbk_host_free(void* p);
  * compute domain (tb_plan.compute). host_desc (page-locked) and dev_desc hold
  * tbk_group_bytes(n) bytes each and must stay valid until the launch has run. */
 size_t tbk_group_bytes(int n);
+/* device scratch one execution of the plan allocates from the pool */
+size_t tbk_scratch_bytes(const tb_plan* plan);
 int tbk_run_group(const tb_plan* const* plans, const tb_ptrs* ptrs, int n, void* host_desc, void* dev_desc,
                   void* stream);
 

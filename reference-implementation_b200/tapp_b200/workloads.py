@@ -228,3 +228,20 @@ def served_stream(rng, n: int = 20000, max_tensor_bytes: int = 64 << 30) -> list
             a, b = float(rng.uniform(-1, 1)), float(rng.uniform(-1, 1))
         out.append(RequestSpec(kind, storage, prec, tuple(list(e) for e in ext), tuple(list(i) for i in idx), a, b))
     return out
+
+
+def case_from_spec(rng, spec: RequestSpec) -> Case:
+    """A Case with the spec's shapes (dense column-major) and values uniform
+    in [-1, 1] (real and imaginary parts for complex storage)."""
+    ts = []
+    for k in range(4):
+        ext = list(spec.extents[k])
+        T = alloc(spec.storage, ext, colmajor(ext), list(spec.idx[k]))
+        n = T.buf.size
+        if spec.storage in (TAPP_C32, TAPP_C64):
+            T.buf[:] = rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)
+        else:
+            T.buf[:] = rng.uniform(-1, 1, n)
+        ts.append(T)
+    return Case(*ts, scalar(spec.storage, spec.alpha), scalar(spec.storage, spec.beta), spec.prec, False,
+                f"{spec.kind}")

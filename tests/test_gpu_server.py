@@ -135,9 +135,12 @@ def test_budget_backpressure_and_grouping(tapp, gpu):
 
 def test_refuses_product_beyond_budget(tapp, gpu):
     rng = np.random.default_rng(8)
-    case = dense_contraction_case(rng, extent=16)   # four 256 KiB host operands
+    # four 256 KiB host operands to stage, plus 1 MiB of split-contraction
+    # sums: 2 MiB in all, more than the budget; from device memory only the
+    # split sums count, and they fit
+    case = dense_contraction_case(rng, extent=16)
     prep = Prepared(tapp, case)
-    with Server(tapp, 512 * 1024) as srv:
+    with Server(tapp, 1536 * 1024) as srv:
         err, t = srv.submit(prep.plan, case.alpha.ctypes.data, case.A.ptr(), case.B.ptr(), case.beta.ctypes.data,
                             case.C.ptr(), case.D.ptr())
         assert err == ERR_BUDGET and t == -1

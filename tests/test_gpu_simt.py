@@ -112,3 +112,64 @@ def test_complex_double_4index_sampled(tapp, oracle, gpu):
     bound = n * 2.0 ** -53 * scale * 4 + 2 * 2.0 ** -53 * np.abs(D64)
     assert (np.abs(got - D64) <= bound).all()
     tapp.lib.TAPP_destroy_executor(ex)
+
+
+def spec_case(rng, storage, prec, extents, idx, kind="shape"):
+    from tapp_b200.workloads import RequestSpec, case_from_spec
+    cplx = storage in (2, 3)
+    a = complex(rng.uniform(-1, 1), rng.uniform(-1, 1)) if cplx else float(rng.uniform(-1, 1))
+    b = complex(rng.uniform(-1, 1), rng.uniform(-1, 1)) if cplx else float(rng.uniform(-1, 1))
+    return case_from_spec(rng, RequestSpec(kind, storage, prec, extents, idx, a, b))
+
+
+@pytest.mark.parametrize("storage,prec", [(0, 0), (0, 6), (1, -1), (2, -1), (3, -1)])
+@pytest.mark.parametrize("rank", [4, 12, 24, 40])
+def test_mode_n_products_narrow_tiles(tapp, oracle, gpu, storage, prec, rank):
+    """Tucker mode-n products D[i,r,k] = sum_j core[i,j,k] U[r,j] (and on the
+    first and last mode): N is the factor rank, so the narrow 128x16 and
+    128x32 tiles and the square tile all appear."""
+    rng = np.random.default_rng(70 + rank + 7 * storage + prec)
+    core = [101, 61, 43]
+    for mode in range(3):
+        d_ext = list(core)
+        d_ext[mode] = rank
+        d_idx = [0, 1, 2]
+        d_idx[mode] = 3
+        case = spec_case(rng, storage, prec, ([*core], [rank, core[mode]], d_ext, d_ext),
+                         ([0, 1, 2], [3, mode], d_idx, d_idx), "tucker")
+        ex = tapp.create_executor()
+        assert "path=simt" in describe(tapp, case, ex)
+        check_against_f64(tapp, oracle, case, device=bool(mode % 2), executor=ex)
+        tapp.lib.TAPP_destroy_executor(ex)
+
+
+@pytest.mark.parametrize("storage,prec", [(0, 0), (1, -1), (2, -1), (0, 6)])
+@pytest.mark.parametrize("turned", [False, True])
+def test_long_contraction_split(tapp, oracle, gpu, storage, prec, turned):
+    """Few output tiles and a long contraction: the contraction is split over
+    the grid and the splits are added by the final kernel. turned=True puts
+    the long side on B (the view is turned so that M >= N)."""
+    rng = np.random.default_rng(90 + storage + 3 * prec + int(turned))
+    A = ([12, 10, 30, 24], [0, 1, 4, 2])
+    B = ([14, 12, 24, 10], [3, 0, 2, 1])
+    D = ([14, 30], [3, 4])
+    if turned:
+        A, B = B, A
+    case = spec_case(rng, storage, prec, (A[0], B[0], D[0], D[0]), (A[1], B[1], D[1], D[1]))
+    ex = tapp.create_executor()
+    assert "path=simt" in describe(tapp, case, ex)
+    check_against_f64(tapp, oracle, case, device=True, executor=ex)
+    tapp.lib.TAPP_destroy_executor(ex)
+
+
+@pytest.mark.parametrize("storage,prec", [(0, 0), (1, -1), (2, -1), (3, -1), (0, 6)])
+def test_few_outputs_split_reduction(tapp, oracle, gpu, storage, prec):
+    """D[x] = sum_{a,b,c} A[a,x,b,c] B[c,a,b] with 5 outputs and 36000 terms
+    each: the reduction path with the contraction split over blocks."""
+    rng = np.random.default_rng(110 + storage + prec)
+    case = spec_case(rng, storage, prec, ([30, 5, 40, 30], [30, 30, 40], [5], [5]),
+                     ([0, 4, 1, 2], [2, 0, 1], [4], [4]))
+    ex = tapp.create_executor()
+    assert "path=reduce" in describe(tapp, case, ex)
+    check_against_f64(tapp, oracle, case, device=False, executor=ex)
+    tapp.lib.TAPP_destroy_executor(ex)
