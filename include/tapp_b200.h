@@ -47,7 +47,8 @@ enum {
      *     bfloat16 high and low part, three products accumulate in binary32. */
     TAPP_B200_ATTR_F32_MODE = 0x1002,
     /* value: int*. Force an execution path: 0 automatic (default),
-     * 1 CUDA-core element kernel, 3 tiled CUDA-core GEMM, 4 tensor cores. */
+     * 1 CUDA-core element kernel, 2 CUDA-core reduction, 3 tiled CUDA-core
+     * GEMM, 4 tensor cores, 5 sliced binary64 (needs TAPP_B200_ATTR_F64_MODE). */
     TAPP_B200_ATTR_PATH = 0x1004,
     /* value: int* (0/1). 1: TAPP_execute_product writes a status object to
      * *status, to be read with TAPP_attr_get and freed with
@@ -58,6 +59,19 @@ enum {
      * returns when the product has completed; concurrent callers (threads)
      * are batched together. Detach before destroying the server. */
     TAPP_B200_ATTR_SERVER = 0x1006,
+    /* value: int*. Arithmetic of binary64 and complex-double products
+     * (F64F64_ACCUM_F64, and DEFAULT on double data):
+     *   0 native binary64 on CUDA cores (default),
+     *   S in 2..16: sliced on the integer tensor cores. Every row of A and
+     *     column of B is scaled by a power of two and cut into S signed
+     *     7-bit digits; the digit products of total order < S are exact
+     *     32-bit integer sums, added up in binary64. The result errs by at
+     *     most about |alpha| K (S + 4) 2^(-7S) 2^(E_row + F_col) per element
+     *     (K contracted terms, 2K for complex; |A[row,:]| < 2^E_row,
+     *     |B[:,col]| < 2^F_col); S = 8 keeps about 56 bits of the largest
+     *     element of each row. Inputs must be finite (a row or column with
+     *     a non-finite value gives NaN). Environment: TAPP_B200_F64_MODE. */
+    TAPP_B200_ATTR_F64_MODE = 0x1007,
 };
 
 /* ---- keys readable from a status object with TAPP_attr_get ---- */
@@ -67,7 +81,8 @@ enum {
     TAPP_B200_STATUS_FLOPS = 0x1102,     /* double: algorithmic flops (2|D||K|, 8|D||K| complex) */
     TAPP_B200_STATUS_DEVICE_US = 0x1103, /* double: device time of the launches, microseconds
                                           * (synchronous executions only) */
-    TAPP_B200_STATUS_TC_MODE = 0x1104,   /* int: tensor-core operand mode (0 bf16, 1 f16, 2 split bf16) */
+    TAPP_B200_STATUS_TC_MODE = 0x1104,   /* int: tensor-core operand mode (0 bf16, 1 f16, 2 split bf16,
+                                          * 3 sliced 8-bit integer) */
     TAPP_B200_STATUS_MAIN_US = 0x1105,   /* double: device time of the dominant kernel (the tensor-core
                                           * GEMM, or the CUDA-core kernel), microseconds */
 };

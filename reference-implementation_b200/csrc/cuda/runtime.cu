@@ -69,6 +69,8 @@ cudaError_t launch_simt(const tb_plan* P, const tb_ptrs* d, cudaStream_t s);
 cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t s, int* kernels, void** main_timer);
 size_t group_descriptor_bytes(int n);
 size_t simt_scratch_bytes(const tb_plan* P);
+size_t sliced_scratch_bytes(const tb_plan* P);
+cudaError_t launch_sliced(const tb_plan* P, const tb_ptrs* d, cudaStream_t s, int* kernels, void** main_timer);
 size_t reduce_scratch_bytes(const tb_plan* P, size_t real_bytes);
 cudaError_t launch_generic_group(const tb_plan* const* P, const tb_ptrs* d, int n, void* host, void* dev,
                                  cudaStream_t s);
@@ -170,6 +172,7 @@ int tbk_run_plan(const tb_plan* plan, const tb_ptrs* ptrs, void* stream, int* ke
     switch (plan->path) {
     case TB_PATH_NOOP: return 0;
     case TB_PATH_TC: e = tb::launch_tc(plan, ptrs, 1, s, kernels, main_timer); break;
+    case TB_PATH_SLICED: e = tb::launch_sliced(plan, ptrs, s, kernels, main_timer); break;
     case TB_PATH_SIMT:
         if (main_timer) tbk_timer_begin(stream, main_timer);
         e = tb::launch_simt(plan, ptrs, s);
@@ -252,6 +255,7 @@ size_t tbk_scratch_bytes(const tb_plan* plan)
     switch (plan->path) {
     case TB_PATH_TC: return tbk_tc_scratch_bytes(plan);
     case TB_PATH_SIMT: return tb::simt_scratch_bytes(plan);
+    case TB_PATH_SLICED: return tb::sliced_scratch_bytes(plan);
     case TB_PATH_REDUCE:
         return tb::reduce_scratch_bytes(plan, plan->compute == TB_R32 || plan->compute == TB_C32 ? 4 : 8);
     default: return 0;

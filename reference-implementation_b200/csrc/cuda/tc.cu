@@ -377,6 +377,11 @@ struct EpiParams {
     float alpha_re, alpha_im, beta_re, beta_im;
     int64_t M, N, L;   // output sizes (N counts complex elements when cplx)
     ModeList mm, nn, ll;  // s0 = stride in C, s1 = stride in D
+    // EPI_I32 (integer slice products): W[l][m][n] = (first ? 0 : W) + level_scale * acc,
+    // W dense binary64 with N columns
+    double* W;
+    double level_scale;
+    int32_t w_first, w_pad;
 };
 
 struct GemmParams {
@@ -540,6 +545,27 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr)
     return d;
 }
 
+// signed 8-bit operands, 32-bit integer accumulators (exact)
+__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_i8_pair(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
 __device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t accumulate)
 {
     asm volatile(
@@ -616,7 +642,9 @@ __device__ __forceinline__ void finish_out(const EpiParams& e, int64_t offD, flo
 // EPI_ANY: every storage type, complex outputs, op_C / op_D.
 // EPI_TMA: like EPI_F32, with C and D moved by TMA tensor copies through a
 // per-warp shared-memory box (C and D expressible as tensor maps).
-enum { EPI_ANY = 0, EPI_F32 = 1, EPI_TMA = 2 };
+// EPI_I32: signed 8-bit operands (kind::i8, rows of 128 elements per stage),
+// 32-bit integer accumulators added into a binary64 workspace.
+enum { EPI_ANY = 0, EPI_F32 = 1, EPI_TMA = 2, EPI_I32 = 3 };
 
 template <int EPI, bool CTA2>
 __global__ void __launch_bounds__(NTHREADS, 1)
@@ -625,6 +653,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 {
     using G = Geo<CTA2>;
     constexpr int NS = G::stages;
+    constexpr int KSTEP = EPI == EPI_I32 ? 2 * BK : BK;  // elements per 128-byte stage row
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     // 1024-byte alignment by pointer arithmetic on the shared array (an
     // integer round trip would turn every access below into a generic one)
@@ -704,12 +733,12 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                         // both halves land on the leader's barrier, which expects the pair's bytes
                         const uint32_t fb = cluster_addr(&full[s], 0);
                         if (rank == 0) mbar_expect_tx(&full[s], 2 * G::stage_bytes);
-                        tma_load_3d_pair(a, &tmA, fb, kb * BK, tm * G::tile_m + (int)rank * BM, l);
-                        tma_load_3d_pair(a + G::a_bytes, &tmB, fb, kb * BK, tn * BN + (int)rank * G::b_rows, l);
+                        tma_load_3d_pair(a, &tmA, fb, kb * KSTEP, tm * G::tile_m + (int)rank * BM, l);
+                        tma_load_3d_pair(a + G::a_bytes, &tmB, fb, kb * KSTEP, tn * BN + (int)rank * G::b_rows, l);
                     } else {
                         mbar_expect_tx(&full[s], G::stage_bytes);
-                        tma_load_3d(a, &tmA, &full[s], kb * BK, tm * BM, l);
-                        tma_load_3d(a + G::a_bytes, &tmB, &full[s], kb * BK, tn * BN, l);
+                        tma_load_3d(a, &tmA, &full[s], kb * KSTEP, tm * BM, l);
+                        tma_load_3d(a + G::a_bytes, &tmB, &full[s], kb * KSTEP, tn * BN, l);
                     }
                     last_issued[s] = g;
                 }
@@ -748,9 +777,14 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                     const uint32_t a = smem_u32(tiles + s * G::stage_bytes);
                     const uint32_t b = a + G::a_bytes;
 #pragma unroll
-                    for (int k = 0; k < BK / 16; k++) {
-                        if (CTA2) mma_f16_pair(d_tmem, smem_desc(a + k * 32), smem_desc(b + k * 32), idesc, (kb | k) != 0);
-                        else mma_f16(d_tmem, smem_desc(a + k * 32), smem_desc(b + k * 32), idesc, (kb | k) != 0);
+                    for (int k = 0; k < BK / 16; k++) {  // 32 bytes of K per instruction
+                        if (EPI == EPI_I32) {
+                            if (CTA2) mma_i8_pair(d_tmem, smem_desc(a + k * 32), smem_desc(b + k * 32), idesc, (kb | k) != 0);
+                            else mma_i8(d_tmem, smem_desc(a + k * 32), smem_desc(b + k * 32), idesc, (kb | k) != 0);
+                        } else {
+                            if (CTA2) mma_f16_pair(d_tmem, smem_desc(a + k * 32), smem_desc(b + k * 32), idesc, (kb | k) != 0);
+                            else mma_f16(d_tmem, smem_desc(a + k * 32), smem_desc(b + k * 32), idesc, (kb | k) != 0);
+                        }
                     }
                     if (CTA2) mma_commit_pair(&empty[s]);
                     else mma_commit(&empty[s]);
@@ -798,7 +832,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             const int64_t row0 = (int64_t)tm * G::tile_m + (int64_t)rank * BM;  // this CTA's first row
             // column offsets of this tile (the TMA epilogue needs none: its
             // staging boxes share this memory)
-            for (int c = et; EPI != EPI_TMA && c < cols_out; c += EPI_THREADS) {
+            for (int c = et; EPI != EPI_TMA && EPI != EPI_I32 && c < cols_out; c += EPI_THREADS) {
                 const int64_t n = (int64_t)tn * cols_out + c;
                 int64_t oc = 0, od = 0;
                 if (n < e.N) decode2(e.nn, n, oc, od);
@@ -905,6 +939,58 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                     __syncwarp();
                     if (!cok) ok = false;
                     if (t + 1 < nch && ok) issue_c(t + 1);
+                }
+                fence_before();
+                release_acc(acc);
+                epi_bar();
+                continue;
+            }
+            if (EPI == EPI_I32) {
+                // integer products of one level of slices: scaled exactly by a
+                // power of two and added into the binary64 workspace row m
+                if (et == 0) *epi_ok = mbar_wait(&tfull[acc], aph, abort_flag) ? 1 : 0;
+                epi_bar();
+                const bool ok = *epi_ok != 0;
+                fence_after();
+                if (ok) {
+                    const double sc = e.level_scale;
+                    const bool first = e.w_first != 0;
+                    double* wrow = e.W + ((int64_t)l * e.M + m) * e.N;
+                    const bool pairs = (e.N & 1) == 0;
+#pragma unroll 1
+                    for (int t = 0; t < BN / 64; t++) {
+                        const int ch = half + 2 * t;
+                        uint32_t r[32];
+                        __syncwarp();
+                        tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + acc * BN + ch * 32, r);
+                        const int64_t c0 = (int64_t)tn * BN + ch * 32;
+                        if (!mok || c0 >= e.N) {
+                        } else if (pairs && c0 + 32 <= e.N) {
+                            double2* w2 = (double2*)(wrow + c0);
+                            double2 old[16];
+                            if (!first) {
+#pragma unroll
+                                for (int j = 0; j < 16; j++) old[j] = w2[j];
+                            }
+#pragma unroll
+                            for (int j = 0; j < 16; j++) {
+                                double2 v;
+                                v.x = (double)(int)r[2 * j] * sc;
+                                v.y = (double)(int)r[2 * j + 1] * sc;
+                                if (!first) {
+                                    v.x += old[j].x;
+                                    v.y += old[j].y;
+                                }
+                                w2[j] = v;
+                            }
+                        } else {
+                            for (int j = 0; j < 32 && c0 + j < e.N; j++) {
+                                double v = (double)(int)r[j] * sc;
+                                if (!first) v += wrow[c0 + j];
+                                wrow[c0 + j] = v;
+                            }
+                        }
+                    }
                 }
                 fence_before();
                 release_acc(acc);
@@ -1140,9 +1226,13 @@ static cudaError_t launch_gemm(int kind, bool cta2, int grid, const CUtensorMap&
                                cudaStream_t s)
 {
     void (*kern)(CUtensorMap, CUtensorMap, GemmParams, uint32_t, CUtensorMap, CUtensorMap);
-    if (cta2) kern = kind == EPI_TMA ? k_gemm<EPI_TMA, true> : kind == EPI_F32 ? k_gemm<EPI_F32, true> : k_gemm<EPI_ANY, true>;
-    else kern = kind == EPI_TMA ? k_gemm<EPI_TMA, false> : kind == EPI_F32 ? k_gemm<EPI_F32, false> : k_gemm<EPI_ANY, false>;
-    static int attr_done[64][3][2];
+    if (cta2)
+        kern = kind == EPI_TMA ? k_gemm<EPI_TMA, true> : kind == EPI_F32 ? k_gemm<EPI_F32, true>
+               : kind == EPI_I32 ? k_gemm<EPI_I32, true> : k_gemm<EPI_ANY, true>;
+    else
+        kern = kind == EPI_TMA ? k_gemm<EPI_TMA, false> : kind == EPI_F32 ? k_gemm<EPI_F32, false>
+               : kind == EPI_I32 ? k_gemm<EPI_I32, false> : k_gemm<EPI_ANY, false>;
+    static int attr_done[64][4][2];
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64 || !attr_done[dev][kind][cta2]) {
@@ -1165,7 +1255,63 @@ static cudaError_t launch_gemm(int kind, bool cta2, int grid, const CUtensorMap&
     return cudaLaunchKernelEx(&cfg, kern, tmA, tmB, gp, idesc, tmC, tmD);
 }
 
+// Tensor map of an 8-bit panel view: rows of `kext` bytes (the K range one
+// GEMM reads) `row_bytes` apart, `rows` rows per batch, L batches.
+static bool make_map_i8(CUtensorMap* tm, const void* base, uint64_t kext, uint64_t row_bytes, uint64_t rows,
+                        uint64_t L, uint32_t box_rows)
+{
+    EncodeTiledFn enc = encode_fn();
+    if (!enc || ((uintptr_t)base & 15) || (row_bytes & 15) || (kext & 15)) return false;
+    cuuint64_t dims[3] = {kext, rows, L};
+    cuuint64_t strides[2] = {row_bytes, row_bytes * rows};
+    cuuint32_t box[3] = {(cuuint32_t)(2 * BK), box_rows, 1};
+    cuuint32_t es[3] = {1, 1, 1};
+    return enc(tm, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void*>(base), dims, strides, box, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 }  // namespace tc
+
+// One integer GEMM over 8-bit slice panels: A8 [L][M][row_bytes] and B8
+// [L][Nout][row_bytes] bytes, each GEMM reading `klen` bytes per row from
+// byte a_off (A) and b_off (B) on; W[l][m][n] (+)= scale * sum. |sum| must
+// stay below 2^31 (the caller bounds the number of terms).
+cudaError_t launch_gemm_i8(const void* A8, const void* B8, int64_t row_bytes, int64_t M, int64_t Nout, int64_t L,
+                           int64_t a_off, int64_t b_off, int64_t klen, double* W, double scale, int first,
+                           cudaStream_t s)
+{
+    using namespace tc;
+    int* flag = device_error_word();
+    if (!flag) return cudaErrorMemoryAllocation;
+    const bool cta2 = M >= 2 * BM && num_sms() % 2 == 0;
+    CUtensorMap tmA, tmB;
+    if (!make_map_i8(&tmA, (const char*)A8 + a_off, (uint64_t)klen, (uint64_t)row_bytes, (uint64_t)M, (uint64_t)L, BM) ||
+        !make_map_i8(&tmB, (const char*)B8 + b_off, (uint64_t)klen, (uint64_t)row_bytes, (uint64_t)Nout, (uint64_t)L,
+                     cta2 ? Geo<true>::b_rows : BN))
+        return cudaErrorInvalidValue;
+    GemmParams gp;
+    memset(&gp, 0, sizeof(gp));
+    gp.tiles_m = (int)((M + (cta2 ? 2 * BM : BM) - 1) / (cta2 ? 2 * BM : BM));
+    gp.tiles_n = (int)((Nout + BN - 1) / BN);
+    gp.num_tiles = gp.tiles_m * gp.tiles_n * (int)L;
+    gp.num_kb = (int)((klen + 2 * BK - 1) / (2 * BK));
+    gp.error = flag;
+    gp.e.M = M;
+    gp.e.N = Nout;
+    gp.e.L = L;
+    gp.e.W = W;
+    gp.e.level_scale = scale;
+    gp.e.w_first = first;
+    const uint32_t mma_m = cta2 ? 2 * BM : BM;
+    // D: signed 32-bit (2), A and B: signed 8-bit (1)
+    const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((mma_m >> 4) << 24);
+    const int units = cta2 ? num_sms() / 2 : num_sms();
+    const int grid = (gp.num_tiles < units ? gp.num_tiles : units) * (cta2 ? 2 : 1);
+    cudaError_t e = launch_gemm(EPI_I32, cta2, grid, tmA, tmB, gp, idesc, tmA, tmA, s);
+    count_launch();
+    return e;
+}
 
 cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t s, int* kernels, void** main_timer)
 {

@@ -57,7 +57,7 @@ TAPP_error tapp_b200_execute_product_noalloc(TAPP_tensor_product plan, TAPP_exec
     }
 
     tb_plan P;
-    tb_plan_options opt = {f32_mode, TB_PATH_TC};
+    tb_plan_options opt = {f32_mode, TB_PATH_TC, 0};
     err = tb_build_plan(&v[0], &v[1], &v[2], &v[3], p->prec, alpha, beta, &opt, &P);
     if (err) return err;
     if (P.path == TB_PATH_NOOP) return 0;

@@ -96,6 +96,8 @@ TAPP_error TAPP_create_executor(TAPP_executor* exec)
     e->id = 1;
     e->f32_mode = env_int("TAPP_B200_F32_MODE", 0);
     e->force_path = env_int("TAPP_B200_PATH", 0);
+    e->f64_mode = env_int("TAPP_B200_F64_MODE", 0);
+    if (e->f64_mode < 2 || e->f64_mode > 16) e->f64_mode = 0;
     *exec = (TAPP_executor)e;
     reg_add(exec_reg, &exec_n, *exec);
     return 0;
@@ -139,6 +141,12 @@ TAPP_error TAPP_attr_set(TAPP_attr attr, TAPP_key key, void* value)
     case TAPP_B200_ATTR_F32_MODE: e->f32_mode = value ? *(int*)value : 0; return 0;
     case TAPP_B200_ATTR_PATH: e->force_path = value ? *(int*)value : 0; return 0;
     case TAPP_B200_ATTR_WANT_STATUS: e->want_status = value ? *(int*)value : 0; return 0;
+    case TAPP_B200_ATTR_F64_MODE: {
+        const int v = value ? *(int*)value : 0;
+        if (v != 0 && (v < 2 || v > 16)) return TAPP_B200_ERR_INVALID;
+        e->f64_mode = v;
+        return 0;
+    }
     case TAPP_B200_ATTR_SERVER:
         if (value && !tb_server_is_live((const struct tb_server*)value)) return TAPP_B200_ERR_INVALID;
         e->server = (struct tb_server*)value;
@@ -162,6 +170,7 @@ TAPP_error TAPP_attr_get(TAPP_attr attr, TAPP_key key, void** value)
         case TAPP_B200_ATTR_PATH: *(int*)*value = e->force_path; return 0;
         case TAPP_B200_ATTR_WANT_STATUS: *(int*)*value = e->want_status; return 0;
         case TAPP_B200_ATTR_SERVER: *value = e->server; return 0;
+        case TAPP_B200_ATTR_F64_MODE: *(int*)*value = e->f64_mode; return 0;
         default: return TAPP_B200_ERR_INVALID;
         }
     }
@@ -190,6 +199,7 @@ TAPP_error TAPP_attr_clear(TAPP_attr attr, TAPP_key key)
     case TAPP_B200_ATTR_PATH: e->force_path = 0; return 0;
     case TAPP_B200_ATTR_WANT_STATUS: e->want_status = 0; return 0;
     case TAPP_B200_ATTR_SERVER: e->server = NULL; return 0;
+    case TAPP_B200_ATTR_F64_MODE: e->f64_mode = 0; return 0;
     default: return TAPP_B200_ERR_INVALID;
     }
 }

@@ -375,10 +375,25 @@ int tb_build_plan(const tb_tensor_view* A, const tb_tensor_view* B,
                          (short_side >= 4 || P->L.size == 1);
     if (simt_ok && simt_big) path = TB_PATH_SIMT;
     if (tc_ok && big) path = TB_PATH_TC;
+    /* sliced binary64: digit panels must fit the slicing grid (batch in
+     * grid.z, 64-byte column tiles in grid.y) */
+    const int64_t kreal = ksz * (P->compute == TB_C64 ? 2 : 1);
+    const int sliced_ok = (P->compute == TB_R64 || P->compute == TB_C64) && opt && opt->f64_mode >= 2 &&
+                          opt->f64_mode <= 16 && simt_ok && P->L.size <= 65535 && (kreal + 15) / 16 * 16 / 64 < 65535 &&
+                          (double)((P->M.size + 255) / 256) * (double)((P->N.size * 2 + 255) / 256) * (double)P->L.size < 1e9;
+    if (sliced_ok) P->slices = opt->f64_mode;
+    if (sliced_ok && big) {
+        path = TB_PATH_SLICED;
+        P->tc_mode = TB_TC_SLICED_I8;
+    }
     if (opt && opt->force_path) {
         int f = opt->force_path;
         if (f == TB_PATH_TC && tc_ok) path = TB_PATH_TC;
         else if (f == TB_PATH_SIMT && simt_ok) path = TB_PATH_SIMT;
+        else if (f == TB_PATH_SLICED && sliced_ok) {
+            path = TB_PATH_SLICED;
+            P->tc_mode = TB_TC_SLICED_I8;
+        }
         else if (f == TB_PATH_GENERIC || f == TB_PATH_REDUCE) path = f;
     }
     P->path = path;
@@ -414,14 +429,15 @@ static size_t put_modes(char* out, size_t maxlen, size_t at, const char* name, c
 /* Text form of a plan; modes print as (extent:strideA,strideB,strideC,strideD). */
 size_t tb_describe(const tb_plan* p, size_t maxlen, char* out)
 {
-    static const char* paths[] = {"noop", "generic", "reduce", "simt", "tc"};
+    static const char* paths[] = {"noop", "generic", "reduce", "simt", "tc", "sliced"};
     static const char* comp[] = {"r32", "r64", "c32", "c64"};
-    static const char* tcm[] = {"bf16", "f16", "split_bf16"};
+    static const char* tcm[] = {"bf16", "f16", "split_bf16", "sliced_i8"};
     size_t at = 0;
     at = put(out, maxlen, at, "path=%s compute=%s prec=%d round_in=%d conj=%d%d%d%d beta_zero=%d",
              paths[p->path], comp[p->compute], p->prec, p->round_in, p->conjA, p->conjB, p->conjC, p->conjD,
              p->beta_zero);
     if (p->path == TB_PATH_TC) at = put(out, maxlen, at, " tc_mode=%s", tcm[p->tc_mode]);
+    if (p->path == TB_PATH_SLICED) at = put(out, maxlen, at, " slices=%d", p->slices);
     at = put_modes(out, maxlen, at, "F", &p->F);
     at = put_modes(out, maxlen, at, "K", &p->K);
     at = put_modes(out, maxlen, at, "UA", &p->UA);

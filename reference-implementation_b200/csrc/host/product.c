@@ -77,6 +77,7 @@ static int resolve_executor(TAPP_executor exec, tb_exec_settings* s)
         s->force_path = e->force_path;
         s->want_status = e->want_status;
         s->server = e->server;
+        s->f64_mode = e->f64_mode;
         return 0;
     }
     int id = *(const int*)exec;
@@ -115,13 +116,13 @@ int tb_product_plan(struct tb_product* p, const tb_tensor_view v[4], const void*
             key[n++] = v[k].strides[i];
         }
     }
-    tb_plan_options opt = {s->f32_mode, s->force_path};
+    tb_plan_options opt = {s->f32_mode, s->force_path, s->f64_mode};
     int err;
     if (fits) {
         pthread_mutex_lock(&p->lock);
         struct tb_plan_cache* c = &p->cache;
         if (c->valid && c->key_len == n && !memcmp(c->key, key, sizeof(int64_t) * (size_t)n) &&
-            c->f32_mode == s->f32_mode && c->force_path == s->force_path) {
+            c->f32_mode == s->f32_mode && c->force_path == s->force_path && c->f64_mode == s->f64_mode) {
             *out = c->plan;
             pthread_mutex_unlock(&p->lock);
             /* scalars may change per call; beta's zero-ness changes the plan */
@@ -141,6 +142,7 @@ int tb_product_plan(struct tb_product* p, const tb_tensor_view v[4], const void*
         c->key_len = n;
         c->f32_mode = s->f32_mode;
         c->force_path = s->force_path;
+        c->f64_mode = s->f64_mode;
         c->plan = *out;
         c->valid = 1;
     }
@@ -297,7 +299,7 @@ static int run(struct tb_product* p, TAPP_executor exec, TAPP_status* status, co
         if (!s.async || st.staged_any) {
             int e = tbk_stream_sync(s.stream);
             if (!err && e) err = cuda_err(e);
-            if (!err && P.path == TB_PATH_TC && (e = tbk_check_device_error())) err = cuda_err(e);
+            if (!err && (P.path == TB_PATH_TC || P.path == TB_PATH_SLICED) && (e = tbk_check_device_error())) err = cuda_err(e);
         }
         if (timer) tbk_timer_elapsed_us(timer, &dev_us);
         if (main_timer) tbk_timer_elapsed_us(main_timer, &main_us);
@@ -383,7 +385,7 @@ TAPP_error TAPP_execute_batched_product(TAPP_tensor_product plan, TAPP_executor 
         if (!s.async) {
             e = tbk_stream_sync(s.stream);
             if (e) return cuda_err(e);
-            if (P.path == TB_PATH_TC && (e = tbk_check_device_error())) return cuda_err(e);
+            if ((P.path == TB_PATH_TC || P.path == TB_PATH_SLICED) && (e = tbk_check_device_error())) return cuda_err(e);
         }
         if (s.want_status && status) {
             struct tb_status* so = calloc(1, sizeof(*so));
@@ -425,7 +427,7 @@ size_t tapp_b200_describe_plan(TAPP_tensor_product plan, TAPP_executor exec, siz
     default: break;
     }
     tb_plan P;
-    tb_plan_options opt = {s.f32_mode, s.force_path};
+    tb_plan_options opt = {s.f32_mode, s.force_path, s.f64_mode};
     if (tb_build_plan(&v[0], &v[1], &v[2], &v[3], p->prec, &one, &one, &opt, &P)) return 0;
     return tb_describe(&P, maxlen, out);
 }

@@ -268,7 +268,7 @@ static void issue(struct tb_server* s, srv_unit* u)
     s->units++;
     if (u->n > 1) s->grouped += u->n;
     for (int i = 0; i < u->n; i++)
-        if (u->req[i]->P.path == TB_PATH_TC) s->tc_ran = 1;
+        if (u->req[i]->P.path == TB_PATH_TC || u->req[i]->P.path == TB_PATH_SLICED) s->tc_ran = 1;
     pthread_mutex_unlock(&s->lock);
     if (tbk_host_func(stream, unit_done, u)) {
         tbk_stream_sync(stream);
@@ -461,7 +461,7 @@ int tb_server_enqueue(struct tb_server* s, struct tb_product* p, const tb_tensor
     memset(rc, 0, sizeof(*rc));
     rc->t_submit = t;
     rc->flops = tb_plan_flops(&r->P);
-    rc->tc = r->P.path == TB_PATH_TC;
+    rc->tc = r->P.path == TB_PATH_TC || r->P.path == TB_PATH_SLICED;
     if (!s->submitted) s->t_first = t;
     s->submitted++;
     *ticket = r->ticket;

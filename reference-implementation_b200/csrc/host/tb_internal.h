@@ -37,6 +37,7 @@ struct tb_executor {
     int force_path;
     int want_status;
     struct tb_server* server;   /* TAPP_B200_ATTR_SERVER */
+    int f64_mode;               /* TAPP_B200_ATTR_F64_MODE */
 };
 
 struct tb_handle {
@@ -59,7 +60,7 @@ struct tb_plan_cache {
     int valid;
     int key_len;
     int64_t* key;
-    int f32_mode, force_path;
+    int f32_mode, force_path, f64_mode;
     tb_plan plan;
 };
 
@@ -101,6 +102,7 @@ int tb_scalar_is_zero(const void* s, TAPP_datatype t);
 typedef struct tb_plan_options {
     int f32_mode;     /* TAPP_B200_ATTR_F32_MODE */
     int force_path;   /* TAPP_B200_ATTR_PATH */
+    int f64_mode;     /* TAPP_B200_ATTR_F64_MODE: 0 native, S >= 2 sliced */
 } tb_plan_options;
 
 int tb_build_plan(const tb_tensor_view* A, const tb_tensor_view* B,
@@ -119,6 +121,7 @@ typedef struct tb_exec_settings {
     void* stream;
     int async, f32_mode, force_path, want_status;
     struct tb_server* server;
+    int f64_mode;
 } tb_exec_settings;
 
 int tb_product_views(struct tb_product* p, tb_tensor_view v[4]);

@@ -37,9 +37,10 @@ enum {
     TB_PATH_REDUCE = 2,    /* CUDA-core kernel, one block per element of D (long K) */
     TB_PATH_SIMT = 3,      /* tiled CUDA-core GEMM over the L/M/N/K view */
     TB_PATH_TC = 4,        /* pack pre-pass + tcgen05 GEMM + fused epilogue */
+    TB_PATH_SLICED = 5,    /* binary64 as 8-bit digit slices on the integer tensor cores */
 };
 /* tensor-core operand modes */
-enum { TB_TC_BF16 = 0, TB_TC_F16 = 1, TB_TC_SPLIT_BF16 = 2 };
+enum { TB_TC_BF16 = 0, TB_TC_F16 = 1, TB_TC_SPLIT_BF16 = 2, TB_TC_SLICED_I8 = 3 };
 
 typedef struct tb_modes {
     int32_t n;
@@ -64,7 +65,7 @@ typedef struct tb_plan {
     int32_t beta_zero;            /* C is not read */
     int32_t path;
     int32_t tc_mode;              /* TB_TC_* */
-    int32_t reserved0;
+    int32_t slices;               /* TB_PATH_SLICED: digit slices per operand */
     double alpha_re, alpha_im;    /* scalars, already rounded per precision */
     double beta_re, beta_im;
     tb_modes F;                   /* free modes, sorted by |stride in D| */

@@ -60,3 +60,28 @@ def test_unknown_handles_are_refused(lib, tapp):
 def test_budget_code_text(tapp):
     assert "budget" in tapp.explain(ERR_BUDGET)
     assert not tapp.lib.TAPP_check_success(ERR_BUDGET)
+
+
+def test_f64_mode_attribute(tapp):
+    """TAPP_B200_ATTR_F64_MODE: 0 or 2..16 slices; the planner takes the sliced
+    path for large binary64 products only when it is set."""
+    import numpy as np
+    from tapp_b200.workloads import double_case
+    ex = tapp.create_executor()
+    for bad in (1, 17, -3):
+        assert tapp.set_int(ex, 0x1007, bad) == tapp_b200.ERR_INVALID
+    case = double_case(np.random.default_rng(0), cplx=True, ab=16, ij=16)
+    infos = [tapp.tensor_info(t.dtype, t.extents, t.strides)[1] for t in (case.A, case.B, case.C, case.D)]
+    _, plan = tapp.create_product(0, [t.op for t in (case.A, case.B, case.C, case.D)], infos,
+                                  [case.A.idx, case.B.idx, case.C.idx, case.D.idx], -1)
+    assert "path=simt" in tapp.describe(plan, ex)
+    assert tapp.set_int(ex, 0x1007, 8) == 0
+    d = tapp.describe(plan, ex)
+    assert "path=sliced" in d and "slices=8" in d and "compute=c64" in d
+    box = C.c_int(0)
+    p = C.c_void_p(C.addressof(box))
+    assert tapp.lib.TAPP_attr_get(ex, 0x1007, C.byref(p)) == 0 and box.value == 8
+    assert tapp.lib.TAPP_attr_clear(ex, 0x1007) == 0
+    assert "path=simt" in tapp.describe(plan, ex)
+    tapp.lib.TAPP_destroy_tensor_product(plan)
+    tapp.lib.TAPP_destroy_executor(ex)
