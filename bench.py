@@ -68,6 +68,11 @@ def parse():
     ap.add_argument("--served", type=int, default=1000,
                     help="requests in the served-stream measurement (0 skips it)")
     ap.add_argument("--only-served", action="store_true", help="print only the served-stream measurement")
+    ap.add_argument("--no-double", action="store_true", help="skip the binary64 / complex-double measurement")
+    ap.add_argument("--only-double", action="store_true", help="print only the binary64 / complex-double measurement")
+    ap.add_argument("--slices", type=str, default="7,8", help="digit slices of the sliced binary64 runs")
+    ap.add_argument("--double-ab", type=int, default=160, help="extent of a, b, e, f in the binary64 workload")
+    ap.add_argument("--double-ij", type=int, default=40, help="extent of i, j in the binary64 workload")
     ap.add_argument("--only-headline", action="store_true",
                     help="run only the timed headline steps (for profiling); prints its timing")
     return ap.parse_args()
@@ -356,6 +361,109 @@ def slab_values(case_D, dbuf, j_count=2):
     return dbuf[case_D.base + sub.offsets()].astype(np.float64)
 
 
+C4_AB, C4_IJ = 160, 40
+
+
+def double_measure(lib, torch, slices_list=(7, 8), steps=2, samples=256, ab=C4_AB, ij=C4_IJ):
+    """The binary64 configuration: D[a,b,i,j] = sum_{e,f} A[a,b,e,f] B[e,f,i,j] + C
+    with a = b = e = f = 160 and i = j = 40 (M = K = 25600, N = 1600), once in
+    binary64 and once in complex double with conj(A); |x| log-uniform in
+    [1e-8, 1] with random sign (phase), beta = 1; synthetic, generated on the
+    GPU. Native binary64 CUDA-core path against the sliced path (S 8-bit digit
+    slices on the integer tensor cores). Error: max |D - D_ref| / max |D_ref|
+    over sampled outputs, D_ref accumulated in extended precision (numpy
+    longdouble) from the same inputs."""
+    import math
+    import tapp_b200
+    from tapp_b200.case import Case, Tensor, scalar
+    from tapp_b200.abi import TAPP_F64, TAPP_C64, TAPP_CONJUGATE
+    M, N, K = ab * ab, ij * ij, ab * ab
+    g = torch.Generator(device="cuda")
+    g.manual_seed(4)
+    rng = np.random.default_rng(44)
+    out = {}
+    for cplx in (False, True):
+        dt = torch.complex128 if cplx else torch.float64
+
+        def logu(n):
+            mag = torch.pow(10.0, torch.rand(n, dtype=torch.float64, device="cuda", generator=g) * 8 - 8)
+            if cplx:
+                ph = torch.rand(n, dtype=torch.float64, device="cuda", generator=g) * (2 * math.pi)
+                return torch.polar(mag, ph)
+            return mag * torch.where(torch.rand(n, device="cuda", generator=g) < 0.5, -1.0, 1.0).to(torch.float64)
+
+        A, B, Cc = logu(M * K), logu(K * N), logu(M * N)
+        D = torch.zeros(M * N, dtype=dt, device="cuda")
+        ty = TAPP_C64 if cplx else TAPP_F64
+
+        def T(ext, idx, op=0):
+            st, acc = [], 1
+            for e_ in ext:
+                st.append(acc)
+                acc *= e_
+            return Tensor(ty, ext, st, [ord(c) for c in idx], op, None, 0)
+
+        case = Case(T([ab] * 4, "abef", TAPP_CONJUGATE if cplx else 0), T([ab, ab, ij, ij], "efij"),
+                    T([ab, ab, ij, ij], "abij"), T([ab, ab, ij, ij], "abij"), scalar(ty, 1.0), scalar(ty, 1.0), -1)
+        ptrs = [A.data_ptr(), B.data_ptr(), Cc.data_ptr(), D.data_ptr()]
+        flops = 2.0 * M * N * K * (4 if cplx else 1)
+        ms = rng.integers(0, M, samples)
+        ns = rng.integers(0, N, samples)
+        a_rows = A.view(K, M)[:, torch.from_numpy(ms).cuda()].cpu().numpy()        # [k, sample]
+        b_cols = B.view(N, K)[torch.from_numpy(ns).cuda(), :].cpu().numpy()        # [sample, k]
+        c_vals = Cc.view(N, M)[torch.from_numpy(ns).cuda(), torch.from_numpy(ms).cuda()].cpu().numpy()
+        ld = np.clongdouble if cplx else np.longdouble
+        ref = np.empty(samples, dtype=ld)
+        for i in range(samples):
+            a = a_rows[:, i].astype(ld)
+            if cplx:
+                a = np.conj(a)
+            ref[i] = np.sum(a * b_cols[i].astype(ld)) + ld(c_vals[i])
+        ref_max = float(np.max(np.abs(ref)))
+
+        def run(label, f64_mode):
+            ex = make_executor(lib, torch.cuda.current_stream().cuda_stream)
+            lib.set_int(ex, 0x1007, f64_mode)
+            prod = Product(lib, case, ptrs, ex)
+            t_ms = time_device(torch, prod, steps, 1, lambda: None)
+            ex_s = make_executor(lib, torch.cuda.current_stream().cuda_stream, async_=False, status=True)
+            lib.set_int(ex_s, 0x1007, f64_mode)
+            prod_s = Product(lib, case, ptrs, ex_s)
+            st = []
+            prod_s(st)
+            path = lib.status_value(st[0], tapp_b200.STATUS_PATH)
+            main_us = lib.status_value(st[0], tapp_b200.STATUS_MAIN_US)
+            kernels = lib.status_value(st[0], tapp_b200.STATUS_KERNELS)
+            lib.lib.TAPP_destroy_status(st[0])
+            got = D.view(N, M)[torch.from_numpy(ns).cuda(), torch.from_numpy(ms).cuda()].cpu().numpy()
+            err = float(np.max(np.abs(got.astype(ld) - ref))) / ref_max
+            r = {"tflops": flops / (t_ms * 1e-3) / 1e12, "ms": t_ms, "path": ["noop", "generic", "reduce", "simt",
+                 "tc", "sliced"][path], "kernels": kernels, "max_abs_err_rel_to_max": err}
+            if f64_mode:
+                levels = f64_mode * (f64_mode + 1) // 2
+                int8_ops = 2.0 * M * N * (2 if cplx else 1) * K * (2 if cplx else 1) * levels
+                r["slices"] = f64_mode
+                r["int8_gemm_ms"] = main_us / 1e3
+                r["int8_tops"] = int8_ops / (main_us * 1e-6) / 1e12
+            prod.close()
+            prod_s.close()
+            lib.lib.TAPP_destroy_executor(ex)
+            lib.lib.TAPP_destroy_executor(ex_s)
+            return r
+
+        res = {"native": run("native", 0)}
+        for S in slices_list:
+            res[f"sliced_{S}"] = run(f"sliced_{S}", S)
+            res[f"sliced_{S}"]["vs_native"] = res[f"sliced_{S}"]["tflops"] / res["native"]["tflops"]
+        out["c64_conjA" if cplx else "f64"] = res
+        del A, B, Cc, D
+        torch.cuda.empty_cache()
+    out["config"] = (f"D[a,b,i,j] = sum_{{e,f}} A[a,b,e,f] B[e,f,i,j] + C, a=b=e=f={ab}, i=j={ij}; "
+                     "|x| log-uniform [1e-8,1], random sign / phase, beta=1")
+    out["error_reference"] = f"{samples} sampled outputs accumulated in numpy longdouble"
+    return out
+
+
 def served_measure(lib, torch, n, seed=5, max_tensor_bytes=1 << 30):
     """The served configuration on a reduced stream: n requests of the served
     mix (every tensor at most max_tensor_bytes), operands resident in HBM.
@@ -430,6 +538,11 @@ def run_b200(args):
     if args.only_served:
         if rank == 0:
             print(json.dumps(served_measure(lib, torch, max(args.served, 1))), flush=True)
+        return
+    slices = tuple(int(x) for x in args.slices.split(",") if x)
+    if args.only_double:
+        if rank == 0:
+            print(json.dumps(double_measure(lib, torch, slices, ab=args.double_ab, ij=args.double_ij)), flush=True)
         return
 
     # ---------------- headline: BF16BF16_ACCUM_F32, operands in HBM ----------------
@@ -541,6 +654,9 @@ def run_b200(args):
     served = None
     if world == 1 and args.served > 0:
         served = served_measure(lib, torch, args.served)
+    double = None
+    if world == 1 and not args.no_double:
+        double = double_measure(lib, torch, slices)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -558,7 +674,7 @@ def run_b200(args):
                            "l2": "inputs 256 MiB > 126 MB L2 (A,B,C,D 64 MiB each)",
                            "step": "pack A, pack B, tcgen05 GEMM + fused epilogue"},
                 "vs_plain_gpu": (value / world / plain) if plain else None,
-                "modes": modes, "served": served, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu,
+                "modes": modes, "double": double, "served": served, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu,
                 "clocks": clocks, "gpu_launches": gpu_launches}
         print(json.dumps(line), flush=True)
     prod.close()
