@@ -41,9 +41,11 @@ namespace sl {
 
 constexpr int TR = 32;                  // source rows per slicing tile
 constexpr int TK = 64;                  // digit bytes per slice row per tile
-constexpr int EXP_BAD = 0x40000000;     // the row holds a non-finite value
-constexpr int EXP_ZERO = -0x40000000;   // the row is zero
-constexpr int EXP_NONE = -100000;       // exponent of zero while reducing
+// Row exponents are kept as code = e + EXP_BIAS (0 for a zero row, EXP_BAD
+// when the row holds a non-finite value), so that a zeroed array and
+// atomicMax over blocks that each see part of a row give the row's code.
+constexpr int EXP_BIAS = 2048;
+constexpr int EXP_BAD = 1 << 20;
 constexpr int64_t MAX_TERMS = 2147483647ll / (127 * 127);  // products per int32 sum
 constexpr int64_t K_CHUNK = MAX_TERMS / 128 * 128;         // 133,120
 
@@ -93,77 +95,71 @@ struct SliceParams {
     int8_t* dst;          // [L][Rout][S][Kp]
 };
 
-// exponent e with |x| < 2^e (IEEE binary64 fields); EXP_NONE for zero
-__device__ __forceinline__ int exp_bound(double x, int& bad)
+// code of x: 0 for zero, e + EXP_BIAS with |x| < 2^e (IEEE binary64
+// fields), EXP_BAD for a non-finite value
+__device__ __forceinline__ int exp_code(double x)
 {
     const unsigned long long b = (unsigned long long)__double_as_longlong(x);
     const int be = (int)((b >> 52) & 0x7ff);
-    if (be == 0x7ff) {
-        bad = 1;
-        return EXP_NONE;
-    }
-    if ((b << 1) == 0) return EXP_NONE;
-    return be == 0 ? -1022 : be - 1022;
+    if (be == 0x7ff) return EXP_BAD;
+    if ((b << 1) == 0) return 0;
+    return (be == 0 ? -1022 : be - 1022) + EXP_BIAS;
 }
 
-__device__ __forceinline__ void write_exp(const SliceParams& p, int64_t l, int64_t r, int e, int bad)
+// 2^-e for a row code (0 for zero and non-finite rows: their digits are 0)
+__device__ __forceinline__ double row_inverse(int code)
 {
-    p.expo[l * p.R + r] = bad ? EXP_BAD : (e == EXP_NONE ? EXP_ZERO : e);
+    return (code == 0 || code >= EXP_BAD) ? 0.0 : scalbn(1.0, EXP_BIAS - code);
 }
 
-// row exponents; RF: rows contiguous in the source (threads along rows),
-// otherwise one warp per row along k
+// Row exponent codes, the contracted range split over grid.y; partial maxima
+// meet in p.expo (zeroed first) by atomicMax. RF: rows contiguous in the
+// source (threads along rows), otherwise one warp per row along k.
 template <bool RF>
-__global__ void __launch_bounds__(256) k_exponents(SliceParams p)
+__global__ void __launch_bounds__(256) k_exponents(SliceParams p, int64_t kchunk)
 {
     __shared__ int part[8][TR];
-    __shared__ int badp[8][TR];
     const int t = threadIdx.x;
     const int64_t r0 = (int64_t)blockIdx.x * TR;
     const int64_t l = blockIdx.z;
     const int64_t lo = mode_offset(p.ls, l);
+    const int64_t kb = (int64_t)blockIdx.y * kchunk;
+    const int64_t ke = kb + kchunk < p.K ? kb + kchunk : p.K;
     if (RF) {
         const int r = t % TR, kq = t / TR;
-        int e = EXP_NONE, bad = 0;
+        int c = 0;
         if (r0 + r < p.R) {
             const int64_t ro = p.roff[r0 + r] + lo;
-            for (int64_t k = kq; k < p.K; k += 8) {
+            for (int64_t k = kb + kq; k < ke; k += 8) {
                 double re, im;
                 load_elem<double>(p.src, ro + p.koff[k], p.type, re, im);
-                e = max(e, exp_bound(re, bad));
-                if (p.cplx) e = max(e, exp_bound(im, bad));
+                c = max(c, exp_code(re));
+                if (p.cplx) c = max(c, exp_code(im));
             }
         }
-        part[kq][r] = e;
-        badp[kq][r] = bad;
+        part[kq][r] = c;
         __syncthreads();
         if (t < TR && r0 + t < p.R) {
-            int m = EXP_NONE, b = 0;
-            for (int j = 0; j < 8; j++) {
-                m = max(m, part[j][t]);
-                b |= badp[j][t];
-            }
-            write_exp(p, l, r0 + t, m, b);
+            int m = 0;
+            for (int j = 0; j < 8; j++) m = max(m, part[j][t]);
+            if (m) atomicMax(&p.expo[l * p.R + r0 + t], m);
         }
     } else {
         const int w = t >> 5, lane = t & 31;
         for (int i = 0; i < TR / 8; i++) {
             const int r = w * (TR / 8) + i;
-            int e = EXP_NONE, bad = 0;
+            int c = 0;
             if (r0 + r < p.R) {
                 const int64_t ro = p.roff[r0 + r] + lo;
-                for (int64_t k = lane; k < p.K; k += 32) {
+                for (int64_t k = kb + lane; k < ke; k += 32) {
                     double re, im;
                     load_elem<double>(p.src, ro + p.koff[k], p.type, re, im);
-                    e = max(e, exp_bound(re, bad));
-                    if (p.cplx) e = max(e, exp_bound(im, bad));
+                    c = max(c, exp_code(re));
+                    if (p.cplx) c = max(c, exp_code(im));
                 }
             }
-            for (int o = 16; o > 0; o >>= 1) {
-                e = max(e, __shfl_xor_sync(0xffffffffu, e, o));
-                bad |= __shfl_xor_sync(0xffffffffu, bad, o);
-            }
-            if (lane == 0 && r0 + r < p.R) write_exp(p, l, r0 + r, e, bad);
+            for (int o = 16; o > 0; o >>= 1) c = max(c, __shfl_xor_sync(0xffffffffu, c, o));
+            if (lane == 0 && c && r0 + r < p.R) atomicMax(&p.expo[l * p.R + r0 + r], c);
         }
     }
 }
@@ -213,8 +209,7 @@ __global__ void __launch_bounds__(256) k_slice(SliceParams p)
     const int r = t >> 3, kc = (t & 7) * 8;
     const int64_t kbyte = kt * TK + kc;
     if (r0 + r >= p.R || kbyte >= p.Kp) return;
-    const int E = p.expo[l * p.R + r0 + r];
-    const double inv = (E == EXP_BAD || E == EXP_ZERO) ? 0.0 : scalbn(1.0, -E);
+    const double inv = row_inverse(p.expo[l * p.R + r0 + r]);
     if (!CPLX) {
         double y[8];
 #pragma unroll
@@ -277,14 +272,15 @@ __global__ void __launch_bounds__(256) k_sliced_finish(FinishParams p)
         const double* w = p.W + (l * p.M + m) * p.Nout + (CPLX ? 2 * n : n);
         const int Ea = p.expA[l * p.M + m], Fb = p.expB[l * p.N + n];
         double xr, xi = 0.0;
-        if (Ea == EXP_BAD || Fb == EXP_BAD) {
+        if (Ea >= EXP_BAD || Fb >= EXP_BAD) {
             xr = __longlong_as_double(0x7ff8000000000000ll);
             xi = CPLX ? xr : 0.0;
-        } else if (Ea == EXP_ZERO || Fb == EXP_ZERO) {
+        } else if (Ea == 0 || Fb == 0) {
             xr = 0.0;
         } else {
-            xr = scalbn(w[0], Ea + Fb);
-            if (CPLX) xi = scalbn(w[1], Ea + Fb);
+            const int sh = Ea + Fb - 2 * EXP_BIAS;
+            xr = scalbn(w[0], sh);
+            if (CPLX) xi = scalbn(w[1], sh);
         }
         double vr = p.alpha_re * xr - (CPLX ? p.alpha_im * xi : 0.0);
         double vi = CPLX ? p.alpha_re * xi + p.alpha_im * xr : 0.0;
@@ -439,9 +435,19 @@ cudaError_t launch_sliced(const tb_plan* P, const tb_ptrs* d, cudaStream_t s, in
         sp.expo = side == 0 ? EA : EB;
         sp.dst = side == 0 ? A8 : B8;
         const bool rf = min_abs(side == 0 ? P->M : P->N, side) < min_abs(P->K, side);
-        const dim3 ge((unsigned)((sp.R + TR - 1) / TR), 1, (unsigned)L);
-        if (rf) k_exponents<true><<<ge, 256, 0, s>>>(sp);
-        else k_exponents<false><<<ge, 256, 0, s>>>(sp);
+        // about 8 blocks per SM, each over at least 256 contracted terms
+        const int64_t row_tiles = (sp.R + TR - 1) / TR * L;
+        int64_t ky = (148 * 8 + row_tiles - 1) / row_tiles;
+        if (ky > (K + 255) / 256) ky = (K + 255) / 256;
+        if (ky > 65535) ky = 65535;
+        if (ky < 1) ky = 1;
+        const int64_t kchunk = (K + ky - 1) / ky;
+        ky = (K + kchunk - 1) / kchunk;
+        e = cudaMemsetAsync(sp.expo, 0, (size_t)(L * sp.R) * sizeof(int32_t), s);
+        if (e != cudaSuccess) break;
+        const dim3 ge((unsigned)((sp.R + TR - 1) / TR), (unsigned)ky, (unsigned)L);
+        if (rf) k_exponents<true><<<ge, 256, 0, s>>>(sp, kchunk);
+        else k_exponents<false><<<ge, 256, 0, s>>>(sp, kchunk);
         const dim3 gs((unsigned)((sp.R + TR - 1) / TR), (unsigned)((y.Kp + TK - 1) / TK), (unsigned)L);
         if (cplx) {
             if (rf) k_slice<true, true><<<gs, 256, 0, s>>>(sp);
