@@ -88,6 +88,7 @@ __host__ __device__ inline void decode2(const ModeList& m, int64_t idx, int64_t&
 // pack
 struct PackParams {
     const void* src;
+    const void* const* srcs;  // batched product: source of batch b (grid.z = b * Lsz + l), else NULL
     void* dst;
     int32_t type, conj, round_mode, cplx, is_B, split, fmt, rows_fast;
     int64_t R, K, Lsz, Kseg, Kld, Rout;
@@ -116,6 +117,8 @@ __global__ void __launch_bounds__(256) k_pack(PackParams p)
     __shared__ int64_t kOff[PK];
     __shared__ int64_t lOff;
     const int64_t r0 = (int64_t)blockIdx.x * PR, k0 = (int64_t)blockIdx.y * PK, l = blockIdx.z;
+    const int64_t lsrc = p.srcs ? l % p.Lsz : l;  // batch mode of the source; l also counts batches
+    const void* src = p.srcs ? p.srcs[l / p.Lsz] : p.src;
     const int t = threadIdx.x;
     if (t < PR) {
         int64_t o = 0, dummy;
@@ -127,7 +130,7 @@ __global__ void __launch_bounds__(256) k_pack(PackParams p)
         kOff[t - PR] = o;
     } else if (t == PR + PK) {
         int64_t o, dummy;
-        decode2(p.ls, l, o, dummy);
+        decode2(p.ls, lsrc, o, dummy);
         lOff = o;
     }
     __syncthreads();
@@ -140,7 +143,7 @@ __global__ void __launch_bounds__(256) k_pack(PackParams p)
         if (r0 + r < p.R && k0 + kk < p.K) {
             const int64_t off = lOff + rowOff[r] + kOff[kk];
             if (p.us.n == 0) {
-                load_rounded<float>(p.src, off, p.type, p.round_mode, re, im);
+                load_rounded<float>(src, off, p.type, p.round_mode, re, im);
                 if (p.conj) im = -im;
             } else {
                 int64_t c[TB_MAXMODES];
@@ -148,7 +151,7 @@ __global__ void __launch_bounds__(256) k_pack(PackParams p)
                 int64_t o = off;
                 for (int64_t u = 0; u < p.usize; u++) {
                     float xr, xi;
-                    load_elem<float>(p.src, o, p.type, xr, xi);
+                    load_elem<float>(src, o, p.type, xr, xi);
                     if (p.conj) xi = -xi;
                     re += xr;
                     im += xi;
@@ -249,6 +252,8 @@ __global__ void __launch_bounds__(256, 4) k_pack_real(PackParams p)
     __shared__ int64_t kOff[FK];
     __shared__ int64_t lOff;
     const int64_t r0 = (int64_t)blockIdx.x * FR, k0 = (int64_t)blockIdx.y * FK, l = blockIdx.z;
+    const int64_t lsrc = p.srcs ? l % p.Lsz : l;  // batch mode of the source; l also counts batches
+    const void* src = p.srcs ? p.srcs[l / p.Lsz] : p.src;
     const int t = threadIdx.x;
     if (t < FR) {
         int64_t o = 0, dummy;
@@ -260,7 +265,7 @@ __global__ void __launch_bounds__(256, 4) k_pack_real(PackParams p)
         kOff[t - FR] = o;
     } else if (t == FR + FK) {
         int64_t o, dummy;
-        decode2(p.ls, l, o, dummy);
+        decode2(p.ls, lsrc, o, dummy);
         lOff = o;
     }
     __syncthreads();
@@ -277,10 +282,10 @@ __global__ void __launch_bounds__(256, 4) k_pack_real(PackParams p)
         const int64_t off = lOff + rowOff[r] + kOff[kk];
         if (VEC == 4) {
             float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (in) q = __ldg((const float4*)((const float*)p.src + off));
+            if (in) q = __ldg((const float4*)((const float*)src + off));
             x[u][0] = q.x; x[u][VEC > 1 ? 1 : 0] = q.y; x[u][VEC > 2 ? 2 : 0] = q.z; x[u][VEC > 3 ? 3 : 0] = q.w;
         } else {
-            x[u][0] = in ? load_as_float<T>(p.src, off) : 0.f;
+            x[u][0] = in ? load_as_float<T>(src, off) : 0.f;
         }
     }
 #pragma unroll
@@ -349,13 +354,15 @@ static bool vec4_ok(const ModeList& fast, const ModeList* others[], int nothers,
     return true;
 }
 
+// grid.z = lz panel batches (the batch modes, times the batches of a batched
+// product); aligned: every source base of a batched product is 16-byte aligned
 template <typename T>
-static void launch_pack_real(const PackParams& pp, int split, int fmt, cudaStream_t s)
+static void launch_pack_real(const PackParams& pp, int split, int fmt, int64_t lz, bool aligned, cudaStream_t s)
 {
-    dim3 grid((unsigned)((pp.R + FR - 1) / FR), (unsigned)((pp.Kseg + FK - 1) / FK), (unsigned)pp.Lsz);
+    dim3 grid((unsigned)((pp.R + FR - 1) / FR), (unsigned)((pp.Kseg + FK - 1) / FK), (unsigned)lz);
     const bool rf = pp.rows_fast != 0;
     bool v4 = false;
-    if (sizeof(T) == 4) {
+    if (sizeof(T) == 4 && aligned) {
         const ModeList* others[3] = {rf ? &pp.ks : &pp.rows, &pp.ls, &pp.us};
         v4 = vec4_ok(rf ? pp.rows : pp.ks, others, 2, pp.src);
     }
@@ -382,6 +389,10 @@ struct EpiParams {
     double* W;
     double level_scale;
     int32_t w_first, w_pad;
+    // batched product: C and D of batch b = l / Lper (device arrays), else NULL
+    const void* const* Cs;
+    void* const* Ds;
+    int64_t Lper;
 };
 
 struct GemmParams {
@@ -608,13 +619,13 @@ __device__ __forceinline__ float ld_nc_f32(const float* p)
 __device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, %0;" ::"n"(EPI_THREADS) : "memory"); }
 
 // beta * op_C(C) for one output (0 when beta == 0)
-__device__ __forceinline__ void load_beta_c(const EpiParams& e, int64_t offC, float& br, float& bi)
+__device__ __forceinline__ void load_beta_c(const EpiParams& e, const void* Cbase, int64_t offC, float& br, float& bi)
 {
     br = 0.f;
     bi = 0.f;
     if (e.beta_zero) return;
     float cr, ci;
-    load_rounded<float>(e.C, offC, e.tC, e.round_C, cr, ci);
+    load_rounded<float>(Cbase, offC, e.tC, e.round_C, cr, ci);
     if (e.conjC) ci = -ci;
     if (e.cplx) {
         br = e.beta_re * cr - e.beta_im * ci;
@@ -624,7 +635,8 @@ __device__ __forceinline__ void load_beta_c(const EpiParams& e, int64_t offC, fl
     }
 }
 
-__device__ __forceinline__ void finish_out(const EpiParams& e, int64_t offD, float ar, float ai, float br, float bi)
+__device__ __forceinline__ void finish_out(const EpiParams& e, void* Dbase, int64_t offD, float ar, float ai, float br,
+                                           float bi)
 {
     float accr, acci;
     if (e.cplx) {
@@ -635,7 +647,7 @@ __device__ __forceinline__ void finish_out(const EpiParams& e, int64_t offD, flo
         acci = 0.f;
     }
     if (e.conjD) acci = -acci;
-    store_elem<float>(e.D, offD, e.tD, accr, acci);
+    store_elem<float>(Dbase, offD, e.tD, accr, acci);
 }
 
 // EPI_F32: real product, C and D binary32 (the common case, specialised);
@@ -840,7 +852,15 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                 colD[c] = od;
             }
             int64_t lC, lD;
-            decode2(e.ll, l, lC, lD);
+            const void* Cbase = e.C;
+            void* Dbase = e.D;
+            int64_t lt = l;
+            if (e.Ds) {  // batched product: this tile's batch and batch mode
+                lt = l % e.Lper;
+                Cbase = e.Cs[l / e.Lper];
+                Dbase = e.Ds[l / e.Lper];
+            }
+            decode2(e.ll, lt, lC, lD);
             const int64_t m = row0 + q * 32 + lane;
             const bool mok = m < e.M;
             int64_t rC = 0, rD = 0;
@@ -1002,7 +1022,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                 // while the MMAs of this tile may still run
                 epi_bar();  // column offsets of this tile are visible
                 float buf[2][32];  // ping-pong: chunk t uses buf[t & 1], chunk t+1 loads into the other
-                const float* Cb = (const float*)e.C + rC;
+                const float* Cb = (const float*)Cbase + rC;
                 auto fetch = [&](int ch, float (&dst)[32]) {
 #pragma unroll
                     for (int j = 0; j < 32; j++) {
@@ -1026,7 +1046,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                         for (int j = 0; j < 32; j++) {
                             const int c = ch * 32 + j;
                             if (mok && (int64_t)tn * BN + c < e.N)
-                                ((float*)e.D)[rD + colD[c]] = fmaf(e.alpha_re, __uint_as_float(r[j]),
+                                ((float*)Dbase)[rD + colD[c]] = fmaf(e.alpha_re, __uint_as_float(r[j]),
                                                                    e.beta_re * round_in<float>(buf[t & 1][j], e.round_C));
                         }
                     }
@@ -1049,7 +1069,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                         for (int j = 0; j < 32; j++) {
                             const int c = ch * 32 + j;
                             br[j] = bi[j] = 0.f;
-                            if (mok && (int64_t)tn * BN + c < e.N) load_beta_c(e, rC + colC[c], br[j], bi[j]);
+                            if (mok && (int64_t)tn * BN + c < e.N) load_beta_c(e, Cbase, rC + colC[c], br[j], bi[j]);
                         }
                         uint32_t r[32];
                         tmem_ld32(taddr, r);
@@ -1057,7 +1077,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                         for (int j = 0; j < 32; j++) {
                             const int c = ch * 32 + j;
                             if (mok && (int64_t)tn * BN + c < e.N)
-                                finish_out(e, rD + colD[c], __uint_as_float(r[j]), 0.f, br[j], bi[j]);
+                                finish_out(e, Dbase, rD + colD[c], __uint_as_float(r[j]), 0.f, br[j], bi[j]);
                         }
                     } else {
                         float br[16], bi[16];
@@ -1065,7 +1085,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                         for (int j = 0; j < 16; j++) {
                             const int c = ch * 16 + j;
                             br[j] = bi[j] = 0.f;
-                            if (mok && (int64_t)tn * cols_out + c < e.N) load_beta_c(e, rC + colC[c], br[j], bi[j]);
+                            if (mok && (int64_t)tn * cols_out + c < e.N) load_beta_c(e, Cbase, rC + colC[c], br[j], bi[j]);
                         }
                         uint32_t r[32];
                         tmem_ld32(taddr, r);
@@ -1073,7 +1093,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                         for (int j = 0; j < 16; j++) {
                             const int c = ch * 16 + j;
                             if (mok && (int64_t)tn * cols_out + c < e.N)
-                                finish_out(e, rD + colD[c], __uint_as_float(r[2 * j]), __uint_as_float(r[2 * j + 1]),
+                                finish_out(e, Dbase, rD + colD[c], __uint_as_float(r[2 * j]), __uint_as_float(r[2 * j + 1]),
                                            br[j], bi[j]);
                         }
                     }
@@ -1313,6 +1333,19 @@ cudaError_t launch_gemm_i8(const void* A8, const void* B8, int64_t row_bytes, in
     return e;
 }
 
+static void CUDART_CB free_host_block(void* p) { free(p); }
+
+// Batches per launch group of a batched product: the panels of one group at
+// most 2 GiB (one batch always), grid.z = batches x batch modes <= 65535.
+static int64_t group_batches(int64_t num, size_t per_batch, int64_t Lsz, int64_t tiles_per_batch)
+{
+    int64_t G = per_batch ? (int64_t)(((size_t)2 << 30) / per_batch) : num;
+    if (G > 65535 / Lsz) G = 65535 / Lsz;
+    if (G * tiles_per_batch > (1ll << 30)) G = (1ll << 30) / tiles_per_batch;
+    if (G > num) G = num;
+    return G < 1 ? 1 : G;
+}
+
 cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t s, int* kernels, void** main_timer)
 {
     using namespace tc;
@@ -1326,7 +1359,14 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
     const int64_t Kld = Kseg * split;
     const int64_t Nout = N * (cplx ? 2 : 1);
     const size_t bytesA = (size_t)Lsz * M * Kld * 2, bytesB = (size_t)Lsz * Nout * Kld * 2;
-    const size_t scratch = round_up(bytesA, 256) + round_up(bytesB, 256);
+    const bool cta2 = M >= 2 * BM && num_sms() % 2 == 0;
+    const int64_t tiles_per_batch = ((M + (cta2 ? 2 * BM : BM) - 1) / (cta2 ? 2 * BM : BM)) * ((Nout + BN - 1) / BN) * Lsz;
+    // A batched product runs in groups of G batches: one pack launch per
+    // operand and one GEMM launch per group, the batches' panels side by side
+    // (batch b, mode l at panel batch index b * Lsz + l) and the epilogue
+    // finding each tile's C and D through pointer arrays.
+    const int64_t G = num > 1 ? group_batches(num, bytesA + bytesB, Lsz, tiles_per_batch) : 1;
+    const size_t scratch = round_up((int64_t)(bytesA * G), 256) + round_up((int64_t)(bytesB * G), 256);
 
     void* ws = nullptr;
     cudaError_t e = pool_alloc(&ws, scratch, s);  // reused by every group: same stream, in order
@@ -1336,16 +1376,47 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
         cudaFreeAsync(ws, s);
         return cudaErrorMemoryAllocation;
     }
-    for (int b = 0; b < num; b++) {
+    const void** dptr = nullptr;  // device copy of [A...][B...][C...][D...]
+    bool a_vec_ok = true, b_vec_ok = true;
+    if (G > 1) {
+        const size_t pbytes = sizeof(void*) * 4 * (size_t)num;
+        const void** host = (const void**)malloc(pbytes);
+        if (!host) {
+            cudaFreeAsync(ws, s);
+            return cudaErrorMemoryAllocation;
+        }
+        for (int b = 0; b < num; b++) {
+            host[b] = d[b].A;
+            host[num + b] = d[b].B;
+            host[2 * num + b] = d[b].C;
+            host[3 * num + b] = d[b].D;
+            if (((uintptr_t)d[b].A & 15) != 0) a_vec_ok = false;
+            if (((uintptr_t)d[b].B & 15) != 0) b_vec_ok = false;
+        }
+        e = pool_alloc((void**)&dptr, pbytes, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(dptr, host, pbytes, cudaMemcpyHostToDevice, s);
+        // the host block is freed once the copy has run
+        if (e == cudaSuccess) e = cudaLaunchHostFunc(s, free_host_block, host);
+        else free(host);
+        if (e != cudaSuccess) {
+            if (dptr) cudaFreeAsync(dptr, s);
+            cudaFreeAsync(ws, s);
+            return e;
+        }
+    }
+    for (int64_t b0 = 0; b0 < num; b0 += G) {
+        const int64_t g = num - b0 < G ? num - b0 : G;  // batches in this group
+        const int64_t Lg = g * Lsz;
         char* base = (char*)ws;
         void* pA = base;
-        void* pB = base + round_up(bytesA, 256);
+        void* pB = base + round_up((int64_t)(bytesA * G), 256);
 
         // pack A and B
         for (int side = 0; side < 2; side++) {
             PackParams pp;
             memset(&pp, 0, sizeof(pp));
-            pp.src = side == 0 ? d[b].A : d[b].B;
+            pp.src = side == 0 ? d[b0].A : d[b0].B;
+            if (G > 1) pp.srcs = dptr + (side == 0 ? 0 : num) + b0;
             pp.dst = side == 0 ? pA : pB;
             pp.type = side == 0 ? P->tA : P->tB;
             pp.conj = side == 0 ? P->conjA : P->conjB;
@@ -1369,15 +1440,17 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
             pp.rows_fast = min_stride(side == 0 ? P->M : P->N, which) < min_stride(P->K, which);
             if (!cplx && pp.us.n == 0 && (pp.type == T_F32 || pp.type == T_F64 || pp.type == T_F16 ||
                                            pp.type == T_BF16)) {
+                // the vector loads need every batch's base 16-byte aligned
+                const bool al = side == 0 ? a_vec_ok : b_vec_ok;
                 switch (pp.type) {
-                case T_F32: launch_pack_real<float>(pp, split, fmt, s); break;
-                case T_F64: launch_pack_real<double>(pp, split, fmt, s); break;
-                case T_F16: launch_pack_real<__half>(pp, split, fmt, s); break;
-                default: launch_pack_real<__nv_bfloat16>(pp, split, fmt, s); break;
+                case T_F32: launch_pack_real<float>(pp, split, fmt, Lg, al, s); break;
+                case T_F64: launch_pack_real<double>(pp, split, fmt, Lg, al, s); break;
+                case T_F16: launch_pack_real<__half>(pp, split, fmt, Lg, al, s); break;
+                default: launch_pack_real<__nv_bfloat16>(pp, split, fmt, Lg, al, s); break;
                 }
             } else {
                 dim3 grid((unsigned)((pp.R + PR - 1) / PR), (unsigned)((Kseg / (cplx ? 2 : 1) + PK - 1) / PK),
-                          (unsigned)Lsz);
+                          (unsigned)Lg);
                 k_pack<<<grid, 256, 0, s>>>(pp);
             }
             count_launch();
@@ -1386,10 +1459,9 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
         e = cudaGetLastError();
         if (e != cudaSuccess) break;
 
-        const bool cta2 = M >= 2 * BM && num_sms() % 2 == 0;
         CUtensorMap tmA, tmB;
-        if (!make_map(&tmA, pA, fmt, Kld, M, Lsz, BM) ||
-            !make_map(&tmB, pB, fmt, Kld, Nout, Lsz, cta2 ? Geo<true>::b_rows : BN)) {
+        if (!make_map(&tmA, pA, fmt, Kld, M, Lg, BM) ||
+            !make_map(&tmB, pB, fmt, Kld, Nout, Lg, cta2 ? Geo<true>::b_rows : BN)) {
             e = cudaErrorInvalidValue;
             break;
         }
@@ -1397,12 +1469,17 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
         memset(&gp, 0, sizeof(gp));
         gp.tiles_m = (int)((M + (cta2 ? 2 * BM : BM) - 1) / (cta2 ? 2 * BM : BM));
         gp.tiles_n = (int)((Nout + BN - 1) / BN);
-        gp.num_tiles = gp.tiles_m * gp.tiles_n * (int)Lsz;
+        gp.num_tiles = gp.tiles_m * gp.tiles_n * (int)Lg;
         gp.num_kb = (int)((Kld + BK - 1) / BK);
         gp.error = flag;
         EpiParams& ep = gp.e;
-        ep.C = d[b].C;
-        ep.D = d[b].D;
+        ep.C = d[b0].C;
+        ep.D = d[b0].D;
+        if (G > 1) {
+            ep.Cs = dptr + 2 * num + b0;
+            ep.Ds = (void* const*)(dptr + 3 * num + b0);
+            ep.Lper = Lsz;
+        }
         ep.tC = P->tC;
         ep.tD = P->tD;
         ep.cplx = cplx;
@@ -1417,7 +1494,7 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
         ep.beta_im = (float)P->beta_im;
         ep.M = M;
         ep.N = N;
-        ep.L = Lsz;
+        ep.L = Lg;
         fill_modes(ep.mm, P->M, 2, 3);
         fill_modes(ep.nn, P->N, 2, 3);
         fill_modes(ep.ll, P->L, 2, 3);
@@ -1427,18 +1504,20 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
                                ((mma_m >> 4) << 24);
         const bool f32_epi = !cplx && P->tD == T_F32 && (P->beta_zero || P->tC == T_F32) && !P->conjD;
         CUtensorMap tmC = tmA, tmD = tmA;  // placeholders when the TMA epilogue is not used
-        const bool tma_epi = f32_epi && make_epi_map(&tmD, d[b].D, P, 3) &&
-                             (P->beta_zero || make_epi_map(&tmC, const_cast<void*>(d[b].C), P, 2));
+        // tensor maps of C and D describe one batch's tensors: single products only
+        const bool tma_epi = G == 1 && f32_epi && make_epi_map(&tmD, d[b0].D, P, 3) &&
+                             (P->beta_zero || make_epi_map(&tmC, const_cast<void*>(d[b0].C), P, 2));
         const int kind = tma_epi ? EPI_TMA : (f32_epi ? EPI_F32 : EPI_ANY);
         const int units = cta2 ? num_sms() / 2 : num_sms();
         const int grid = (gp.num_tiles < units ? gp.num_tiles : units) * (cta2 ? 2 : 1);
-        if (main_timer && b == 0) tbk_timer_begin(s, main_timer);
+        if (main_timer && b0 == 0) tbk_timer_begin(s, main_timer);
         e = launch_gemm(kind, cta2, grid, tmA, tmB, gp, idesc, tmC, tmD, s);
-        if (main_timer && b == 0) tbk_timer_end(s, *main_timer);
+        if (main_timer && b0 == 0) tbk_timer_end(s, *main_timer);
         count_launch();
         (*kernels)++;
         if (e != cudaSuccess) break;
     }
+    if (dptr) cudaFreeAsync(dptr, s);
     cudaFreeAsync(ws, s);
     return e;
 }
@@ -1570,10 +1649,10 @@ int tbk_run_plan_tc_noalloc(const tb_plan* P, const tb_ptrs* d, void* stream, in
         pp.rows_fast = min_stride(side == 0 ? P->M : P->N, side) < min_stride(P->K, side);
         if (!cplx && pp.us.n == 0 && (pp.type == T_F32 || pp.type == T_F64 || pp.type == T_F16 || pp.type == T_BF16)) {
             switch (pp.type) {
-            case T_F32: launch_pack_real<float>(pp, split, fmt, s); break;
-            case T_F64: launch_pack_real<double>(pp, split, fmt, s); break;
-            case T_F16: launch_pack_real<__half>(pp, split, fmt, s); break;
-            default: launch_pack_real<__nv_bfloat16>(pp, split, fmt, s); break;
+            case T_F32: launch_pack_real<float>(pp, split, fmt, pp.Lsz, true, s); break;
+            case T_F64: launch_pack_real<double>(pp, split, fmt, pp.Lsz, true, s); break;
+            case T_F16: launch_pack_real<__half>(pp, split, fmt, pp.Lsz, true, s); break;
+            default: launch_pack_real<__nv_bfloat16>(pp, split, fmt, pp.Lsz, true, s); break;
             }
         } else {
             dim3 grid((unsigned)((pp.R + PR - 1) / PR), (unsigned)((Kseg / (cplx ? 2 : 1) + PK - 1) / PK),

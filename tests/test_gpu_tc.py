@@ -166,3 +166,106 @@ def test_tma_epilogue_4index_sampled(tapp, oracle, gpu):
     bound = (n * 2.0 ** -24 + SPLIT_REL) * scale + 2 * 2.0 ** -24 * np.abs(D64)
     assert (np.abs(got - D64) <= bound).all()
     tapp.lib.TAPP_destroy_executor(ex)
+
+
+def _batched_against_single(tapp, cases, ex, shared=(), misalign=0):
+    """Runs TAPP_execute_batched_product over the cases (device operands,
+    batch i = cases[i]; operands named in `shared` all point at case 0's
+    buffers; `misalign` elements of padding shift every base) and compares
+    each D bit for bit with a solo TAPP_execute_product of the same batch."""
+    import ctypes as C
+    import torch
+    c0 = cases[0]
+    infos = [tapp.tensor_info(t.dtype, t.extents, t.strides)[1] for t in (c0.A, c0.B, c0.C, c0.D)]
+    _, plan = tapp.create_product(0, [t.op for t in (c0.A, c0.B, c0.C, c0.D)], infos,
+                                  [c0.A.idx, c0.B.idx, c0.C.idx, c0.D.idx], c0.prec)
+    n = len(cases)
+    keep = []
+
+    def dev(t):
+        raw = np.zeros(t.buf.nbytes + misalign * t.itemsize, dtype=np.uint8)
+        raw[misalign * t.itemsize:] = t.buf.view(np.uint8)
+        x = torch.from_numpy(raw).cuda()
+        keep.append(x)
+        return x, x.data_ptr() + (misalign + t.base) * t.itemsize
+
+    arrs = {k: (C.c_void_p * n)() for k in "ABCD"}
+    outs = []
+    for i, c in enumerate(cases):
+        for k in "ABCD":
+            src = c0 if k in shared else c
+            t = getattr(src, k)
+            if k in shared and i > 0:
+                arrs[k][i] = arrs[k][0]
+                continue
+            x, ptr = dev(t)
+            arrs[k][i] = ptr
+            if k == "D":
+                outs.append((x, t))
+    st = tapp_b200.intptr(0)
+    err = tapp.lib.TAPP_execute_batched_product(plan, ex, C.byref(st), n, c0.alpha.ctypes.data, arrs["A"],
+                                                arrs["B"], c0.beta.ctypes.data,
+                                                None if c0.C_is_null else arrs["C"], arrs["D"])
+    torch.cuda.synchronize()
+    assert err == 0, tapp.explain(err)
+    kernels = tapp.status_value(st.value, tapp_b200.STATUS_KERNELS)
+    tapp.lib.TAPP_destroy_status(st.value)
+    solos = {}
+    for i, c in enumerate(cases):
+        if id(c) not in solos:
+            solo = c.copy()
+            for k in shared:
+                setattr(solo, k, getattr(cases[0], k).copy())
+            assert run_on_device(tapp, solo, ex) == 0
+            solos[id(c)] = solo.D.buf
+        x, t = outs[i]
+        got = x.cpu().numpy()[misalign * t.itemsize:].view(t.buf.dtype)
+        assert np.array_equal(got.view(np.uint8), solos[id(c)].view(np.uint8)), i
+    tapp.lib.TAPP_destroy_tensor_product(plan)
+    for h in infos:
+        tapp.lib.TAPP_destroy_tensor_info(h)
+    return kernels
+
+
+@pytest.mark.parametrize("prec,split,misalign", [(6, False, 0), (6, False, 1), (5, False, 0), (0, True, 0)])
+def test_batched_product_one_gemm(tapp, gpu, prec, split, misalign):
+    """Seven batches of the 4-index contraction (extent 16) run as one pack
+    launch per operand and one GEMM launch; every batch equals its solo run.
+    misalign = 1 moves every base off 16-byte alignment (scalar pack loads)."""
+    rng = np.random.default_rng(60 + prec)
+    cases = [large_dense_case(rng, prec, 0, extent=16) for _ in range(7)]
+    ex = tc_executor(tapp, split=split)
+    kernels = _batched_against_single(tapp, cases, ex, misalign=misalign)
+    assert kernels == 3
+    tapp.lib.TAPP_destroy_executor(ex)
+
+
+def test_batched_complex_hadamard_misaligned(tapp, gpu):
+    """Complex float with a Hadamard (batch) mode, conj(B), beta = 0 with C
+    absent, and base pointers off 16-byte alignment (scalar loads in the
+    pack): five batches against their solo runs."""
+    rng = np.random.default_rng(64)
+    cases = [bounded_case(rng, dtype=2, prec=6, n_contracted=1, n_hadamard=1, n_freeA=1, n_freeB=1,
+                          ext_choices=[67, 70], ops=[0, 1, 0, 0], beta_zero=True, C_null=True, max_work=1e9)
+             for _ in range(1)]
+    base = cases[0]
+    cases = [base] + [base.copy() for _ in range(4)]
+    for c in cases[1:]:
+        for t in (c.A, c.B):
+            t.buf[:] = (rng.uniform(-1, 1, t.buf.size) + 1j * rng.uniform(-1, 1, t.buf.size)).astype(t.buf.dtype)
+    ex = tc_executor(tapp)
+    assert "path=tc" in path_of(tapp, base, ex)
+    _batched_against_single(tapp, cases, ex, misalign=1)
+    tapp.lib.TAPP_destroy_executor(ex)
+
+
+def test_batched_groups_split_by_grid_limit(tapp, gpu):
+    """2048 batch modes per product x 40 products exceed grid.z = 65535, so
+    the batches run in groups (31 + 9); A, B and C are shared, D is not."""
+    rng = np.random.default_rng(65)
+    base = _matmul_case(rng, 64, 64, 64, 2048, 6, beta=0.5)
+    cases = [base] * 40
+    ex = tc_executor(tapp)
+    kernels = _batched_against_single(tapp, cases, ex, shared=("A", "B", "C"))
+    assert kernels == 6
+    tapp.lib.TAPP_destroy_executor(ex)
