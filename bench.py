@@ -70,6 +70,7 @@ def parse():
     ap.add_argument("--only-served", action="store_true", help="print only the served-stream measurement")
     ap.add_argument("--no-double", action="store_true", help="skip the binary64 / complex-double measurement")
     ap.add_argument("--only-double", action="store_true", help="print only the binary64 / complex-double measurement")
+    ap.add_argument("--only-batched", action="store_true", help="print only the batched-product measurement")
     ap.add_argument("--slices", type=str, default="7,8", help="digit slices of the sliced binary64 runs")
     ap.add_argument("--double-ab", type=int, default=160, help="extent of a, b, e, f in the binary64 workload")
     ap.add_argument("--double-ij", type=int, default=40, help="extent of i, j in the binary64 workload")
@@ -364,6 +365,48 @@ def slab_values(case_D, dbuf, j_count=2):
 C4_AB, C4_IJ = 160, 40
 
 
+def batched_measure(lib, torch, batches=64, n=512, steps=20):
+    """TAPP_execute_batched_product against one TAPP_execute_product per batch:
+    `batches` products D[a,b] = sum_k A[a,k] B[k,b] + 0.5 C with a = b = k = n,
+    float32 storage, BF16BF16_ACCUM_F32, operands resident in HBM (synthetic,
+    uniform in [-1, 1]). The batched call runs one pack launch per operand and
+    one GEMM for all batches."""
+    import ctypes as Cty
+    from tapp_b200.case import Case, Tensor, scalar
+    T = lambda ext, idx: Tensor(0, ext, [1, ext[0]], [ord(c) for c in idx], 0, None, 0)
+    case = Case(T([n, n], "ak"), T([n, n], "kb"), T([n, n], "ab"), T([n, n], "ab"), scalar(0, 1.0), scalar(0, 0.5), 6)
+    bufs = {k: torch.rand(batches, n * n, device="cuda") * 2 - 1 for k in "ABCD"}
+    arrs = {k: (Cty.c_void_p * batches)(*[bufs[k][i].data_ptr() for i in range(batches)]) for k in "ABCD"}
+    ex = make_executor(lib, torch.cuda.current_stream().cuda_stream)
+    prod = Product(lib, case, [bufs[k][0].data_ptr() for k in "ABCD"], ex)
+
+    def batched():
+        st = Cty.c_ssize_t(0)
+        err = lib.lib.TAPP_execute_batched_product(prod.plan, ex, Cty.byref(st), batches, case.alpha.ctypes.data,
+                                                   arrs["A"], arrs["B"], case.beta.ctypes.data, arrs["C"], arrs["D"])
+        if err:
+            raise RuntimeError(f"TAPP_execute_batched_product: {err}")
+
+    def singles():
+        for i in range(batches):
+            prod.ptrs = [bufs[k][i].data_ptr() for k in "ABCD"]
+            prod()
+
+    flops = 2.0 * n ** 3 * batches
+    n0 = lib.launches()
+    t_b = time_device(torch, batched, steps, 3, lambda: None)
+    l_b = (lib.launches() - n0) // (steps + 3)
+    n0 = lib.launches()
+    t_s = time_device(torch, singles, steps, 3, lambda: None)
+    l_s = (lib.launches() - n0) // (steps + 3)
+    prod.close()
+    lib.lib.TAPP_destroy_executor(ex)
+    return {"workload": f"{batches} x D[a,b] = sum_k A[a,k] B[k,b] + 0.5 C, a=b=k={n}, f32 storage, BF16BF16_ACCUM_F32",
+            "batched": {"tflops": flops / (t_b * 1e-3) / 1e12, "ms": t_b, "launches": l_b},
+            "one_call_per_batch": {"tflops": flops / (t_s * 1e-3) / 1e12, "ms": t_s, "launches": l_s},
+            "speedup": t_s / t_b}
+
+
 def double_measure(lib, torch, slices_list=(7, 8), steps=2, samples=256, ab=C4_AB, ij=C4_IJ):
     """The binary64 configuration: D[a,b,i,j] = sum_{e,f} A[a,b,e,f] B[e,f,i,j] + C
     with a = b = e = f = 160 and i = j = 40 (M = K = 25600, N = 1600), once in
@@ -540,6 +583,10 @@ def run_b200(args):
             print(json.dumps(served_measure(lib, torch, max(args.served, 1))), flush=True)
         return
     slices = tuple(int(x) for x in args.slices.split(",") if x)
+    if args.only_batched:
+        if rank == 0:
+            print(json.dumps(batched_measure(lib, torch)), flush=True)
+        return
     if args.only_double:
         if rank == 0:
             print(json.dumps(double_measure(lib, torch, slices, ab=args.double_ab, ij=args.double_ij)), flush=True)
@@ -654,6 +701,7 @@ def run_b200(args):
     served = None
     if world == 1 and args.served > 0:
         served = served_measure(lib, torch, args.served)
+    batched = batched_measure(lib, torch) if world == 1 and not args.no_modes else None
     double = None
     if world == 1 and not args.no_double:
         double = double_measure(lib, torch, slices)
@@ -674,7 +722,7 @@ def run_b200(args):
                            "l2": "inputs 256 MiB > 126 MB L2 (A,B,C,D 64 MiB each)",
                            "step": "pack A, pack B, tcgen05 GEMM + fused epilogue"},
                 "vs_plain_gpu": (value / world / plain) if plain else None,
-                "modes": modes, "double": double, "served": served, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu,
+                "modes": modes, "batched": batched, "double": double, "served": served, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu,
                 "clocks": clocks, "gpu_launches": gpu_launches}
         print(json.dumps(line), flush=True)
     prod.close()

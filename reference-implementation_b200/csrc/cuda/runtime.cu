@@ -1,6 +1,8 @@
 // C ABI of the CUDA layer (tb_cuda.h): pointer queries, stream-ordered
 // device memory, copies, timing, launch counting and the dispatch of a launch
 // plan to its kernels.
+#include <cuda.h>
+
 #include <atomic>
 #include <cstdio>
 #include <mutex>
@@ -64,6 +66,55 @@ cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t s)
     return cudaMallocFromPoolAsync(p, bytes, g_pool[dev], s);
 }
 
+// Small host-to-device copies of launch descriptors (pointer arrays) through
+// a page-locked ring per device, so that they are truly asynchronous: slot i
+// is reused only after the copy that last read it has run (an event per
+// slot). Larger blocks go through pageable memory.
+constexpr int RING_SLOTS = 64;
+constexpr size_t RING_SLOT_BYTES = 64 << 10;
+struct StageRing {
+    char* host = nullptr;
+    cudaEvent_t ev[RING_SLOTS];
+    bool used[RING_SLOTS];
+    int next = 0;
+};
+static StageRing g_ring[64];
+static std::mutex g_ring_mutex;
+
+cudaError_t stage_copy(void* dev_dst, const void* src, size_t bytes, cudaStream_t s)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (bytes > RING_SLOT_BYTES || dev < 0 || dev >= 64)
+        return cudaMemcpyAsync(dev_dst, src, bytes, cudaMemcpyHostToDevice, s);
+    std::lock_guard<std::mutex> lk(g_ring_mutex);
+    StageRing& r = g_ring[dev];
+    if (!r.host) {
+        e = cudaMallocHost((void**)&r.host, RING_SLOTS * RING_SLOT_BYTES);
+        if (e != cudaSuccess) {
+            r.host = nullptr;
+            return cudaMemcpyAsync(dev_dst, src, bytes, cudaMemcpyHostToDevice, s);
+        }
+        for (int i = 0; i < RING_SLOTS; i++) {
+            cudaEventCreateWithFlags(&r.ev[i], cudaEventDisableTiming);
+            r.used[i] = false;
+        }
+    }
+    const int i = r.next;
+    r.next = (r.next + 1) % RING_SLOTS;
+    if (r.used[i]) {
+        e = cudaEventSynchronize(r.ev[i]);
+        if (e != cudaSuccess) return e;
+    }
+    char* slot = r.host + (size_t)i * RING_SLOT_BYTES;
+    memcpy(slot, src, bytes);
+    e = cudaMemcpyAsync(dev_dst, slot, bytes, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaEventRecord(r.ev[i], s);
+    r.used[i] = e == cudaSuccess;
+    return e;
+}
+
 cudaError_t launch_generic(const tb_plan* P, const tb_ptrs* d, cudaStream_t s);
 cudaError_t launch_simt(const tb_plan* P, const tb_ptrs* d, cudaStream_t s);
 cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t s, int* kernels, void** main_timer);
@@ -101,6 +152,39 @@ int tbk_pointer_kind(const void* p, int* kind, int* device)
     case cudaMemoryTypeManaged: *kind = TBK_PTR_MANAGED; break;
     case cudaMemoryTypeHost: *kind = TBK_PTR_HOST_PINNED; break;
     default: *kind = TBK_PTR_HOST; break;
+    }
+    return 0;
+}
+
+typedef CUresult (*PointerAttrFn)(void*, CUpointer_attribute, CUdeviceptr);
+
+static PointerAttrFn pointer_attr_fn()
+{
+    static PointerAttrFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuPointerGetAttribute", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PointerAttrFn)p;
+    });
+    return fn;
+}
+
+int tbk_pointer_range(const void* p, int* kind, int* device, uintptr_t* start, size_t* size)
+{
+    int e = tbk_pointer_kind(p, kind, device);
+    *start = (uintptr_t)p;
+    *size = 1;
+    if (e || (*kind != TBK_PTR_DEVICE && *kind != TBK_PTR_MANAGED)) return e;
+    PointerAttrFn fn = pointer_attr_fn();
+    CUdeviceptr st = 0;
+    size_t sz = 0;
+    if (fn && fn(&st, CU_POINTER_ATTRIBUTE_RANGE_START_ADDR, (CUdeviceptr)p) == CUDA_SUCCESS &&
+        fn(&sz, CU_POINTER_ATTRIBUTE_RANGE_SIZE, (CUdeviceptr)p) == CUDA_SUCCESS && sz > 0) {
+        *start = (uintptr_t)st;
+        *size = sz;
     }
     return 0;
 }

@@ -31,6 +31,7 @@ namespace tb {
 cudaError_t launch_generic(const tb_plan* P, const tb_ptrs* d, cudaStream_t s);
 int* device_error_word();
 cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t s);
+cudaError_t stage_copy(void* dev_dst, const void* src, size_t bytes, cudaStream_t s);
 
 namespace tc {
 
@@ -389,9 +390,12 @@ struct EpiParams {
     double* W;
     double level_scale;
     int32_t w_first, w_pad;
-    // batched product: C and D of batch b = l / Lper (device arrays), else NULL
+    // batched product: C and D of batch b = l / Lper (device arrays), else NULL;
+    // with the TMA epilogue, also their tensor maps (tmCs NULL when beta = 0)
     const void* const* Cs;
     void* const* Ds;
+    const CUtensorMap* tmCs;
+    const CUtensorMap* tmDs;
     int64_t Lper;
 };
 
@@ -887,9 +891,21 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                         mc[j] = (int)c;
                     }
                 }
+                // the tensor maps of this tile's batch (written to global memory
+                // before the launch: acquire them for the tensor-map proxy)
+                const CUtensorMap* mapC = &tmC;
+                const CUtensorMap* mapD = &tmD;
+                if (e.tmDs) {
+                    mapD = e.tmDs + l / e.Lper;
+                    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(mapD) : "memory");
+                    if (e.tmCs) {
+                        mapC = e.tmCs + l / e.Lper;
+                        asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(mapC) : "memory");
+                    }
+                }
                 int lc[5];
                 {
-                    int64_t r = l;
+                    int64_t r = lt;
                     for (int j = 0; j < e.ll.n; j++) {
                         lc[j] = (int)(r % e.ll.ext[j]);
                         r /= e.ll.ext[j];
@@ -921,7 +937,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                 auto issue_c = [&](int t) {
                     if (lane == 0 && !bzero) {
                         mbar_expect_tx(&cbar[ew], STAGE_EPI_BYTES);
-                        tma_load_5d(box, &tmC, &cbar[ew], cc[t]);
+                        tma_load_5d(box, mapC, &cbar[ew], cc[t]);
                     }
                 };
                 issue_c(0);
@@ -951,7 +967,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                     }
                     __syncwarp();
                     if (lane == 0 && ok && cok) {
-                        tma_store_5d(&tmD, box, cc[t]);
+                        tma_store_5d(mapD, box, cc[t]);
                         asm volatile("cp.async.bulk.commit_group;" ::: "memory");
                         // the box is reused by the next load: wait until the store has read it
                         asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
@@ -1333,8 +1349,6 @@ cudaError_t launch_gemm_i8(const void* A8, const void* B8, int64_t row_bytes, in
     return e;
 }
 
-static void CUDART_CB free_host_block(void* p) { free(p); }
-
 // Batches per launch group of a batched product: the panels of one group at
 // most 2 GiB (one batch always), grid.z = batches x batch modes <= 65535.
 static int64_t group_batches(int64_t num, size_t per_batch, int64_t Lsz, int64_t tiles_per_batch)
@@ -1377,6 +1391,8 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
         return cudaErrorMemoryAllocation;
     }
     const void** dptr = nullptr;  // device copy of [A...][B...][C...][D...]
+    CUtensorMap* maps = nullptr;    // host staging of one group's epilogue tensor maps
+    CUtensorMap* dmaps = nullptr;   // their device copy
     bool a_vec_ok = true, b_vec_ok = true;
     if (G > 1) {
         const size_t pbytes = sizeof(void*) * 4 * (size_t)num;
@@ -1394,10 +1410,16 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
             if (((uintptr_t)d[b].B & 15) != 0) b_vec_ok = false;
         }
         e = pool_alloc((void**)&dptr, pbytes, s);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(dptr, host, pbytes, cudaMemcpyHostToDevice, s);
-        // the host block is freed once the copy has run
-        if (e == cudaSuccess) e = cudaLaunchHostFunc(s, free_host_block, host);
-        else free(host);
+        if (e == cudaSuccess) e = stage_copy(dptr, host, pbytes, s);
+        free(host);
+        if (e == cudaSuccess) {
+            maps = (CUtensorMap*)aligned_alloc(64, sizeof(CUtensorMap) * 2 * (size_t)G);
+            if (maps && pool_alloc((void**)&dmaps, sizeof(CUtensorMap) * 2 * (size_t)G, s) != cudaSuccess) {
+                free(maps);
+                maps = nullptr;
+                dmaps = nullptr;
+            }
+        }
         if (e != cudaSuccess) {
             if (dptr) cudaFreeAsync(dptr, s);
             cudaFreeAsync(ws, s);
@@ -1504,9 +1526,24 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
                                ((mma_m >> 4) << 24);
         const bool f32_epi = !cplx && P->tD == T_F32 && (P->beta_zero || P->tC == T_F32) && !P->conjD;
         CUtensorMap tmC = tmA, tmD = tmA;  // placeholders when the TMA epilogue is not used
-        // tensor maps of C and D describe one batch's tensors: single products only
-        const bool tma_epi = G == 1 && f32_epi && make_epi_map(&tmD, d[b0].D, P, 3) &&
-                             (P->beta_zero || make_epi_map(&tmC, const_cast<void*>(d[b0].C), P, 2));
+        bool tma_epi = false;
+        if (G == 1) {
+            tma_epi = f32_epi && make_epi_map(&tmD, d[b0].D, P, 3) &&
+                      (P->beta_zero || make_epi_map(&tmC, const_cast<void*>(d[b0].C), P, 2));
+        } else if (f32_epi && maps) {
+            // one C and one D tensor map per batch of the group, in global memory
+            bool ok = true;
+            const int nm = P->beta_zero ? 1 : 2;
+            for (int64_t b = 0; b < g && ok; b++) {
+                ok = make_epi_map(&maps[b], d[b0 + b].D, P, 3) &&
+                     (P->beta_zero || make_epi_map(&maps[g + b], const_cast<void*>(d[b0 + b].C), P, 2));
+            }
+            if (ok && stage_copy(dmaps, maps, sizeof(CUtensorMap) * (size_t)(nm * g), s) == cudaSuccess) {
+                ep.tmDs = dmaps;
+                ep.tmCs = P->beta_zero ? nullptr : dmaps + g;
+                tma_epi = true;
+            }
+        }
         const int kind = tma_epi ? EPI_TMA : (f32_epi ? EPI_F32 : EPI_ANY);
         const int units = cta2 ? num_sms() / 2 : num_sms();
         const int grid = (gp.num_tiles < units ? gp.num_tiles : units) * (cta2 ? 2 : 1);
@@ -1518,6 +1555,8 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
         if (e != cudaSuccess) break;
     }
     if (dptr) cudaFreeAsync(dptr, s);
+    if (dmaps) cudaFreeAsync(dmaps, s);
+    free(maps);
     cudaFreeAsync(ws, s);
     return e;
 }

@@ -357,16 +357,31 @@ TAPP_error TAPP_execute_batched_product(TAPP_tensor_product plan, TAPP_executor 
     if (P.path == TB_PATH_NOOP) return 0;
 
     /* all operands on the device: one grouped launch */
+    /* batches are often slices of a few allocations: a pointer inside an
+     * allocation already found to be device memory needs no query */
     int all_dev = 1;
+    enum { NR = 16 };
+    uintptr_t r_lo[NR], r_hi[NR];
+    int nr = 0, next = 0;
     for (int i = 0; i < num_batches && all_dev; i++) {
         const void* q[4] = {A[i], B[i], C ? C[i] : NULL, D[i]};
         for (int k = 0; k < 4; k++) {
             if (!q[k]) continue;
+            const uintptr_t a = (uintptr_t)q[k];
+            int known = 0;
+            for (int j = 0; j < nr && !known; j++) known = a >= r_lo[j] && a < r_hi[j];
+            if (known) continue;
             int kind = 0, d = -1;
-            if (tbk_pointer_kind(q[k], &kind, &d) || (kind != TBK_PTR_DEVICE && kind != TBK_PTR_MANAGED)) {
+            uintptr_t st = 0;
+            size_t sz = 0;
+            if (tbk_pointer_range(q[k], &kind, &d, &st, &sz) || (kind != TBK_PTR_DEVICE && kind != TBK_PTR_MANAGED)) {
                 all_dev = 0;
                 break;
             }
+            r_lo[next] = st;
+            r_hi[next] = st + sz;
+            next = (next + 1) % NR;
+            if (nr < NR) nr++;
         }
     }
     if (all_dev) {

@@ -21,6 +21,9 @@ enum { TBK_ERR_NOMEM = 2 };  /* cudaErrorMemoryAllocation */
 
 int tbk_device_count(int* count);
 int tbk_pointer_kind(const void* p, int* kind, int* device);
+/* as tbk_pointer_kind; for device and managed memory also the allocation
+ * holding p, [start, start + size) */
+int tbk_pointer_range(const void* p, int* kind, int* device, uintptr_t* start, size_t* size);
 int tbk_get_device(int* dev);
 int tbk_set_device(int dev);
 int tbk_malloc(void** p, size_t bytes, void* stream);

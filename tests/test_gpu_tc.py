@@ -269,3 +269,15 @@ def test_batched_groups_split_by_grid_limit(tapp, gpu):
     kernels = _batched_against_single(tapp, cases, ex, shared=("A", "B", "C"))
     assert kernels == 6
     tapp.lib.TAPP_destroy_executor(ex)
+
+
+@pytest.mark.parametrize("beta", [0.5, 0.0])
+def test_batched_tma_epilogue_per_batch_maps(tapp, gpu, beta):
+    """Dense D[a,b] = sum_k A[a,k] B[k,b] + beta C batches (a = b = k = 256):
+    the epilogue moves each batch's C and D through that batch's own tensor
+    maps; beta = 0 leaves C out. Every batch equals its solo run."""
+    rng = np.random.default_rng(66)
+    cases = [_matmul_case(rng, 256, 256, 256, 1, 6, beta) for _ in range(9)]
+    ex = tc_executor(tapp)
+    assert _batched_against_single(tapp, cases, ex) == 3
+    tapp.lib.TAPP_destroy_executor(ex)
