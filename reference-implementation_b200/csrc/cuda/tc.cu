@@ -403,7 +403,32 @@ struct GemmParams {
     int32_t tiles_m, tiles_n, num_tiles, num_kb;
     EpiParams e;
     int* error;       // set to 1 when a wait times out
+    // The last split_tiles tiles (the last, partial round of the persistent
+    // schedule) run as two work items each, the two halves of the
+    // contraction. Whichever half finishes first (pcount, per tile and CTA
+    // rank) writes its raw sums to partial ([col][row]) and raises pready; the
+    // other adds them and runs the epilogue. The first is running when the
+    // second waits for it, so the wait cannot depend on scheduling. pcount and
+    // pready start at zero.
+    int32_t split_tiles, pad_s;
+    float* partial;
+    int* pcount;
+    int* pready;
 };
+
+// work item it of the persistent schedule: tile, contraction-block range and
+// role (0 whole tile, 1 and 2 the two halves of a split tile)
+struct Item {
+    int tile, kb0, kb1, role;
+};
+
+__device__ __forceinline__ Item item_of(const GemmParams& p, int it)
+{
+    const int nfull = p.num_tiles - p.split_tiles;
+    if (it < nfull) return Item{it, 0, p.num_kb, 0};
+    const int j = it - nfull, kh = p.num_kb / 2;
+    return (j & 1) ? Item{nfull + j / 2, kh, p.num_kb, 2} : Item{nfull + j / 2, 0, kh, 1};
+}
 
 // TMA epilogue: C and D as (up to) 5-d tensor maps whose dims are
 // [first M mode, first N mode, further M modes, further N modes, L modes];
@@ -459,6 +484,25 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volati
     for (uint32_t i = 1;; i++) {
         if (mbar_try(bar, parity)) return true;
         if ((i & 255) == 0) {
+            if (*abort_flag) return false;
+            if (now_ns() - t0 > WAIT_NS) {
+                *abort_flag = 1;
+                return false;
+            }
+        }
+    }
+}
+
+// Waits until another CTA raised *flag (acquire, GPU scope); gives up like
+// mbar_wait.
+__device__ __forceinline__ bool flag_wait(const int* flag, volatile int* abort_flag)
+{
+    const unsigned long long t0 = now_ns();
+    for (uint32_t i = 0;; i++) {
+        int v;
+        asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(flag) : "memory");
+        if (v) return true;
+        if ((i & 63) == 63) {
             if (*abort_flag) return false;
             if (now_ns() - t0 > WAIT_NS) {
                 *abort_flag = 1;
@@ -684,6 +728,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     uint32_t* tmem_slot = (uint32_t*)(bars + 192);
     volatile int* abort_flag = (volatile int*)(bars + 196);
     volatile int* epi_ok = (volatile int*)(bars + 200);
+    volatile int* epi_first = (volatile int*)(bars + 204);
     uint8_t* staging = smem + STAGES * STAGE_BYTES + 256;
     int64_t* colC = (int64_t*)staging;
     int64_t* colD = colC + BN;
@@ -725,7 +770,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     // tiles: one CTA walks 128x256 tiles; a pair walks 256x256 tiles together
     const int unit = CTA2 ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;
     const int units = CTA2 ? (int)(gridDim.x >> 1) : (int)gridDim.x;
-    const int my_tiles = p.num_tiles > unit ? (p.num_tiles - 1 - unit) / units + 1 : 0;
+    const int num_items = p.num_tiles + p.split_tiles;
+    const int my_tiles = num_items > unit ? (num_items - 1 - unit) / units + 1 : 0;
 
     if (warp == 0) {
         // ---------------- TMA producer ----------------
@@ -735,12 +781,13 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             for (int s = 0; s < NS; s++) last_issued[s] = -1;
             bool ok = true;
             for (int i = 0; i < my_tiles && ok; i++) {
-                const int tile = unit + i * units;
+                const Item it = item_of(p, unit + i * units);
+                const int tile = it.tile;
                 const int tm = tile % p.tiles_m;
                 const int rest = tile / p.tiles_m;
                 const int tn = rest % p.tiles_n;
                 const int l = rest / p.tiles_n;
-                for (int kb = 0; kb < p.num_kb; kb++, g++) {
+                for (int kb = it.kb0; kb < it.kb1; kb++, g++) {
                     const int s = g % NS;
                     const uint32_t ph = (g / NS) & 1;
                     if (!mbar_wait(&empty[s], ph ^ 1, abort_flag)) { ok = false; break; }
@@ -785,7 +832,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                 if (!mbar_wait(&tempty[acc], aph ^ 1, abort_flag)) break;
                 fence_after();
                 const uint32_t d_tmem = tmem_base + acc * BN;
-                for (int kb = 0; kb < p.num_kb; kb++, g++) {
+                const Item it = item_of(p, unit + i * units);
+                for (int kb = it.kb0; kb < it.kb1; kb++, g++) {
+                    const int kr = kb - it.kb0;  // accumulate from the item's second block on
                     const int s = g % NS;
                     const uint32_t ph = (g / NS) & 1;
                     if (!mbar_wait(&full[s], ph, abort_flag)) { ok = false; break; }
@@ -795,11 +844,11 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 #pragma unroll
                     for (int k = 0; k < BK / 16; k++) {  // 32 bytes of K per instruction
                         if (EPI == EPI_I32) {
-                            if (CTA2) mma_i8_pair(d_tmem, smem_desc(a + k * 32), smem_desc(b + k * 32), idesc, (kb | k) != 0);
-                            else mma_i8(d_tmem, smem_desc(a + k * 32), smem_desc(b + k * 32), idesc, (kb | k) != 0);
+                            if (CTA2) mma_i8_pair(d_tmem, smem_desc(a + k * 32), smem_desc(b + k * 32), idesc, (kr | k) != 0);
+                            else mma_i8(d_tmem, smem_desc(a + k * 32), smem_desc(b + k * 32), idesc, (kr | k) != 0);
                         } else {
-                            if (CTA2) mma_f16_pair(d_tmem, smem_desc(a + k * 32), smem_desc(b + k * 32), idesc, (kb | k) != 0);
-                            else mma_f16(d_tmem, smem_desc(a + k * 32), smem_desc(b + k * 32), idesc, (kb | k) != 0);
+                            if (CTA2) mma_f16_pair(d_tmem, smem_desc(a + k * 32), smem_desc(b + k * 32), idesc, (kr | k) != 0);
+                            else mma_f16(d_tmem, smem_desc(a + k * 32), smem_desc(b + k * 32), idesc, (kr | k) != 0);
                         }
                     }
                     if (CTA2) mma_commit_pair(&empty[s]);
@@ -840,7 +889,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             }
         };
         for (int i = 0; i < my_tiles; i++) {
-            const int tile = unit + i * units;
+            const Item it = item_of(p, unit + i * units);
+            const int tile = it.tile;
             const int tm = tile % p.tiles_m;
             const int rest = tile / p.tiles_m;
             const int tn = rest % p.tiles_n;
@@ -873,6 +923,46 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             rD += lD;
             const int acc = i & 1;
             const uint32_t aph = (i >> 1) & 1;
+            // split tiles: this CTA's slice of the partial sums and its flag
+            const int slot = it.role ? (it.tile - (p.num_tiles - p.split_tiles)) * 2 + (int)rank : 0;
+            float* part = it.role ? p.partial + (size_t)slot * BN * BM : nullptr;
+            bool pre = false, pre_ok = true, add_part = false;
+            if ((EPI == EPI_TMA || EPI == EPI_F32) && it.role) {
+                // a half of a split tile: the first half to finish hands its
+                // raw sums over, the second adds them and writes D
+                if (et == 0) {
+                    const int w = mbar_wait(&tfull[acc], aph, abort_flag) ? 1 : 0;
+                    *epi_first = w ? (atomicAdd(&p.pcount[slot], 1) == 0) : 0;
+                    *epi_ok = w;
+                }
+                epi_bar();
+                const bool ok0 = *epi_ok != 0, first = *epi_first != 0;
+                fence_after();
+                if (ok0 && first) {
+#pragma unroll 1
+                    for (int t = 0; t < BN / 64; t++) {
+                        const int ch = half + 2 * t;
+                        uint32_t r[32];
+                        tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + acc * BN + ch * 32, r);
+#pragma unroll
+                        for (int j = 0; j < 32; j++) part[(ch * 32 + j) * BM + q * 32 + lane] = __uint_as_float(r[j]);
+                    }
+                    __threadfence();
+                }
+                if (!ok0 || first) {
+                    fence_before();
+                    release_acc(acc);
+                    epi_bar();
+                    if (et == 0 && ok0) atomicExch(&p.pready[slot], 1);
+                    continue;
+                }
+                epi_bar();  // every thread has read the outcome above
+                if (et == 0) *epi_ok = flag_wait(&p.pready[slot], abort_flag) ? 1 : 0;
+                epi_bar();
+                pre = true;
+                pre_ok = *epi_ok != 0;
+                add_part = true;
+            }
             if (EPI == EPI_TMA) {
                 // Per chunk: TMA-load the 32x32 box of C into this warp's
                 // staging box, combine with the accumulators, write D into the
@@ -941,15 +1031,24 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                     }
                 };
                 issue_c(0);
-                if (et == 0) *epi_ok = mbar_wait(&tfull[acc], aph, abort_flag) ? 1 : 0;
-                epi_bar();
-                ok = *epi_ok != 0;
+                if (!pre) {
+                    if (et == 0) *epi_ok = mbar_wait(&tfull[acc], aph, abort_flag) ? 1 : 0;
+                    epi_bar();
+                    ok = *epi_ok != 0;
+                } else {
+                    ok = pre_ok;
+                }
                 fence_after();
 #pragma unroll 1
                 for (int t = 0; t < nch; t++) {
                     const int ch = half + 2 * t;
                     uint32_t r[32];
                     if (ok) tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + acc * BN + ch * 32, r);
+                    if (ok && add_part) {
+#pragma unroll
+                        for (int j = 0; j < 32; j++)
+                            r[j] = __float_as_uint(__uint_as_float(r[j]) + __ldcg(&part[(ch * 32 + j) * BM + q * 32 + lane]));
+                    }
                     bool cok = true;
                     if (!bzero) {
                         cok = mbar_wait(&cbar[ew], epi_cphase & 1, abort_flag);
@@ -1047,9 +1146,12 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                     }
                 };
                 fetch(half, buf[0]);
-                if (et == 0) *epi_ok = mbar_wait(&tfull[acc], aph, abort_flag) ? 1 : 0;
-                epi_bar();
-                const bool ok = *epi_ok != 0;
+                bool ok = pre_ok;
+                if (!pre) {
+                    if (et == 0) *epi_ok = mbar_wait(&tfull[acc], aph, abort_flag) ? 1 : 0;
+                    epi_bar();
+                    ok = *epi_ok != 0;
+                }
                 fence_after();
                 if (ok) {
 #pragma unroll
@@ -1058,6 +1160,12 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                         if (t + 1 < BN / 64) fetch(ch + 2, buf[(t + 1) & 1]);
                         uint32_t r[32];
                         tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + acc * BN + ch * 32, r);
+                        if (add_part) {
+#pragma unroll
+                            for (int j = 0; j < 32; j++)
+                                r[j] = __float_as_uint(__uint_as_float(r[j]) +
+                                                       __ldcg(&part[(ch * 32 + j) * BM + q * 32 + lane]));
+                        }
 #pragma unroll
                         for (int j = 0; j < 32; j++) {
                             const int c = ch * 32 + j;
@@ -1546,10 +1654,33 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
         }
         const int kind = tma_epi ? EPI_TMA : (f32_epi ? EPI_F32 : EPI_ANY);
         const int units = cta2 ? num_sms() / 2 : num_sms();
-        const int grid = (gp.num_tiles < units ? gp.num_tiles : units) * (cta2 ? 2 : 1);
+        // A last round that fills at most half the units runs its tiles as
+        // two half-contraction items each (partial sums handed over in memory)
+        void* split_ws = nullptr;
+        if ((kind == EPI_TMA || kind == EPI_F32) && gp.num_tiles > units && gp.num_kb >= 2) {
+            const int r = gp.num_tiles % units;
+            if (r > 0 && 2 * r <= units) {
+                const size_t pbytes = (size_t)r * 2 * BN * BM * sizeof(float);
+                const size_t fbytes = (size_t)r * 2 * 2 * sizeof(int);
+                if (pool_alloc(&split_ws, pbytes + fbytes, s) == cudaSuccess &&
+                    cudaMemsetAsync((char*)split_ws + pbytes, 0, fbytes, s) == cudaSuccess) {
+                    gp.split_tiles = r;
+                    gp.partial = (float*)split_ws;
+                    gp.pcount = (int*)((char*)split_ws + pbytes);
+                    gp.pready = gp.pcount + r * 2;
+                } else if (split_ws) {
+                    cudaFreeAsync(split_ws, s);
+                    split_ws = nullptr;
+                }
+                (void)cudaGetLastError();
+            }
+        }
+        const int items = gp.num_tiles + gp.split_tiles;
+        const int grid = (items < units ? items : units) * (cta2 ? 2 : 1);
         if (main_timer && b0 == 0) tbk_timer_begin(s, main_timer);
         e = launch_gemm(kind, cta2, grid, tmA, tmB, gp, idesc, tmC, tmD, s);
         if (main_timer && b0 == 0) tbk_timer_end(s, *main_timer);
+        if (split_ws) cudaFreeAsync(split_ws, s);
         count_launch();
         (*kernels)++;
         if (e != cudaSuccess) break;
