@@ -330,6 +330,136 @@ static int64_t min_abs(const tb_modes& m, int w)
     return best;
 }
 
+// ---------------------------------------------------------------------------
+// Narrow products (N <= 64 after turning, short contraction, real): the
+// mode-n products of Tucker decompositions and their kin. A 64-wide tile
+// wastes most of its FMAs on them and its set-up dominates, so instead every
+// block stages B[l] (K x NB, padded with zeros) in shared memory once and
+// streams 256 rows of A per step, one row per thread: K loads and K x NB
+// FMAs per row, accumulators in registers, then the epilogue of its N
+// outputs. A loads coalesce when A's rows are contiguous (the common case);
+// row offsets decode with 32-bit multiply-high division.
+constexpr int NARROW_MAX_SMEM = 100 * 1024;
+
+struct NarrowParams {
+    Params p;
+    FastDiv fm[TB_MAXMODES];  // M extents
+    int32_t nb;               // padded N
+    int32_t pad;
+};
+
+// DIRECT: A is stored as T and not rounded (plain loads, no type dispatch)
+template <typename T, int NB, bool DIRECT>
+__global__ void __launch_bounds__(256) k_narrow(NarrowParams np)
+{
+    const Params& p = np.p;
+    extern __shared__ __align__(16) unsigned char nsm[];
+    T* Bs = (T*)nsm;                                     // [K][NB]
+    int64_t* kA = (int64_t*)(nsm + sizeof(T) * NB * p.K);  // [K] contracted offsets in A
+    int64_t* nC = kA + p.K;                              // [NB] column offsets in C
+    int64_t* nD = nC + NB;                               // [NB] column offsets in D
+    const int t = threadIdx.x;
+    const int64_t l = blockIdx.y;
+    int64_t lA, lB, lC, lD, dummy;
+    decode(p.al, l, lA, dummy);
+    decode(p.bl, l, lB, dummy);
+    decode(p.cl, l, lC, lD);
+    for (int64_t k = t; k < p.K; k += 256) {
+        int64_t o;
+        decode(p.ak, k, o, dummy);
+        kA[k] = o + lA;
+    }
+    if (t < NB) {
+        int64_t oc = 0, od = 0;
+        if (t < p.N) decode(p.cn, t, oc, od);
+        nC[t] = oc + lC;
+        nD[t] = od + lD;
+    }
+    // B panel: element (k, n) = op_B(B)[l, k, n], rounded as the precision asks
+    for (int64_t e = t; e < p.K * NB; e += 256) {
+        const int64_t k = e / NB;
+        const int n = (int)(e % NB);
+        T x = 0, xi = 0;
+        if (n < p.N) {
+            int64_t ob, ok;
+            decode(p.bn, n, ob, dummy);
+            decode(p.bk, k, ok, dummy);
+            load_rounded<T>(p.B, lB + ob + ok, p.tB, p.round_in, x, xi);
+        }
+        Bs[k * NB + n] = x;
+    }
+    __syncthreads();
+    const int64_t tiles = (p.M + 255) / 256;
+    for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const int64_t m = tile * 256 + t;
+        if (m >= p.M) continue;
+        // row offsets in A, C and D
+        int64_t oA = 0, oC = 0, oD = 0;
+        uint32_t r = (uint32_t)m;
+        for (int j = 0; j < p.am.n; j++) {
+            const uint32_t q = fdiv(r, np.fm[j]);
+            const int64_t c = (int64_t)(r - q * np.fm[j].d);
+            r = q;
+            oA += c * p.am.s0[j];
+            oC += c * p.cm.s0[j];
+            oD += c * p.cm.s1[j];
+        }
+        T acc[NB];
+#pragma unroll
+        for (int n = 0; n < NB; n++) acc[n] = 0;
+        // contraction in chunks of U, the next chunk's loads in flight while
+        // the current one is multiplied
+        constexpr int U = 8;
+        T cur[U], nxt[U];
+        auto load_chunk = [&](int64_t k0, T (&dst)[U]) {
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                T im;
+                dst[u] = 0;
+                if (k0 + u < p.K) {
+                    if (DIRECT) dst[u] = __ldg((const T*)p.A + oA + kA[k0 + u]);
+                    else load_rounded<T>(p.A, oA + kA[k0 + u], p.tA, p.round_in, dst[u], im);
+                }
+            }
+        };
+        load_chunk(0, cur);
+        for (int64_t k0 = 0; k0 < p.K; k0 += U) {
+            if (k0 + U < p.K) load_chunk(k0 + U, nxt);
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                if (k0 + u < p.K) {
+                    const T* b = Bs + (k0 + u) * NB;
+#pragma unroll
+                    for (int n = 0; n < NB; n++) acc[n] = fma(cur[u], b[n], acc[n]);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) cur[u] = nxt[u];
+        }
+        // epilogue in groups of 8 outputs: the group's C values first (loads
+        // in flight together), then D = op_D(alpha acc + beta C)
+        const T al = (T)p.alpha, be = (T)p.beta;
+#pragma unroll
+        for (int g = 0; g < NB; g += 8) {
+            T cv[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                T im;
+                cv[j] = 0;
+                if (!p.beta_zero && g + j < p.N) load_rounded<T>(p.C, oC + nC[g + j], p.tC, p.round_in, cv[j], im);
+            }
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                if (g + j < p.N) {
+                    T v = p.beta_zero ? al * acc[g + j] : fma(be, cv[j], al * acc[g + j]);
+                    if (p.conjD && p.conjD_f32) v = (T)(float)v;  // op_D under the F64 precision rounds as conjf
+                    store_elem<T>(p.D, oD + nD[g + j], p.tD, v, (T)0);
+                }
+            }
+        }
+    }
+}
+
 // Split of the contraction: enough CTAs to fill the GPU when the tiles do
 // not, each split at least 4 slices long, the workspace at most 256 MiB.
 struct Split {
@@ -476,13 +606,55 @@ static void simt_params(const tb_plan* P, const tb_ptrs* d, simt::Params& p)
     p.d_rows_fast = min_abs(Mm, 3) <= min_abs(Nm, 3);
 }
 
+static int narrow_width(const tb_plan* P, const simt::Params& p);
+
 size_t simt_scratch_bytes(const tb_plan* P)
 {
     using namespace simt;
     Params p;
     tb_ptrs d = {nullptr, nullptr, nullptr, nullptr};
     simt_params(P, &d, p);
+    if (narrow_width(P, p)) return 0;
     return with_cfg(P->compute, tile_for(P->compute, p.M, p.N), [&](auto cfg) { return decltype(cfg)::split(p).ws_bytes; });
+}
+
+// padded width of the narrow kernel for a turned view, or 0 when it does not apply
+static int narrow_width(const tb_plan* P, const simt::Params& p)
+{
+    if (P->compute != TB_R32 && P->compute != TB_R64) return 0;
+    if (p.N > 64 || p.M < 1024 || p.M >= (1ll << 31) || p.L > 65535 || p.K < 1) return 0;
+    const int nb = p.N <= 8 ? 8 : p.N <= 16 ? 16 : p.N <= 32 ? 32 : p.N <= 48 ? 48 : 64;
+    const size_t es = P->compute == TB_R32 ? 4 : 8;
+    const size_t smem = es * (size_t)nb * (size_t)p.K + 8 * ((size_t)p.K + 2 * (size_t)nb);
+    if (smem > (size_t)simt::NARROW_MAX_SMEM) return 0;
+    // worth it only where a 64-wide tile wastes work or the contraction is short
+    if (p.N > 48 && p.K > 64) return 0;
+    return nb;
+}
+
+template <typename T, int NB>
+static cudaError_t launch_narrow_t(simt::NarrowParams& np, cudaStream_t s)
+{
+    using namespace simt;
+    const Params& p = np.p;
+    const size_t smem = sizeof(T) * NB * (size_t)p.K + 8 * ((size_t)p.K + 2 * NB);
+    const bool direct = p.tA == (sizeof(T) == 4 ? T_F32 : T_F64) && p.round_in == TB_ROUND_NONE;
+    auto kern = direct ? k_narrow<T, NB, true> : k_narrow<T, NB, false>;
+    static int attr_done[64][2];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64 || !attr_done[dev][direct]) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, NARROW_MAX_SMEM);
+        if (e != cudaSuccess) return e;
+        if (dev >= 0 && dev < 64) attr_done[dev][direct] = 1;
+    }
+    const int64_t tiles = (p.M + 255) / 256;
+    int64_t gx = (148 * 8 + p.L - 1) / p.L;
+    if (gx > tiles) gx = tiles;
+    if (gx < 1) gx = 1;
+    kern<<<dim3((unsigned)gx, (unsigned)p.L), 256, smem, s>>>(np);
+    count_launch();
+    return cudaGetLastError();
 }
 
 cudaError_t launch_simt(const tb_plan* P, const tb_ptrs* d, cudaStream_t s)
@@ -490,6 +662,30 @@ cudaError_t launch_simt(const tb_plan* P, const tb_ptrs* d, cudaStream_t s)
     using namespace simt;
     Params p;
     simt_params(P, d, p);
+    const int nb = narrow_width(P, p);
+    if (nb) {
+        NarrowParams np;
+        memset(&np, 0, sizeof(np));
+        np.p = p;
+        np.nb = nb;
+        for (int j = 0; j < p.am.n; j++) np.fm[j] = make_fastdiv((uint32_t)p.am.ext[j]);
+        if (P->compute == TB_R32) {
+            switch (nb) {
+            case 8: return launch_narrow_t<float, 8>(np, s);
+            case 16: return launch_narrow_t<float, 16>(np, s);
+            case 32: return launch_narrow_t<float, 32>(np, s);
+            case 48: return launch_narrow_t<float, 48>(np, s);
+            default: return launch_narrow_t<float, 64>(np, s);
+            }
+        }
+        switch (nb) {
+        case 8: return launch_narrow_t<double, 8>(np, s);
+        case 16: return launch_narrow_t<double, 16>(np, s);
+        case 32: return launch_narrow_t<double, 32>(np, s);
+        case 48: return launch_narrow_t<double, 48>(np, s);
+        default: return launch_narrow_t<double, 64>(np, s);
+        }
+    }
     return with_cfg(P->compute, tile_for(P->compute, p.M, p.N), [&](auto cfg) { return decltype(cfg)::launch(p, s); });
 }
 
