@@ -85,6 +85,14 @@ enum {
                                           * 3 sliced 8-bit integer) */
     TAPP_B200_STATUS_MAIN_US = 0x1105,   /* double: device time of the dominant kernel (the tensor-core
                                           * GEMM, or the CUDA-core kernel), microseconds */
+    /* double: a-priori error bound of the arithmetic the product ran in:
+     * |D - D_exact| <= bound * (|alpha| sum|op_A(a) op_B(b)| + |beta| |c|)
+     * + 2 u_D |D|, D_exact computed exactly from the operands as the
+     * precision rounds them (16-bit operands, binary32 C under 16-bit
+     * precisions) and u_D the unit roundoff of D's type. For the sliced
+     * binary64 path the bound is relative to |alpha| 2^(E_row + F_col)
+     * instead (see TAPP_B200_ATTR_F64_MODE). */
+    TAPP_B200_STATUS_ERR_BOUND = 0x1106,
 };
 
 /*

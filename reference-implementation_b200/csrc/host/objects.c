@@ -183,6 +183,7 @@ TAPP_error TAPP_attr_get(TAPP_attr attr, TAPP_key key, void** value)
     case TAPP_B200_STATUS_FLOPS: *(double*)*value = s->flops; return 0;
     case TAPP_B200_STATUS_DEVICE_US: *(double*)*value = s->device_us; return 0;
     case TAPP_B200_STATUS_MAIN_US: *(double*)*value = s->main_us; return 0;
+    case TAPP_B200_STATUS_ERR_BOUND: *(double*)*value = s->err_bound; return 0;
     default: return TAPP_B200_ERR_INVALID;
     }
 }

@@ -224,6 +224,30 @@ int tb_plan_set_scalars(tb_plan* P, const void* alpha, const void* beta)
     return bz != P->beta_zero;
 }
 
+/* A-priori bound on the error of the plan's arithmetic (see tapp_b200.h,
+ * TAPP_B200_STATUS_ERR_BOUND): n terms summed in a format with unit
+ * roundoff u err by at most gamma_n = n u / (1 - n u) times the sum of their
+ * magnitudes (Higham, Accuracy and Stability of Numerical Algorithms, 3.1). */
+double tb_plan_error_bound(const tb_plan* p)
+{
+    const int cplx = p->compute == TB_C32 || p->compute == TB_C64;
+    const double K = (double)p->K.size, UA = (double)p->UA.size, UB = (double)p->UB.size;
+    if (p->path == TB_PATH_SLICED) {
+        const double kreal = K * (cplx ? 2.0 : 1.0);
+        return kreal * (p->slices + 4) * ldexp(1.0, -7 * p->slices);
+    }
+    const double u = (p->compute == TB_R64 || p->compute == TB_C64) ? ldexp(1.0, -53) : ldexp(1.0, -24);
+    const double n = K * (UA > 1 ? UA : 1) + UA + UB + 8;
+    double g = n * u / (1.0 - n * u);
+    if (p->path == TB_PATH_TC && p->tc_mode == TB_TC_SPLIT_BF16) g += ldexp(1.0, -16);
+    if (p->round_in == TB_ROUND_BF16 || p->round_in == TB_ROUND_F16) {
+        /* the 16-bit precisions keep running unary sums in 16 bits */
+        const double u16 = p->round_in == TB_ROUND_BF16 ? ldexp(1.0, -8) : ldexp(1.0, -11);
+        if (UA > 1 || UB > 1) g += (UA + UB) * u16;
+    }
+    return g;
+}
+
 double tb_plan_flops(const tb_plan* p)
 {
     double f = (double)p->F.size * (double)p->K.size;

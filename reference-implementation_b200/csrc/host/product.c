@@ -312,6 +312,7 @@ static int run(struct tb_product* p, TAPP_executor exec, TAPP_status* status, co
             so->kernels = kernels;
             so->tc_mode = P.tc_mode;
             so->flops = tb_plan_flops(&P);
+            so->err_bound = tb_plan_error_bound(&P);
             so->device_us = dev_us;
             so->main_us = main_us;
             *status = (TAPP_status)so;
@@ -410,6 +411,7 @@ TAPP_error TAPP_execute_batched_product(TAPP_tensor_product plan, TAPP_executor 
                 so->kernels = kernels;
                 so->tc_mode = P.tc_mode;
                 so->flops = tb_plan_flops(&P) * num_batches;
+                so->err_bound = tb_plan_error_bound(&P);
                 *status = (TAPP_status)so;
             }
         }

@@ -53,6 +53,7 @@ struct tb_status {
     double flops;
     double device_us;
     double main_us;
+    double err_bound;
 };
 
 /* cached launch plan of a product, keyed on the infos' contents */
@@ -112,6 +113,7 @@ int tb_build_plan(const tb_tensor_view* A, const tb_tensor_view* B,
 int tb_plan_set_scalars(tb_plan* P, const void* alpha, const void* beta);
 size_t tb_describe(const tb_plan* p, size_t maxlen, char* out);
 double tb_plan_flops(const tb_plan* p);
+double tb_plan_error_bound(const tb_plan* p);
 int tb_elem_bytes(TAPP_datatype t);
 int tb_is_complex(TAPP_datatype t);
 

@@ -28,6 +28,7 @@ ERR_CUDA, ERR_LIMIT, ERR_UNSUPPORTED, ERR_NOMEM, ERR_INVALID, ERR_LABELS = 0x100
 ATTR_STREAM, ATTR_ASYNC, ATTR_F32_MODE, ATTR_PATH, ATTR_WANT_STATUS = 0x1000, 0x1001, 0x1002, 0x1004, 0x1005
 STATUS_PATH, STATUS_KERNELS, STATUS_FLOPS, STATUS_DEVICE_US, STATUS_TC_MODE, STATUS_MAIN_US = (
     0x1100, 0x1101, 0x1102, 0x1103, 0x1104, 0x1105)
+STATUS_ERR_BOUND = 0x1106
 PATH_NOOP, PATH_GENERIC, PATH_REDUCE, PATH_SIMT, PATH_TC = 0, 1, 2, 3, 4
 
 _lib: "B200Lib | None" = None
@@ -66,7 +67,7 @@ class B200Lib(TappLib):
         return self.lib.TAPP_attr_set(executor, ATTR_STREAM, C.c_void_p(stream_handle))
 
     def status_value(self, status: int, key: int):
-        if key in (STATUS_FLOPS, STATUS_DEVICE_US, STATUS_MAIN_US):
+        if key in (STATUS_FLOPS, STATUS_DEVICE_US, STATUS_MAIN_US, STATUS_ERR_BOUND):
             box = C.c_double(0.0)
         else:
             box = C.c_int(0)

@@ -218,3 +218,51 @@ def test_batched_product_matches_single(tapp, oracle, gpu):
             _, D64, scale = oracle.execute_f64(cases[i].copy())
             assert (np.abs(got - D64) <= error_bound(cases[i], scale, D64)).all()
     tapp.lib.TAPP_destroy_executor(ex)
+
+
+def _run_with_status(tapp, case, ex):
+    import ctypes as C
+    import torch
+    dev = [torch.from_numpy(t.buf.view(np.uint8).copy()).cuda() for t in (case.A, case.B, case.C, case.D)]
+    ptr = [d.data_ptr() + t.base * t.itemsize for d, t in zip(dev, (case.A, case.B, case.C, case.D))]
+    infos = [tapp.tensor_info(t.dtype, t.extents, t.strides)[1] for t in (case.A, case.B, case.C, case.D)]
+    _, plan = tapp.create_product(0, [t.op for t in (case.A, case.B, case.C, case.D)], infos,
+                                  [case.A.idx, case.B.idx, case.C.idx, case.D.idx], case.prec)
+    st = tapp_b200.intptr(0)
+    err = tapp.lib.TAPP_execute_product(plan, ex, C.byref(st), case.alpha.ctypes.data, ptr[0], ptr[1],
+                                        case.beta.ctypes.data, None if case.C_is_null else ptr[2], ptr[3])
+    assert err == 0
+    bound = tapp.status_value(st.value, tapp_b200.STATUS_ERR_BOUND)
+    tapp.lib.TAPP_destroy_status(st.value)
+    case.D.buf[:] = dev[3].cpu().numpy().view(case.D.buf.dtype)
+    tapp.lib.TAPP_destroy_tensor_product(plan)
+    return bound
+
+
+@pytest.mark.parametrize("label", ["plain_f32", "bf16_tc", "split_bf16", "f64", "c32_generic"])
+def test_status_error_bound_holds(tapp, oracle, gpu, label):
+    """The error bound a status reports covers the measured error against
+    the binary64 evaluation of the (precision-rounded) operands."""
+    from tapp_b200.workloads import large_dense_case, dense_contraction_case
+    rng = np.random.default_rng(300)
+    ex = tapp.create_executor()
+    tapp.set_int(ex, tapp_b200.ATTR_WANT_STATUS, 1)
+    if label == "plain_f32":
+        case = dense_contraction_case(rng, extent=16)
+    elif label == "bf16_tc":
+        case = large_dense_case(rng, 6, 0, extent=16)
+    elif label == "split_bf16":
+        case = large_dense_case(rng, 0, 0, extent=16)
+        tapp.set_int(ex, tapp_b200.ATTR_F32_MODE, 1)
+    elif label == "f64":
+        case = dense_contraction_case(rng, extent=12, dtype=1, prec=1)
+    else:
+        case = bounded_case(rng, dtype=2, prec=-1, n_contracted=2, n_freeA=1, n_freeB=1, n_isoA=1, max_ext=6)
+    run = case.copy()
+    bound = _run_with_status(tapp, run, ex)
+    _, D64, scale = oracle.execute_f64(case.copy())
+    got = d_values(run.D)
+    u_d = 2.0 ** -53 if run.D.dtype in (1, 3) else 2.0 ** -24
+    assert 0 < bound < 1e-2
+    assert (np.abs(got - D64) <= bound * scale + 2 * u_d * np.abs(D64) + 1e-300).all()
+    tapp.lib.TAPP_destroy_executor(ex)

@@ -164,3 +164,27 @@ def test_status_reports_sliced_mode(tapp, gpu):
     tapp.lib.TAPP_destroy_status(st.value)
     tapp.lib.TAPP_destroy_executor(ex)
     tapp.lib.TAPP_destroy_tensor_product(plan)
+
+
+def test_status_error_bound_sliced(tapp, oracle, gpu):
+    """The sliced path's reported bound, times |alpha| 2^(E+F) <= 4 |alpha|
+    max|A| max|B|, covers the measured error."""
+    case = double_case(np.random.default_rng(171), cplx=False, ab=24, ij=12)
+    ex = sliced_executor(tapp, 5)
+    tapp.set_int(ex, tapp_b200.ATTR_WANT_STATUS, 1)
+    infos = [tapp.tensor_info(t.dtype, t.extents, t.strides)[1] for t in (case.A, case.B, case.C, case.D)]
+    _, plan = tapp.create_product(0, [0, 0, 0, 0], infos, [case.A.idx, case.B.idx, case.C.idx, case.D.idx], -1)
+    run = case.copy()
+    st = tapp_b200.intptr(0)
+    err = tapp.lib.TAPP_execute_product(plan, ex, C.byref(st), run.alpha.ctypes.data, run.A.ptr(), run.B.ptr(),
+                                        run.beta.ctypes.data, run.C.ptr(), run.D.ptr())
+    assert err == 0
+    bound = tapp.status_value(st.value, tapp_b200.STATUS_ERR_BOUND)
+    tapp.lib.TAPP_destroy_status(st.value)
+    K, _, _ = folded_sizes(case)
+    assert bound == pytest.approx(K * 9 * 2.0 ** -35)
+    _, D64, scale = oracle.execute_f64(case.copy())
+    lim = bound * 4 * maxabs(case.A) * maxabs(case.B) + 8 * 2.0 ** -53 * scale + 2 * 2.0 ** -53 * np.abs(D64)
+    assert (np.abs(d_values(run.D) - D64) <= lim).all()
+    tapp.lib.TAPP_destroy_executor(ex)
+    tapp.lib.TAPP_destroy_tensor_product(plan)
