@@ -134,6 +134,27 @@ TAPP_EXPORT TAPP_error tapp_b200_execute_product_noalloc(TAPP_tensor_product pla
                                                          const void* beta, const void* C, void* D);
 
 /*
+ * A chain of products, such as the mode-n products that rebuild a tensor
+ * from its Tucker core and factor matrices, run back to back on the
+ * executor's stream without a host round trip between them (the reference
+ * runs each product on its own; this entry point has no counterpart there).
+ * Step i is the product plans[i] with alphas[i], betas[i], A[i], B[i],
+ * C ? C[i] : NULL and D[i], as TAPP_execute_product takes them, except:
+ *   - A[i] or B[i] NULL (i > 0): the D of step i - 1;
+ *   - D[i] NULL (i < n - 1): an intermediate the library allocates in device
+ *     memory for the step's D layout and frees after the chain.
+ * D[n - 1] must be given. Each step is validated with the codes of
+ * TAPP_execute_product (the first failing step's code is returned, earlier
+ * steps have run); TAPP_B200_ERR_INVALID for missing pointers or an
+ * executor attached to a server. Synchronous unless the executor is
+ * asynchronous. The host waits once, after the last step.
+ */
+TAPP_EXPORT TAPP_error tapp_b200_execute_chain(int n, const TAPP_tensor_product* plans, TAPP_executor exec,
+                                               const void* const* alphas, const void* const* betas,
+                                               const void* const* A, const void* const* B,
+                                               const void* const* C, void* const* D);
+
+/*
  * Serving: a request loop that runs products as they arrive on one GPU.
  * There is no counterpart in the reference (its handle and executor are
  * placeholders).

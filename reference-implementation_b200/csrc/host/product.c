@@ -448,3 +448,90 @@ size_t tapp_b200_describe_plan(TAPP_tensor_product plan, TAPP_executor exec, siz
     if (tb_build_plan(&v[0], &v[1], &v[2], &v[3], p->prec, &one, &one, &opt, &P)) return 0;
     return tb_describe(&P, maxlen, out);
 }
+
+/* A chain of products on one stream: step i may read the D of step i - 1 as
+ * its A or B (a NULL pointer), and a NULL D before the last step is an
+ * intermediate in device memory from the library's pool. Host operands are
+ * staged per step as TAPP_execute_product stages them; the host waits once,
+ * at the end. The products are validated step by step with the codes of
+ * TAPP_execute_product. */
+TAPP_error tapp_b200_execute_chain(int n, const TAPP_tensor_product* plans, TAPP_executor exec,
+                                   const void* const* alphas, const void* const* betas, const void* const* A,
+                                   const void* const* B, const void* const* C, void* const* D)
+{
+    if (n <= 0 || !plans || !alphas || !betas || !A || !B || !D || !D[n - 1]) return TAPP_B200_ERR_INVALID;
+    tb_exec_settings s;
+    int err = resolve_executor(exec, &s);
+    if (err) return err;
+    if (s.server) return TAPP_B200_ERR_INVALID;
+    void** inter = calloc((size_t)n, sizeof(void*));   /* intermediates to free */
+    void** dout = calloc((size_t)n, sizeof(void*));    /* coordinate 0 of each step's D */
+    if (!inter || !dout) {
+        free(inter);
+        free(dout);
+        return TAPP_B200_ERR_NOMEM;
+    }
+    int any_tc = 0;
+    for (int i = 0; i < n && !err; i++) {
+        struct tb_product* p = (struct tb_product*)plans[i];
+        if (!p || p->magic != TB_MAGIC_PRODUCT) {
+            err = TAPP_B200_ERR_INVALID;
+            break;
+        }
+        const void* a = A[i] ? A[i] : (i > 0 ? dout[i - 1] : NULL);
+        const void* b = B[i] ? B[i] : (i > 0 ? dout[i - 1] : NULL);
+        const void* c = C ? C[i] : NULL;
+        if (!a || !b) {
+            err = TAPP_B200_ERR_INVALID;
+            break;
+        }
+        tb_tensor_view v[4];
+        err = tb_product_views(p, v);
+        if (!err) err = tb_validate(&v[0], &v[1], &v[2], &v[3], betas[i], c != NULL);
+        tb_plan P;
+        if (!err) err = tb_product_plan(p, v, alphas[i], betas[i], &s, &P);
+        if (err) break;
+        void* d = D[i];
+        if (!d) {
+            int64_t lo, hi;
+            if (!tb_span_of(&v[3], &lo, &hi)) {
+                lo = 0;
+                hi = 0;
+            }
+            const int eb = tb_elem_bytes(v[3].type);
+            void* buf = NULL;
+            const int e = tbk_malloc(&buf, (size_t)(hi - lo + 1) * (size_t)eb, s.stream);
+            if (e) {
+                err = cuda_err(e);
+                break;
+            }
+            inter[i] = buf;
+            d = (char*)buf - lo * eb;
+        }
+        dout[i] = d;
+        if (P.path == TB_PATH_NOOP) continue;
+        const void* ptr[4] = {a, b, c, d};
+        staging st;
+        tb_ptrs dp;
+        int device = -1;
+        err = stage_in(&P, v, ptr, &st, &dp, s.stream, &device);
+        int kernels = 0;
+        if (!err) {
+            const int e = tbk_run_plan(&P, &dp, s.stream, &kernels, NULL);
+            if (e) err = cuda_err(e);
+        }
+        const int e2 = stage_out(v, &st, s.stream);
+        if (!err) err = e2;
+        if (P.path == TB_PATH_TC || P.path == TB_PATH_SLICED) any_tc = 1;
+    }
+    for (int i = 0; i < n; i++)
+        if (inter[i]) tbk_free(inter[i], s.stream);
+    if (!s.async) {
+        int e = tbk_stream_sync(s.stream);
+        if (!err && e) err = cuda_err(e);
+        if (!err && any_tc && (e = tbk_check_device_error())) err = cuda_err(e);
+    }
+    free(inter);
+    free(dout);
+    return err;
+}
