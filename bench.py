@@ -71,6 +71,7 @@ def parse():
     ap.add_argument("--no-double", action="store_true", help="skip the binary64 / complex-double measurement")
     ap.add_argument("--only-double", action="store_true", help="print only the binary64 / complex-double measurement")
     ap.add_argument("--only-batched", action="store_true", help="print only the batched-product measurement")
+    ap.add_argument("--only-chain", action="store_true", help="print only the Tucker-chain measurement")
     ap.add_argument("--slices", type=str, default="7,8", help="digit slices of the sliced binary64 runs")
     ap.add_argument("--double-ab", type=int, default=160, help="extent of a, b, e, f in the binary64 workload")
     ap.add_argument("--double-ij", type=int, default=40, help="extent of i, j in the binary64 workload")
@@ -407,6 +408,86 @@ def batched_measure(lib, torch, batches=64, n=512, steps=20):
             "speedup": t_s / t_b}
 
 
+def chain_measure(lib, torch, r=64, n=256, reps=10):
+    """Tucker reconstruction X[a,b,c] = sum_{i,j,k} G[i,j,k] U1[a,i] U2[b,j] U3[c,k] (core r^3,
+    factors n x r, float32, F32F32_ACCUM_F32; synthetic, uniform in [-1, 1]) from pinned HOST
+    buffers: tapp_b200_execute_chain (intermediates stay on the device, one host wait) against
+    three TAPP_execute_product calls (each intermediate copied back and forth). Wall clock."""
+    import ctypes as Cty
+    from tapp_b200.case import Tensor, scalar
+    i_, j_, k_, a_, b_, c_ = (ord(x) for x in "ijkabc")
+    shapes = [([r, r, r], [i_, j_, k_], [n, r], [a_, i_], [n, r, r], [a_, j_, k_]),
+              ([n, r, r], [a_, j_, k_], [n, r], [b_, j_], [n, n, r], [a_, b_, k_]),
+              ([n, n, r], [a_, b_, k_], [n, r], [c_, k_], [n, n, n], [a_, b_, c_])]
+
+    def colmajor(e):
+        st, acc = [], 1
+        for x in e:
+            st.append(acc)
+            acc *= x
+        return st
+
+    def pinned(numel):
+        t = torch.empty(numel, dtype=torch.float32).pin_memory()
+        t.uniform_(-1, 1)
+        return t
+
+    G = pinned(r ** 3)
+    U = [pinned(n * r) for _ in range(3)]
+    outs = [pinned(int(np.prod(s[4]))) for s in shapes]
+    alpha, beta = scalar(0, 1.0), scalar(0, 0.0)
+    plans, infos = [], []
+    for ae, ai, be, bi, de, di in shapes:
+        inf = [lib.tensor_info(0, e, colmajor(e))[1] for e in (ae, be, de, de)]
+        _, plan = lib.create_product(0, [0, 0, 0, 0], inf, [ai, bi, di, di], 0)
+        plans.append(plan)
+        infos += inf
+    ex = lib.create_executor()
+    f = lib.lib.tapp_b200_execute_chain
+    f.restype = Cty.c_int
+    f.argtypes = [Cty.c_int, Cty.POINTER(Cty.c_ssize_t), Cty.c_ssize_t] + [Cty.POINTER(Cty.c_void_p)] * 6
+    arr = lambda v: (Cty.c_void_p * len(v))(*v)
+    P = (Cty.c_ssize_t * 3)(*plans)
+    al, be_ = arr([alpha.ctypes.data] * 3), arr([beta.ctypes.data] * 3)
+    A = arr([G.data_ptr(), None, None])
+    B = arr([u.data_ptr() for u in U])
+    D = arr([None, None, outs[2].data_ptr()])
+
+    def chain():
+        if f(3, P, ex, al, be_, A, B, None, D):
+            raise RuntimeError("tapp_b200_execute_chain failed")
+
+    def steps():
+        src = G
+        for s_, (plan, u, o) in enumerate(zip(plans, U, outs)):
+            st = Cty.c_ssize_t(0)
+            if lib.lib.TAPP_execute_product(plan, ex, Cty.byref(st), alpha.ctypes.data, src.data_ptr(), u.data_ptr(),
+                                            beta.ctypes.data, None, o.data_ptr()):
+                raise RuntimeError("TAPP_execute_product failed")
+            src = o
+
+    def wall(fn):
+        fn()
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            fn()
+            ts.append(time.perf_counter() - t0)
+        return statistics.median(ts) * 1e3
+
+    t_chain, t_steps = wall(chain), wall(steps)
+    for plan in plans:
+        lib.lib.TAPP_destroy_tensor_product(plan)
+    for h in infos:
+        lib.lib.TAPP_destroy_tensor_info(h)
+    lib.lib.TAPP_destroy_executor(ex)
+    flops = 2.0 * (n * r ** 3 + n * n * r ** 2 + n ** 3 * r)
+    return {"workload": f"Tucker reconstruction, core {r}^3, factors {n}x{r}, float32, pinned host operands",
+            "chain_ms": t_chain, "three_calls_ms": t_steps, "speedup": t_steps / t_chain,
+            "chain_tflops_e2e": flops / (t_chain * 1e-3) / 1e12,
+            "h2d_bytes": 4 * (r ** 3 + 3 * n * r), "d2h_bytes": 4 * n ** 3}
+
+
 def double_measure(lib, torch, slices_list=(7, 8), steps=2, samples=256, ab=C4_AB, ij=C4_IJ):
     """The binary64 configuration: D[a,b,i,j] = sum_{e,f} A[a,b,e,f] B[e,f,i,j] + C
     with a = b = e = f = 160 and i = j = 40 (M = K = 25600, N = 1600), once in
@@ -583,6 +664,10 @@ def run_b200(args):
             print(json.dumps(served_measure(lib, torch, max(args.served, 1))), flush=True)
         return
     slices = tuple(int(x) for x in args.slices.split(",") if x)
+    if args.only_chain:
+        if rank == 0:
+            print(json.dumps(chain_measure(lib, torch)), flush=True)
+        return
     if args.only_batched:
         if rank == 0:
             print(json.dumps(batched_measure(lib, torch)), flush=True)
@@ -702,6 +787,7 @@ def run_b200(args):
     if world == 1 and args.served > 0:
         served = served_measure(lib, torch, args.served)
     batched = batched_measure(lib, torch) if world == 1 and not args.no_modes else None
+    chain = chain_measure(lib, torch) if world == 1 and not args.no_modes else None
     double = None
     if world == 1 and not args.no_double:
         double = double_measure(lib, torch, slices)
@@ -722,7 +808,7 @@ def run_b200(args):
                            "l2": "inputs 256 MiB > 126 MB L2 (A,B,C,D 64 MiB each)",
                            "step": "pack A, pack B, tcgen05 GEMM + fused epilogue"},
                 "vs_plain_gpu": (value / world / plain) if plain else None,
-                "modes": modes, "batched": batched, "double": double, "served": served, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu,
+                "modes": modes, "batched": batched, "tucker_chain": chain, "double": double, "served": served, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu,
                 "clocks": clocks, "gpu_launches": gpu_launches}
         print(json.dumps(line), flush=True)
     prod.close()
