@@ -414,6 +414,20 @@ struct GemmParams {
     float* partial;
     int* pcount;
     int* pready;
+    // Operands read in place (16-bit storage, no pack): the tensor map has
+    // the dims (row mode 0, k mode 0, row mode 1, k mode 1, batch) in the
+    // MN-major case and (k mode 0, row mode 0, k mode 1, row mode 1, batch)
+    // in the K-major case; every stage loads 64-row x 64-k boxes. e0/k0 are
+    // the extents of row mode 0 and k mode 0 (multiples of 64).
+    int32_t a_direct, b_direct, a_mn, b_mn;
+    int32_t a_e0, a_k0, b_e0, b_k0;
+    // box shape of each direct operand: 0 one 64-row box per 64 rows, 1 all
+    // rows in one box along row mode 1 (row mode 0 has extent 64), 2 all rows
+    // in one box along row mode 0 (K-major, extent a multiple of the rows)
+    int32_t a_box, b_box;
+    // logical dims present in each direct operand's map (bit j: dim j; dims
+    // of extent 1 are left out, fewer dims copy faster)
+    int32_t a_dims, b_dims;
 };
 
 // work item it of the persistent schedule: tile, contraction-block range and
@@ -544,6 +558,35 @@ __device__ __forceinline__ void tma_load_3d_pair(void* dst, const CUtensorMap* t
         : "memory");
 }
 
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* tm, uint64_t* bar, const int (&c)[5])
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6}], [%2];"
+        ::"r"(smem_u32(dst)), "l"(tm), "r"(smem_u32(bar)), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3])
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_load_4d_pair(void* dst, const CUtensorMap* tm, uint32_t bar_cluster, const int (&c)[5])
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6}], [%2];"
+        ::"r"(smem_u32(dst)), "l"(tm), "r"(bar_cluster), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3])
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_load_3d_c(void* dst, const CUtensorMap* tm, uint64_t* bar, const int (&c)[5])
+{
+    tma_load_3d(dst, tm, bar, c[0], c[1], c[2]);
+}
+
+__device__ __forceinline__ void tma_load_5d_pair(void* dst, const CUtensorMap* tm, uint32_t bar_cluster, const int (&c)[5])
+{
+    asm volatile(
+        "cp.async.bulk.tensor.5d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6, %7}], [%2];"
+        ::"r"(smem_u32(dst)), "l"(tm), "r"(bar_cluster), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(c[4])
+        : "memory");
+}
+
 // address of the same shared-memory location in CTA `rank` of the cluster
 __device__ __forceinline__ uint32_t cluster_addr(const void* p, uint32_t rank)
 {
@@ -623,6 +666,20 @@ __device__ __forceinline__ void mma_i8_pair(uint32_t tmem_d, uint64_t da, uint64
         "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n\t}"
         ::"r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accumulate)
         : "memory");
+}
+
+// MN-major operand tile with 128-byte swizzle: 64-element (128-byte) rows
+// along M/N holding one k each, 8 k-rows per 1024-byte group (SBO), the
+// second 64-row half of the tile 8 KiB further (LBO)
+__device__ __forceinline__ uint64_t smem_desc_mn(uint32_t addr)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((addr & 0x3FFFF) >> 4);
+    d |= (uint64_t)(8192 >> 4) << 16;   // leading byte offset: between 64-row halves
+    d |= (uint64_t)(1024 >> 4) << 32;   // stride byte offset: between 8-k groups
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)2 << 61;             // SWIZZLE_128B
+    return d;
 }
 
 __device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t accumulate)
@@ -773,9 +830,15 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     const int num_items = p.num_tiles + p.split_tiles;
     const int my_tiles = num_items > unit ? (num_items - 1 - unit) / units + 1 : 0;
 
-    if (warp == 0) {
+    // in-place operands take up to six 8 KB boxes a stage: warp 0 issues A's
+    // (and the stage's expected bytes), warp 3 B's, so the two issue streams
+    // overlap; a box that lands before the expectation only drives the
+    // barrier's transaction count below zero for a moment
+    const bool two_producers = p.a_direct || p.b_direct;
+    if (warp == 0 || (warp == 3 && two_producers)) {
         // ---------------- TMA producer ----------------
         if (lane == 0) {
+            const bool do_a = warp == 0, do_b = warp == 3 || !two_producers;
             uint32_t g = 0;
             int64_t last_issued[NS];
             for (int s = 0; s < NS; s++) last_issued[s] = -1;
@@ -787,26 +850,108 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                 const int rest = tile / p.tiles_m;
                 const int tn = rest % p.tiles_n;
                 const int l = rest / p.tiles_n;
+                // in-place operands: row coordinates of this tile's 64-row
+                // chunks (fixed for the tile) and the contraction coordinate
+                // stepped by 64 per block (no divisions in the loop below)
+                const int arow = tm * G::tile_m + (int)rank * BM, brow = tn * BN + (int)rank * G::b_rows;
+                int ar0[2] = {0, 0}, ar1[2] = {0, 0}, br0[4] = {0, 0, 0, 0}, br1[4] = {0, 0, 0, 0};
+                int akc0 = 0, akc1 = 0, bkc0 = 0, bkc1 = 0;
+                if (p.a_direct && do_a) {
+#pragma unroll
+                    for (int c = 0; c < 2; c++) {
+                        ar0[c] = (arow + 64 * c) % p.a_e0;
+                        ar1[c] = (arow + 64 * c) / p.a_e0;
+                    }
+                    akc0 = (it.kb0 * BK) % p.a_k0;
+                    akc1 = (it.kb0 * BK) / p.a_k0;
+                }
+                if (p.b_direct && do_b) {
+#pragma unroll
+                    for (int c = 0; c < 4; c++) {
+                        br0[c] = (brow + 64 * c) % p.b_e0;
+                        br1[c] = (brow + 64 * c) / p.b_e0;
+                    }
+                    bkc0 = (it.kb0 * BK) % p.b_k0;
+                    bkc1 = (it.kb0 * BK) / p.b_k0;
+                }
                 for (int kb = it.kb0; kb < it.kb1; kb++, g++) {
                     const int s = g % NS;
                     const uint32_t ph = (g / NS) & 1;
                     if (!mbar_wait(&empty[s], ph ^ 1, abort_flag)) { ok = false; break; }
                     uint8_t* a = tiles + s * G::stage_bytes;
-                    if (CTA2) {
+                    // one chunk of an in-place operand: logical coordinates
+                    // (row0, k0, row1, k1, batch) or (k0, row0, k1, row1,
+                    // batch), then those of the dims the map keeps
+                    auto chunk = [&](uint8_t* dst, const CUtensorMap* tm_, int rc0, int rc1, int kc0, int kc1, int mn,
+                                     int dims, uint32_t fb) {
+                        const int c0 = mn ? rc0 : kc0, c1 = mn ? kc0 : rc0, c2 = mn ? rc1 : kc1, c3 = mn ? kc1 : rc1;
+                        int q[5] = {c0, c1, 0, 0, 0};
+                        int n = 2;
+                        if (dims & 4) { q[2] = c2; n = 3; }
+                        if (dims & 8) {
+                            if (n == 2) q[2] = c3; else q[3] = c3;
+                            n++;
+                        }
+                        if (dims & 16) {
+                            if (n == 2) q[2] = l; else if (n == 3) q[3] = l; else q[4] = l;
+                            n++;
+                        }
+                        if (n <= 3) {
+                            if (CTA2) tma_load_3d_pair(dst, tm_, fb, q[0], q[1], q[2]);
+                            else tma_load_3d(dst, tm_, &full[s], q[0], q[1], q[2]);
+                        } else if (n == 4) {
+                            if (CTA2) tma_load_4d_pair(dst, tm_, fb, q);
+                            else tma_load_4d(dst, tm_, &full[s], q);
+                        } else {
+                            if (CTA2) tma_load_5d_pair(dst, tm_, fb, q);
+                            else tma_load_5d(dst, tm_, &full[s], q);
+                        }
+                    };
+                    const uint32_t fb = CTA2 ? cluster_addr(&full[s], 0) : 0;
+                    if (!do_a) {
+                    } else if (CTA2) {
                         // both halves land on the leader's barrier, which expects the pair's bytes
-                        const uint32_t fb = cluster_addr(&full[s], 0);
                         if (rank == 0) mbar_expect_tx(&full[s], 2 * G::stage_bytes);
-                        tma_load_3d_pair(a, &tmA, fb, kb * KSTEP, tm * G::tile_m + (int)rank * BM, l);
-                        tma_load_3d_pair(a + G::a_bytes, &tmB, fb, kb * KSTEP, tn * BN + (int)rank * G::b_rows, l);
                     } else {
                         mbar_expect_tx(&full[s], G::stage_bytes);
+                    }
+                    if (!do_a) {
+                    } else if (p.a_direct) {
+                        const int nc = p.a_box ? 1 : BM / 64;
+#pragma unroll
+                        for (int c = 0; c < 2; c++)
+                            if (c < nc) chunk(a + c * 8192, &tmA, ar0[c], ar1[c], akc0, akc1, p.a_mn, p.a_dims, fb);
+                        if ((akc0 += BK) == p.a_k0) { akc0 = 0; akc1++; }
+                    } else if (CTA2) {
+                        tma_load_3d_pair(a, &tmA, fb, kb * KSTEP, arow, l);
+                    } else {
                         tma_load_3d(a, &tmA, &full[s], kb * KSTEP, tm * BM, l);
+                    }
+                    if (!do_b) {
+                    } else if (p.b_direct) {
+                        const int nc = p.b_box ? 1 : G::b_rows / 64;
+#pragma unroll
+                        for (int c = 0; c < 4; c++)
+                            if (c < nc)
+                                chunk(a + G::a_bytes + c * 8192, &tmB, br0[c], br1[c], bkc0, bkc1, p.b_mn, p.b_dims, fb);
+                        if ((bkc0 += BK) == p.b_k0) { bkc0 = 0; bkc1++; }
+                    } else if (CTA2) {
+                        tma_load_3d_pair(a + G::a_bytes, &tmB, fb, kb * KSTEP, brow, l);
+                    } else {
                         tma_load_3d(a + G::a_bytes, &tmB, &full[s], kb * KSTEP, tn * BN, l);
                     }
                     last_issued[s] = g;
                 }
             }
-            if (!CTA2 || rank == 0) {
+            if (!do_a) {
+                // warp 0 drains the stages: a phase completes only when the
+                // boxes of both producers have landed
+                if (CTA2 && rank != 0 && !ok) {
+                    const unsigned long long t0 = now_ns();
+                    while (now_ns() - t0 < 200000ull) {
+                    }
+                }
+            } else if (!CTA2 || rank == 0) {
                 // every issued load must land before the block exits: the phase of
                 // the last load issued on a stage stays complete once reached
                 int never = 0;
@@ -843,7 +988,13 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                     const uint32_t b = a + G::a_bytes;
 #pragma unroll
                     for (int k = 0; k < BK / 16; k++) {  // 32 bytes of K per instruction
-                        if (EPI == EPI_I32) {
+                        if (EPI != EPI_I32 && (p.a_mn | p.b_mn)) {
+                            // an MN-major operand advances 16 k-rows (2048 bytes) per instruction
+                            const uint64_t da = p.a_mn ? smem_desc_mn(a + k * 2048) : smem_desc(a + k * 32);
+                            const uint64_t db = p.b_mn ? smem_desc_mn(b + k * 2048) : smem_desc(b + k * 32);
+                            if (CTA2) mma_f16_pair(d_tmem, da, db, idesc, (kr | k) != 0);
+                            else mma_f16(d_tmem, da, db, idesc, (kr | k) != 0);
+                        } else if (EPI == EPI_I32) {
                             if (CTA2) mma_i8_pair(d_tmem, smem_desc(a + k * 32), smem_desc(b + k * 32), idesc, (kr | k) != 0);
                             else mma_i8(d_tmem, smem_desc(a + k * 32), smem_desc(b + k * 32), idesc, (kr | k) != 0);
                         } else {
@@ -1457,6 +1608,108 @@ cudaError_t launch_gemm_i8(const void* A8, const void* B8, int64_t row_bytes, in
     return e;
 }
 
+// Tensor map reading an operand in place (16-bit storage of the product's
+// 16-bit precision, real, no unary modes): dims (row0, k0, row1, k1, batch)
+// when the first row mode is contiguous (MN-major tiles) or (k0, row0, k1,
+// row1, batch) when the first contracted mode is (K-major tiles); box 64 x 64.
+// False when the layout does not allow it (more than two row or contracted
+// modes or one batch mode, extents of the leading modes not multiples of 64,
+// strides not positive multiples of 16 bytes, base not 16-byte aligned).
+static bool make_direct_map(CUtensorMap* tm, const void* base, const tb_plan* P, int side, int rows, int* mn, int* e0,
+                            int* k0, int* boxmode, int* dmask)
+{
+    using namespace tc;
+    EncodeTiledFn enc = encode_fn();
+    const tb_modes& R = side == 0 ? P->M : P->N;
+    const tb_modes& K = P->K;
+    const tb_modes& L = P->L;
+    auto st = [&](const tb_modes& m, int j) { return side == 0 ? m.sA[j] : m.sB[j]; };
+    if (!enc || !base || ((uintptr_t)base & 15) || R.n < 1 || R.n > 2 || K.n < 1 || K.n > 2 || L.n > 1) return false;
+    int major;
+    if (st(R, 0) == 1 && R.ext[0] % 64 == 0 && K.ext[0] % 64 == 0) major = 1;
+    else if (st(K, 0) == 1 && K.ext[0] % 64 == 0 && R.ext[0] % 64 == 0) major = 0;
+    else return false;
+    cuuint64_t dims[5];
+    int64_t str[5];
+    const tb_modes* first = major ? &R : &K;
+    const tb_modes* second = major ? &K : &R;
+    dims[0] = (cuuint64_t)first->ext[0];
+    str[0] = 1;
+    dims[1] = (cuuint64_t)second->ext[0];
+    str[1] = st(*second, 0);
+    dims[2] = first->n > 1 ? (cuuint64_t)first->ext[1] : 1;
+    str[2] = first->n > 1 ? st(*first, 1) : str[1];
+    dims[3] = second->n > 1 ? (cuuint64_t)second->ext[1] : 1;
+    str[3] = second->n > 1 ? st(*second, 1) : str[2];
+    dims[4] = L.n ? (cuuint64_t)L.ext[0] : 1;
+    str[4] = L.n ? st(L, 0) : str[3];
+    cuuint64_t strides[4];
+    for (int j = 1; j < 5; j++) {
+        if (str[j] <= 0 || (str[j] * 2) % 16 != 0 || str[j] * 2 >= (1ll << 40)) return false;
+        strides[j - 1] = (cuuint64_t)(str[j] * 2);
+    }
+    // one box per tile when the rows allow it (fewer, larger copies)
+    cuuint32_t box[5] = {64, 64, 1, 1, 1};
+    int bm = 0;
+    if (R.ext[0] == 64 && R.n == 2 && R.ext[1] >= rows / 64) {
+        bm = 1;
+        box[major ? 2 : 3] = (cuuint32_t)(rows / 64);
+    } else if (!major && R.ext[0] % rows == 0) {
+        bm = 2;
+        box[1] = (cuuint32_t)rows;
+    }
+    cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    const int fmt = P->tc_mode == TB_TC_F16 ? 1 : 0;
+    // keep dims 0 and 1 and every dim of extent > 1; a 3-d map at least
+    cuuint64_t cd[5];
+    cuuint64_t cs[4];
+    cuuint32_t cb[5];
+    int rank = 0, mask = 0;
+    int64_t cstr[5];
+    for (int j = 0; j < 5; j++) {
+        if (j >= 2 && dims[j] == 1) continue;
+        cd[rank] = dims[j];
+        cstr[rank] = j == 0 ? 1 : str[j];
+        cb[rank] = box[j];
+        mask |= 1 << j;
+        rank++;
+    }
+    for (int j = 2; rank < 3 && j < 5; j++)
+        if (!(mask >> j & 1)) {  // pad with a unit dim, in logical order
+            mask |= 1 << j;
+            rank = 0;
+            for (int i = 0; i < 5; i++)
+                if (mask >> i & 1) {
+                    cd[rank] = dims[i];
+                    cstr[rank] = i == 0 ? 1 : str[i];
+                    cb[rank] = box[i];
+                    rank++;
+                }
+        }
+    for (int j = 1; j < rank; j++) cs[j - 1] = (cuuint64_t)(cstr[j] * 2);
+    if (enc(tm, fmt == 1 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, rank, const_cast<void*>(base),
+            cd, cs, cb, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+    *mn = major;
+    *e0 = (int)R.ext[0];
+    *k0 = (int)K.ext[0];
+    *boxmode = bm;
+    *dmask = mask;
+    return true;
+}
+
+// whether an operand can be read in place (besides its layout, checked by
+// make_direct_map): its storage is the product's 16-bit operand type
+static bool direct_type_ok(const tb_plan* P, int side)
+{
+    const int t = side == 0 ? P->tA : P->tB;
+    const int need = P->tc_mode == TB_TC_BF16 ? T_BF16 : P->tc_mode == TB_TC_F16 ? T_F16 : -1;
+    const tb_modes& U = side == 0 ? P->UA : P->UB;
+    return t == need && U.n == 0 && P->compute == TB_R32 && (int64_t)P->K.size < (1ll << 31) &&
+           (side == 0 ? P->M.size : P->N.size) < (1ll << 31);
+}
+
 // Batches per launch group of a batched product: the panels of one group at
 // most 2 GiB (one batch always), grid.z = batches x batch modes <= 65535.
 static int64_t group_batches(int64_t num, size_t per_batch, int64_t Lsz, int64_t tiles_per_batch)
@@ -1541,8 +1794,20 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
         void* pA = base;
         void* pB = base + round_up((int64_t)(bytesA * G), 256);
 
+        // operands read in place need no pack (single products only: the maps
+        // describe one batch's tensors)
+        CUtensorMap dmap[2];
+        int dir[2] = {0, 0}, dmn[2] = {0, 0}, de0[2] = {0, 0}, dk0[2] = {0, 0}, dbox[2] = {0, 0}, dmask[2] = {0, 0};
+        if (G == 1 && split == 1)
+            for (int side = 0; side < 2; side++)
+                dir[side] = direct_type_ok(P, side) &&
+                            make_direct_map(&dmap[side], side == 0 ? d[b0].A : d[b0].B, P, side,
+                                            side == 0 ? BM : (cta2 ? Geo<true>::b_rows : BN), &dmn[side], &de0[side],
+                                            &dk0[side], &dbox[side], &dmask[side]);
+
         // pack A and B
         for (int side = 0; side < 2; side++) {
+            if (dir[side]) continue;
             PackParams pp;
             memset(&pp, 0, sizeof(pp));
             pp.src = side == 0 ? d[b0].A : d[b0].B;
@@ -1590,8 +1855,10 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
         if (e != cudaSuccess) break;
 
         CUtensorMap tmA, tmB;
-        if (!make_map(&tmA, pA, fmt, Kld, M, Lg, BM) ||
-            !make_map(&tmB, pB, fmt, Kld, Nout, Lg, cta2 ? Geo<true>::b_rows : BN)) {
+        if (dir[0]) tmA = dmap[0];
+        if (dir[1]) tmB = dmap[1];
+        if ((!dir[0] && !make_map(&tmA, pA, fmt, Kld, M, Lg, BM)) ||
+            (!dir[1] && !make_map(&tmB, pB, fmt, Kld, Nout, Lg, cta2 ? Geo<true>::b_rows : BN))) {
             e = cudaErrorInvalidValue;
             break;
         }
@@ -1602,6 +1869,18 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
         gp.num_tiles = gp.tiles_m * gp.tiles_n * (int)Lg;
         gp.num_kb = (int)((Kld + BK - 1) / BK);
         gp.error = flag;
+        gp.a_direct = dir[0];
+        gp.b_direct = dir[1];
+        gp.a_mn = dir[0] && dmn[0];
+        gp.b_mn = dir[1] && dmn[1];
+        gp.a_e0 = de0[0];
+        gp.a_k0 = dk0[0];
+        gp.b_e0 = de0[1];
+        gp.b_k0 = dk0[1];
+        gp.a_box = dbox[0];
+        gp.b_box = dbox[1];
+        gp.a_dims = dmask[0];
+        gp.b_dims = dmask[1];
         EpiParams& ep = gp.e;
         ep.C = d[b0].C;
         ep.D = d[b0].D;
@@ -1630,8 +1909,8 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
         fill_modes(ep.ll, P->L, 2, 3);
         const uint32_t ab = fmt == 1 ? 0u : 1u;  // operand format: 0 f16, 1 bf16
         const uint32_t mma_m = cta2 ? 2 * BM : BM;
-        const uint32_t idesc = (1u << 4) | (ab << 7) | (ab << 10) | ((uint32_t)(BN >> 3) << 17) |
-                               ((mma_m >> 4) << 24);
+        const uint32_t idesc = (1u << 4) | (ab << 7) | (ab << 10) | ((uint32_t)gp.a_mn << 15) |
+                               ((uint32_t)gp.b_mn << 16) | ((uint32_t)(BN >> 3) << 17) | ((mma_m >> 4) << 24);
         const bool f32_epi = !cplx && P->tD == T_F32 && (P->beta_zero || P->tC == T_F32) && !P->conjD;
         CUtensorMap tmC = tmA, tmD = tmA;  // placeholders when the TMA epilogue is not used
         bool tma_epi = false;

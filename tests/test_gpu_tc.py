@@ -281,3 +281,62 @@ def test_batched_tma_epilogue_per_batch_maps(tapp, gpu, beta):
     ex = tc_executor(tapp)
     assert _batched_against_single(tapp, cases, ex) == 3
     tapp.lib.TAPP_destroy_executor(ex)
+
+
+def _mm16(rng, n, storage, prec, a_t, b_t):
+    """D[a,b] = sum_k A B + 0.5 C with 16-bit A and B (storage), binary32 C
+    and D; a_t / b_t store A as [k,a] and B as [b,k] instead of [a,k], [k,b]."""
+    from tapp_b200.case import alloc, fill_uniform, scalar, Case
+    ak = [ord("k"), ord("a")] if a_t else [ord("a"), ord("k")]
+    bk = [ord("b"), ord("k")] if b_t else [ord("k"), ord("b")]
+    def t(dtype, idx):
+        T = alloc(dtype, [n, n], [1, n], idx)
+        fill_uniform(T, rng)
+        return T
+    A, B = t(storage, ak), t(storage, bk)
+    Cc, D = t(0, [ord("a"), ord("b")]), t(0, [ord("a"), ord("b")])
+    return Case(A, B, Cc, D, scalar(0, 1.0), scalar(0, 0.5), prec, False, "mm16")
+
+
+@pytest.mark.parametrize("storage,prec", [(5, 6), (4, 5)])
+@pytest.mark.parametrize("a_t,b_t", [(False, False), (True, True), (True, False), (False, True)])
+def test_16bit_operands_read_in_place(tapp, oracle, gpu, storage, prec, a_t, b_t):
+    """16-bit operands of the product's own type are read by the GEMM in place
+    through 5-d tensor maps (MN-major tiles when rows are contiguous, K-major
+    when the contraction is): no pack launch, same result bound."""
+    from test_gpu_parity import _run_with_status
+    rng = np.random.default_rng(500 + storage + 2 * a_t + b_t)
+    case = _mm16(rng, 256, storage, prec, a_t, b_t)
+    ex = tc_executor(tapp)
+    check_against_f64(tapp, oracle, case, device=True, executor=ex)
+    import ctypes as C
+    import torch
+    infos = [tapp.tensor_info(t.dtype, t.extents, t.strides)[1] for t in (case.A, case.B, case.C, case.D)]
+    _, plan = tapp.create_product(0, [0, 0, 0, 0], infos, [case.A.idx, case.B.idx, case.C.idx, case.D.idx], prec)
+    dev = [torch.from_numpy(t.buf.view(np.uint8).copy()).cuda() for t in (case.A, case.B, case.C, case.D)]
+    st = tapp_b200.intptr(0)
+    assert tapp.lib.TAPP_execute_product(plan, ex, C.byref(st), case.alpha.ctypes.data, dev[0].data_ptr(),
+                                         dev[1].data_ptr(), case.beta.ctypes.data, dev[2].data_ptr(),
+                                         dev[3].data_ptr()) == 0
+    assert tapp.status_value(st.value, tapp_b200.STATUS_KERNELS) == 1   # the GEMM alone
+    tapp.lib.TAPP_destroy_status(st.value)
+    tapp.lib.TAPP_destroy_tensor_product(plan)
+    tapp.lib.TAPP_destroy_executor(ex)
+
+
+@pytest.mark.parametrize("storage,prec", [(5, 6), (4, 5)])
+def test_16bit_4index_in_place_sampled(tapp, oracle, gpu, storage, prec):
+    """The 64^4 contraction with 16-bit A and B: A[a,c,i,d] is read MN-major
+    (a contiguous), B[d,b,c,j] K-major (d contiguous), both as 64 x 64 boxes of
+    5-d maps; 4096 sampled outputs against binary64."""
+    case = large_dense_case(np.random.default_rng(510 + prec), prec, storage, extent=64)
+    ex = tc_executor(tapp)
+    run = case.copy()
+    assert run_on_device(tapp, run, ex) == 0
+    samples = np.random.default_rng(511).integers(0, 64 ** 4, 4096)
+    err, D64, scale, offs = oracle.execute_f64(case.copy(), samples=samples)
+    got = run.D.buf[run.D.base + offs].astype(np.complex128)
+    n = 4096 + 8
+    bound = n * 2.0 ** -24 / (1 - n * 2.0 ** -24) * scale + 2 * 2.0 ** -24 * np.abs(D64)
+    assert (np.abs(got - D64) <= bound).all()
+    tapp.lib.TAPP_destroy_executor(ex)
