@@ -603,7 +603,7 @@ def served_measure(lib, torch, n, seed=5, max_tensor_bytes=1 << 30):
     specs = served_stream(rng, n, max_tensor_bytes=max_tensor_bytes)
     run = StreamRunner(lib, specs, torch, seed=seed)
     ex = make_executor(lib, None, async_=False)
-    run.run_plain(ex, order=range(min(n, 64)))      # warm-up: module loads, pool growth
+    run.run_plain(ex)      # warm-up over the whole stream: first-use kernel loads, pool growth
     service = run.run_plain(ex)
     lib.lib.TAPP_destroy_executor(ex)
     t_plain = float(service.sum())

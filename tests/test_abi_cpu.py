@@ -217,3 +217,29 @@ def test_planner_merges_contiguous_modes(tapp):
     assert " M=[(12:1,0,1,1)]" in d, d
     assert " N=[(6:0,5,12,12)]" in d, d
     assert " K=[(5:12,1,0,0)]" in d, d
+
+
+@pytest.mark.parametrize("dims,path", [
+    # D[a,h] = sum_{b,c,e} A[a,b,c,h,e] B[e,b,h,c]: 4565 outputs x 17,172 terms
+    (([55, 54, 53, 83, 6], [6, 54, 83, 53], [55, 83]), "reduce"),
+    # 666 outputs x 5160 terms
+    (([18, 86, 37, 60], [86, 60, 37], [18, 37]), "reduce"),
+    # 200 x 40 outputs x 30 terms: short contractions stay one thread per output
+    (([200, 30, 40], [30, 40], [200, 40]), "generic"),
+])
+def test_planner_long_contraction_few_outputs(tapp, dims, path):
+    """Hadamard products with few outputs for one thread each and a long
+    contraction take the block-per-output reduction path."""
+    from tapp_b200.workloads import colmajor
+    ea, eb, ed = dims
+    if len(ea) == 5:
+        ia, ib, idd = [0, 1, 2, 3, 4], [4, 1, 3, 2], [0, 3]
+    elif len(ea) == 4:
+        ia, ib, idd = [0, 1, 2, 3], [1, 3, 2], [0, 2]
+    else:
+        ia, ib, idd = [0, 1, 2], [1, 2], [0, 2]
+    ts = [alloc(0, e, colmajor(e), i) for e, i in ((ea, ia), (eb, ib), (ed, idd), (ed, idd))]
+    case = Case(*ts, scalar(0, 1.0), scalar(0, 1.0), -1)
+    plan, infos = _plan(tapp, case)
+    assert f"path={path}" in tapp.describe(plan), tapp.describe(plan)
+    tapp.lib.TAPP_destroy_tensor_product(plan)
