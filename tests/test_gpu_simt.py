@@ -173,3 +173,17 @@ def test_few_outputs_split_reduction(tapp, oracle, gpu, storage, prec):
     assert "path=reduce" in describe(tapp, case, ex)
     check_against_f64(tapp, oracle, case, device=False, executor=ex)
     tapp.lib.TAPP_destroy_executor(ex)
+
+
+@pytest.mark.parametrize("storage,prec", [(0, 0), (1, -1), (2, -1), (3, -1), (0, 6)])
+def test_hadamard_long_contraction_reduction(tapp, oracle, gpu, storage, prec):
+    """D[a,h] = sum_{b,c,e} A[a,b,c,h,e] B[e,b,h,c]: 1200 outputs (a Hadamard
+    mode of 40) of 2880 terms each, too few outputs to give each a thread:
+    one block per output on the reduction path."""
+    rng = np.random.default_rng(130 + storage + prec)
+    case = spec_case(rng, storage, prec, ([30, 24, 20, 40, 6], [6, 24, 40, 20], [30, 40], [30, 40]),
+                     ([0, 1, 2, 3, 4], [4, 1, 3, 2], [0, 3], [0, 3]), kind="hadamard")
+    ex = tapp.create_executor()
+    assert "path=reduce" in describe(tapp, case, ex)
+    check_against_f64(tapp, oracle, case, device=True, executor=ex)
+    tapp.lib.TAPP_destroy_executor(ex)
