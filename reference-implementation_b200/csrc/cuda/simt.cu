@@ -345,7 +345,7 @@ struct NarrowParams {
     Params p;
     FastDiv fm[TB_MAXMODES];  // M extents
     int32_t nb;               // padded N
-    int32_t pad;
+    int32_t stage_c;          // streaming kernel: C (stored as T) staged in shared memory
 };
 
 // DIRECT: A is stored as T and not rounded (plain loads, no type dispatch)
@@ -458,6 +458,229 @@ __global__ void __launch_bounds__(256) k_narrow(NarrowParams np)
             }
         }
     }
+}
+
+// Streaming variant of k_narrow for A stored as T with no rounding: every
+// thread copies its own row of A into its own column of a shared-memory ring
+// with cp.async (S chunks of KC contracted values, S - 1 of them in flight
+// while one is multiplied), across tile boundaries, so the latency of HBM is
+// covered by the copies in flight instead of by registers. A thread only
+// reads what it copied itself: cp.async.wait_group orders the two, and no
+// block barrier is needed after the B panel is staged.
+template <typename T>
+struct StreamRing {
+    static constexpr int KC = sizeof(T) == 4 ? 16 : 8;  // contracted values per chunk
+    static constexpr int S = 4;                         // chunks in the ring
+    static constexpr size_t bytes = sizeof(T) * (size_t)KC * S * 256;
+};
+
+__device__ __forceinline__ void cp_async_elem4(uint32_t dst, const void* src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_elem8(uint32_t dst, const void* src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+template <typename T, int NB>
+__global__ void __launch_bounds__(256) k_narrow_stream(NarrowParams np)
+{
+    using RING = StreamRing<T>;
+    constexpr int KC = RING::KC, S = RING::S;
+    const Params& p = np.p;
+    extern __shared__ __align__(16) unsigned char nsm[];
+    T* ring = (T*)nsm;                                       // [S][KC][256]
+    const size_t cbytes = np.stage_c ? sizeof(T) * NB * 256 : 0;
+    T* Cs = (T*)(nsm + RING::bytes);                         // [NB][256] when staged
+    T* Bs = (T*)(nsm + RING::bytes + cbytes);                // [K][NB]
+    int64_t* kA = (int64_t*)(nsm + RING::bytes + cbytes + sizeof(T) * NB * p.K);  // [K]
+    int64_t* nC = kA + p.K;                                  // [NB]
+    int64_t* nD = nC + NB;                                   // [NB]
+    const int t = threadIdx.x;
+    const int64_t l = blockIdx.y;
+    int64_t lA, lB, lC, lD, dummy;
+    decode(p.al, l, lA, dummy);
+    decode(p.bl, l, lB, dummy);
+    decode(p.cl, l, lC, lD);
+    for (int64_t k = t; k < p.K; k += 256) {
+        int64_t o;
+        decode(p.ak, k, o, dummy);
+        kA[k] = o + lA;
+    }
+    if (t < NB) {
+        int64_t oc = 0, od = 0;
+        if (t < p.N) decode(p.cn, t, oc, od);
+        nC[t] = oc + lC;
+        nD[t] = od + lD;
+    }
+    for (int64_t e = t; e < p.K * NB; e += 256) {
+        const int64_t k = e / NB;
+        const int n = (int)(e % NB);
+        T x = 0, xi = 0;
+        if (n < p.N) {
+            int64_t ob, ok;
+            decode(p.bn, n, ob, dummy);
+            decode(p.bk, k, ok, dummy);
+            load_rounded<T>(p.B, lB + ob + ok, p.tB, p.round_in, x, xi);
+        }
+        Bs[k * NB + n] = x;
+    }
+    __syncthreads();
+
+    const int64_t tiles = (p.M + 255) / 256;
+    if ((int64_t)blockIdx.x >= tiles) return;
+    const int64_t my_tiles = (tiles - 1 - blockIdx.x) / gridDim.x + 1;
+    const int nchunks = (int)((p.K + KC - 1) / KC);
+    const int64_t total = my_tiles * nchunks;
+    const T* A = (const T*)p.A;
+    const uint32_t ring_base = (uint32_t)__cvta_generic_to_shared(ring) + (uint32_t)t * sizeof(T);
+
+    // offsets of this thread's row in tile i (A; C and D), -1: no row
+    auto row_offsets = [&](int64_t i, int64_t& oA, int64_t& oC, int64_t& oD) {
+        const int64_t m = ((int64_t)blockIdx.x + i * gridDim.x) * 256 + t;
+        oA = oC = oD = -1;
+        if (m >= p.M) return;
+        oA = oC = oD = 0;
+        uint32_t r = (uint32_t)m;
+        for (int j = 0; j < p.am.n; j++) {
+            const uint32_t q = fdiv(r, np.fm[j]);
+            const int64_t c = (int64_t)(r - q * np.fm[j].d);
+            r = q;
+            oA += c * p.am.s0[j];
+            oC += c * p.cm.s0[j];
+            oD += c * p.cm.s1[j];
+        }
+    };
+    // producer: the copies of chunk g (tile g / nchunks, chunk g % nchunks)
+    int64_t p_tile = -1, p_oA = -1;
+    int p_chunk = 0;
+    auto issue = [&](int64_t g) {
+        if (g < total) {
+            if (p_chunk == 0) {
+                p_tile++;
+                int64_t c_, d_;
+                row_offsets(p_tile, p_oA, c_, d_);
+            }
+            if (p_oA >= 0) {
+                const int k0 = p_chunk * KC;
+                const uint32_t dst = ring_base + (uint32_t)((g % S) * KC * 256) * sizeof(T);
+#pragma unroll
+                for (int kk = 0; kk < KC; kk++) {
+                    if (k0 + kk < p.K) {
+                        const T* src = A + p_oA + kA[k0 + kk];
+                        if (sizeof(T) == 4) cp_async_elem4(dst + kk * 256 * sizeof(T), src);
+                        else cp_async_elem8(dst + kk * 256 * sizeof(T), src);
+                    }
+                }
+            }
+            if (++p_chunk == nchunks) p_chunk = 0;
+        }
+        cp_async_commit();  // empty groups keep the count uniform
+    };
+#pragma unroll
+    for (int g = 0; g < S - 1; g++) issue(g);
+
+    T acc[NB];
+    int64_t oA = -1, oC = -1, oD = -1;
+    int c = 0;
+    int64_t ti = 0;
+    const T al = (T)p.alpha, be = (T)p.beta;
+    const uint32_t cs_base = (uint32_t)__cvta_generic_to_shared(Cs) + (uint32_t)t * sizeof(T);
+    // the copies of C join the group committed next, so at the tile's last
+    // chunk at most min(S - 1, nchunks - 1) younger groups may be pending
+    const int c_pending = nchunks - 1 < S - 1 ? nchunks - 1 : S - 1;
+    for (int64_t g = 0; g < total; g++) {
+        if (c == 0) {
+            row_offsets(ti, oA, oC, oD);
+#pragma unroll
+            for (int n = 0; n < NB; n++) acc[n] = 0;
+            if (np.stage_c && oA >= 0) {
+                for (int n = 0; n < p.N; n++) {
+                    const T* src = (const T*)p.C + oC + nC[n];
+                    if (sizeof(T) == 4) cp_async_elem4(cs_base + n * 256 * sizeof(T), src);
+                    else cp_async_elem8(cs_base + n * 256 * sizeof(T), src);
+                }
+            }
+        }
+        issue(g + S - 1);
+        cp_async_wait<S - 1>();  // this thread's copies of chunk g have landed
+        if (oA >= 0) {
+            const T* a = ring + (size_t)(g % S) * KC * 256 + t;
+            const int k0 = c * KC;
+            const int kn = p.K - k0 < KC ? (int)(p.K - k0) : KC;
+            // B rows as 16-byte vectors (NB is a multiple of 8, the panel
+            // 16-byte aligned); a short unroll keeps the loop in the
+            // instruction cache
+#pragma unroll 2
+            for (int kk = 0; kk < kn; kk++) {
+                const T x = a[kk * 256];
+                const T* b = Bs + (k0 + kk) * NB;
+                if (sizeof(T) == 4) {
+#pragma unroll
+                    for (int n = 0; n < NB; n += 4) {
+                        const float4 q = *(const float4*)((const float*)b + n);
+                        acc[n] = fma(x, (T)q.x, acc[n]);
+                        acc[n + 1] = fma(x, (T)q.y, acc[n + 1]);
+                        acc[n + 2] = fma(x, (T)q.z, acc[n + 2]);
+                        acc[n + 3] = fma(x, (T)q.w, acc[n + 3]);
+                    }
+                } else {
+#pragma unroll
+                    for (int n = 0; n < NB; n += 2) {
+                        const double2 q = *(const double2*)((const double*)b + n);
+                        acc[n] = fma(x, (T)q.x, acc[n]);
+                        acc[n + 1] = fma(x, (T)q.y, acc[n + 1]);
+                    }
+                }
+            }
+        }
+        if (++c == nchunks) {
+            c = 0;
+            ti++;
+            if (oA >= 0 && np.stage_c) {
+                switch (c_pending) {
+                case 0: cp_async_wait<0>(); break;
+                case 1: cp_async_wait<1>(); break;
+                case 2: cp_async_wait<2>(); break;
+                default: cp_async_wait<3>(); break;
+                }
+                const bool d_as_t = p.tD == (sizeof(T) == 4 ? T_F32 : T_F64);
+#pragma unroll
+                for (int n = 0; n < NB; n++) {
+                    if (n < p.N) {
+                        T v = fma(be, Cs[n * 256 + t], al * acc[n]);
+                        if (p.conjD && p.conjD_f32) v = (T)(float)v;  // op_D under the F64 precision rounds as conjf
+                        if (d_as_t) ((T*)p.D)[oD + nD[n]] = v;
+                        else store_elem<T>(p.D, oD + nD[n], p.tD, v, (T)0);
+                    }
+                }
+            } else if (oA >= 0) {
+#pragma unroll
+                for (int gq = 0; gq < NB; gq += 8) {
+                    T cv[8];
+#pragma unroll
+                    for (int j = 0; j < 8; j++) {
+                        T im;
+                        cv[j] = 0;
+                        if (!p.beta_zero && gq + j < p.N) load_rounded<T>(p.C, oC + nC[gq + j], p.tC, p.round_in, cv[j], im);
+                    }
+#pragma unroll
+                    for (int j = 0; j < 8; j++) {
+                        if (gq + j < p.N) {
+                            T v = p.beta_zero ? al * acc[gq + j] : fma(be, cv[j], al * acc[gq + j]);
+                            if (p.conjD && p.conjD_f32) v = (T)(float)v;  // op_D under the F64 precision rounds as conjf
+                            store_elem<T>(p.D, oD + nD[gq + j], p.tD, v, (T)0);
+                        }
+                    }
+                }
+            }
+        }
+    }
+    cp_async_wait<0>();
 }
 
 // Split of the contraction: enough CTAs to fill the GPU when the tiles do
@@ -637,19 +860,46 @@ static cudaError_t launch_narrow_t(simt::NarrowParams& np, cudaStream_t s)
 {
     using namespace simt;
     const Params& p = np.p;
-    const size_t smem = sizeof(T) * NB * (size_t)p.K + 8 * ((size_t)p.K + 2 * NB);
-    const bool direct = p.tA == (sizeof(T) == 4 ? T_F32 : T_F64) && p.round_in == TB_ROUND_NONE;
-    auto kern = direct ? k_narrow<T, NB, true> : k_narrow<T, NB, false>;
-    static int attr_done[64][2];
+    size_t smem = sizeof(T) * NB * (size_t)p.K + 8 * ((size_t)p.K + 2 * NB);
+    // A read as stored: the streaming kernel (cp.async ring); else the
+    // register-prefetch kernel, which converts and rounds A at load. Not for
+    // binary64 at width 64 (its accumulators leave no registers) nor binary64
+    // products whose D is contiguous along the columns (each thread then
+    // writes a row of its own, and the ring only costs occupancy).
+    constexpr bool stream_ok = !(sizeof(T) == 8 && NB == 64);
+    const bool plain_a = p.tA == (sizeof(T) == 4 ? T_F32 : T_F64) && p.round_in == TB_ROUND_NONE;
+    const bool stream = stream_ok && plain_a && (uintptr_t)p.A % sizeof(T) == 0 && (sizeof(T) == 4 || p.d_rows_fast);
+    void (*kern)(NarrowParams) = plain_a ? k_narrow<T, NB, true> : k_narrow<T, NB, false>;
+    if constexpr (stream_ok) {
+        if (stream) kern = k_narrow_stream<T, NB>;
+    }
+    // C staged when it is read as stored and the shared memory allows
+    np.stage_c = 0;
+    if (stream) {
+        smem += StreamRing<T>::bytes;
+        const size_t cb = sizeof(T) * NB * 256;
+        if (!p.beta_zero && p.tC == (sizeof(T) == 4 ? T_F32 : T_F64) && (uintptr_t)p.C % sizeof(T) == 0 &&
+            smem + cb <= (size_t)NARROW_MAX_SMEM + StreamRing<T>::bytes) {
+            np.stage_c = 1;
+            smem += cb;
+        }
+    }
+    const int variant = stream ? 2 : plain_a ? 1 : 0;
+    static int attr_done[64][3];
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev < 0 || dev >= 64 || !attr_done[dev][direct]) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, NARROW_MAX_SMEM);
+    if (dev < 0 || dev >= 64 || !attr_done[dev][variant]) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             NARROW_MAX_SMEM + (int)StreamRing<T>::bytes);
         if (e != cudaSuccess) return e;
-        if (dev >= 0 && dev < 64) attr_done[dev][direct] = 1;
+        if (dev >= 0 && dev < 64) attr_done[dev][variant] = 1;
     }
     const int64_t tiles = (p.M + 255) / 256;
-    int64_t gx = (148 * 8 + p.L - 1) / p.L;
+    // the streaming kernel: one wave of resident blocks; the others: 8 per SM
+    int per_sm = 8;
+    if (stream && (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem) != cudaSuccess || per_sm < 1))
+        per_sm = 1;
+    int64_t gx = ((int64_t)148 * per_sm + p.L - 1) / p.L;
     if (gx > tiles) gx = tiles;
     if (gx < 1) gx = 1;
     kern<<<dim3((unsigned)gx, (unsigned)p.L), 256, smem, s>>>(np);
