@@ -66,16 +66,15 @@ struct Params {
     void* ws;          // split sums [split][l][m][n][plane], or NULL: epilogue in place
 };
 
-// D = op_D(alpha * acc + beta * op_C(C)) for one element
+// D = op_D(alpha * acc + beta * op_C(C)) for one element whose C value
+// (cr, ci) is already loaded (rounded, not yet conjugated)
 template <typename T, bool CPLX>
-__device__ __forceinline__ void epilogue_store(const Params& p, T xr, T xi, int64_t oc, int64_t od)
+__device__ __forceinline__ void epilogue_store_c(const Params& p, T xr, T xi, T cr, T ci, int64_t od)
 {
     const T ar = (T)p.alpha, ai = (T)p.alpha_im, br = (T)p.beta, bi = (T)p.beta_im;
     T vr = ar * xr - (CPLX ? ai * xi : (T)0);
     T vi = CPLX ? ar * xi + ai * xr : (T)0;
     if (!p.beta_zero) {
-        T cr, ci;
-        load_rounded<T>(p.C, oc, p.tC, p.round_in, cr, ci);
         if (p.conjC) ci = -ci;
         vr = fma(br, cr, vr);
         if (CPLX) {
@@ -91,6 +90,15 @@ __device__ __forceinline__ void epilogue_store(const Params& p, T xr, T xi, int6
         vi = -vi;
     }
     store_elem<T>(p.D, od, p.tD, vr, vi);
+}
+
+// the same, loading C first
+template <typename T, bool CPLX>
+__device__ __forceinline__ void epilogue_store(const Params& p, T xr, T xi, int64_t oc, int64_t od)
+{
+    T cr = 0, ci = 0;
+    if (!p.beta_zero) load_rounded<T>(p.C, oc, p.tC, p.round_in, cr, ci);
+    epilogue_store_c<T, CPLX>(p, xr, xi, cr, ci, od);
 }
 
 template <typename T, bool CPLX, int BM, int BN, int BK, int TM, int TN>
@@ -268,16 +276,25 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN)) k_simt(Params p)
         }
         return;
     }
+    // a row's C values are loaded together (C may alias D, so loads cannot
+    // move past the stores on their own), then its D values stored
 #pragma unroll
     for (int i = 0; i < TM; i++) {
         const int r = tr + i * RT;
         if (m0 + r >= p.M) continue;
+        T cr[TN], ci[TN];
+#pragma unroll
+        for (int j = 0; j < TN; j++) {
+            const int c = tc + j * CT;
+            cr[j] = 0;
+            ci[j] = 0;
+            if (!p.beta_zero && n0 + c < p.N) load_rounded<T>(p.C, cRow[r] + cCol[c], p.tC, p.round_in, cr[j], ci[j]);
+        }
 #pragma unroll
         for (int j = 0; j < TN; j++) {
             const int c = tc + j * CT;
             if (n0 + c >= p.N) continue;
-            epilogue_store<T, CPLX>(p, acc[i][j][0], CPLX ? acc[i][j][NP - 1] : (T)0, cRow[r] + cCol[c],
-                                    dRow[r] + dCol[c]);
+            epilogue_store_c<T, CPLX>(p, acc[i][j][0], CPLX ? acc[i][j][NP - 1] : (T)0, cr[j], ci[j], dRow[r] + dCol[c]);
         }
     }
 }
@@ -486,7 +503,10 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-template <typename T, int NB>
+// RND: A and C are rounded to the precision's 16-bit operand format after
+// their shared-memory reads (binary32 storage only: the same rounding as a
+// rounding load)
+template <typename T, int NB, bool RND>
 __global__ void __launch_bounds__(256) k_narrow_stream(NarrowParams np)
 {
     using RING = StreamRing<T>;
@@ -617,7 +637,8 @@ __global__ void __launch_bounds__(256) k_narrow_stream(NarrowParams np)
             // instruction cache
 #pragma unroll 2
             for (int kk = 0; kk < kn; kk++) {
-                const T x = a[kk * 256];
+                T x = a[kk * 256];
+                if (RND) x = round_in<T>(x, p.round_in);
                 const T* b = Bs + (k0 + kk) * NB;
                 if (sizeof(T) == 4) {
 #pragma unroll
@@ -652,7 +673,9 @@ __global__ void __launch_bounds__(256) k_narrow_stream(NarrowParams np)
 #pragma unroll
                 for (int n = 0; n < NB; n++) {
                     if (n < p.N) {
-                        T v = fma(be, Cs[n * 256 + t], al * acc[n]);
+                        T cv = Cs[n * 256 + t];
+                        if (RND) cv = round_in<T>(cv, p.round_in);
+                        T v = fma(be, cv, al * acc[n]);
                         if (p.conjD && p.conjD_f32) v = (T)(float)v;  // op_D under the F64 precision rounds as conjf
                         if (d_as_t) ((T*)p.D)[oD + nD[n]] = v;
                         else store_elem<T>(p.D, oD + nD[n], p.tD, v, (T)0);
@@ -867,25 +890,33 @@ static cudaError_t launch_narrow_t(simt::NarrowParams& np, cudaStream_t s)
     // products whose D is contiguous along the columns (each thread then
     // writes a row of its own, and the ring only costs occupancy).
     constexpr bool stream_ok = !(sizeof(T) == 8 && NB == 64);
-    const bool plain_a = p.tA == (sizeof(T) == 4 ? T_F32 : T_F64) && p.round_in == TB_ROUND_NONE;
-    const bool stream = stream_ok && plain_a && (uintptr_t)p.A % sizeof(T) == 0 && (sizeof(T) == 4 || p.d_rows_fast);
+    const int t_own = sizeof(T) == 4 ? T_F32 : T_F64;
+    const bool plain_a = p.tA == t_own && p.round_in == TB_ROUND_NONE;
+    // rounding after the copy is the rounding load's only for binary32 storage
+    const bool rnd = p.round_in != TB_ROUND_NONE;
+    const bool stream = stream_ok && p.tA == t_own && (!rnd || sizeof(T) == 4) && (uintptr_t)p.A % sizeof(T) == 0 &&
+                        (sizeof(T) == 4 || p.d_rows_fast);
     void (*kern)(NarrowParams) = plain_a ? k_narrow<T, NB, true> : k_narrow<T, NB, false>;
     if constexpr (stream_ok) {
-        if (stream) kern = k_narrow_stream<T, NB>;
+        if constexpr (sizeof(T) == 4) {
+            if (stream) kern = rnd ? k_narrow_stream<T, NB, true> : k_narrow_stream<T, NB, false>;
+        } else {
+            if (stream) kern = k_narrow_stream<T, NB, false>;
+        }
     }
     // C staged when it is read as stored and the shared memory allows
     np.stage_c = 0;
     if (stream) {
         smem += StreamRing<T>::bytes;
         const size_t cb = sizeof(T) * NB * 256;
-        if (!p.beta_zero && p.tC == (sizeof(T) == 4 ? T_F32 : T_F64) && (uintptr_t)p.C % sizeof(T) == 0 &&
+        if (!p.beta_zero && p.tC == t_own && (uintptr_t)p.C % sizeof(T) == 0 &&
             smem + cb <= (size_t)NARROW_MAX_SMEM + StreamRing<T>::bytes) {
             np.stage_c = 1;
             smem += cb;
         }
     }
-    const int variant = stream ? 2 : plain_a ? 1 : 0;
-    static int attr_done[64][3];
+    const int variant = stream ? 2 + (int)rnd : plain_a ? 1 : 0;
+    static int attr_done[64][4];
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64 || !attr_done[dev][variant]) {
