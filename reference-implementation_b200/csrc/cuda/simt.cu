@@ -102,12 +102,18 @@ __device__ __forceinline__ void epilogue_store(const Params& p, T xr, T xi, int6
 }
 
 template <typename T, bool CPLX, int BM, int BN, int BK, int TM, int TN>
-__global__ void __launch_bounds__((BM / TM) * (BN / TN)) k_simt(Params p)
+__global__ void __launch_bounds__((BM / TM) * (BN / TN), (CPLX && sizeof(T) == 8) ? 1 : 2)
+k_simt(Params p)
 {
     constexpr int NT = (BM / TM) * (BN / TN);
     constexpr int NP = CPLX ? 2 : 1;  // real and imaginary planes
-    __shared__ T As[2][NP][BK][BM + 1];
-    __shared__ T Bs[2][NP][BK][BN + 1];
+    // V4: real binary32 with register tiles in groups of four rows and four
+    // columns, read from shared memory as 16-byte vectors (rows padded by 4
+    // to keep them aligned); else scalar reads (rows padded by 1)
+    constexpr bool V4 = !CPLX && sizeof(T) == 4 && TM % 4 == 0 && TN % 4 == 0;
+    constexpr int PAD = V4 ? 4 : 1;
+    __shared__ __align__(16) T As[2][NP][BK][BM + PAD];
+    __shared__ __align__(16) T Bs[2][NP][BK][BN + PAD];
     __shared__ int64_t aRow[BM], bRow[BN];
     __shared__ int64_t aK[2][BK], bK[2][BK];
     __shared__ int64_t dRow[BM], cRow[BM], dCol[BN], cCol[BN];
@@ -216,6 +222,11 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN)) k_simt(Params p)
     constexpr int RT = BM / TM, CT = BN / TN;
     const int tr = p.d_rows_fast ? t % RT : t / CT;
     const int tc = p.d_rows_fast ? t / RT : t % CT;
+    // row of register row i and column of register column j: strided by RT
+    // (CT), or, with V4, groups of four consecutive rows (columns) RT*4
+    // (CT*4) apart
+    auto row_of = [&](int i) { return V4 ? (i / 4) * (RT * 4) + tr * 4 + (i % 4) : tr + i * RT; };
+    auto col_of = [&](int j) { return V4 ? (j / 4) * (CT * 4) + tc * 4 + (j % 4) : tc + j * CT; };
 
     slice_offsets(kbeg, 0);
     __syncthreads();
@@ -230,14 +241,27 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN)) k_simt(Params p)
 #pragma unroll
         for (int kk = 0; kk < BK; kk++) {
             T a[TM][NP], b[TN][NP];
+            if constexpr (V4) {
 #pragma unroll
-            for (int i = 0; i < TM; i++)
+                for (int i = 0; i < TM; i += 4) {
+                    const float4 q = *(const float4*)&As[buf][0][kk][row_of(i)];
+                    a[i][0] = q.x; a[i + 1][0] = q.y; a[i + 2][0] = q.z; a[i + 3][0] = q.w;
+                }
 #pragma unroll
-                for (int c = 0; c < NP; c++) a[i][c] = As[buf][c][kk][tr + i * RT];
+                for (int j = 0; j < TN; j += 4) {
+                    const float4 q = *(const float4*)&Bs[buf][0][kk][col_of(j)];
+                    b[j][0] = q.x; b[j + 1][0] = q.y; b[j + 2][0] = q.z; b[j + 3][0] = q.w;
+                }
+            } else {
 #pragma unroll
-            for (int j = 0; j < TN; j++)
+                for (int i = 0; i < TM; i++)
 #pragma unroll
-                for (int c = 0; c < NP; c++) b[j][c] = Bs[buf][c][kk][tc + j * CT];
+                    for (int c = 0; c < NP; c++) a[i][c] = As[buf][c][kk][row_of(i)];
+#pragma unroll
+                for (int j = 0; j < TN; j++)
+#pragma unroll
+                    for (int c = 0; c < NP; c++) b[j][c] = Bs[buf][c][kk][col_of(j)];
+            }
 #pragma unroll
             for (int i = 0; i < TM; i++)
 #pragma unroll
@@ -263,11 +287,11 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN)) k_simt(Params p)
         const int64_t base = ((int64_t)blockIdx.y * p.L + l) * p.M;
 #pragma unroll
         for (int i = 0; i < TM; i++) {
-            const int r = tr + i * RT;
+            const int r = row_of(i);
             if (m0 + r >= p.M) continue;
 #pragma unroll
             for (int j = 0; j < TN; j++) {
-                const int c = tc + j * CT;
+                const int c = col_of(j);
                 if (n0 + c >= p.N) continue;
                 const int64_t at = ((base + m0 + r) * p.N + n0 + c) * NP;
 #pragma unroll
@@ -280,19 +304,19 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN)) k_simt(Params p)
     // move past the stores on their own), then its D values stored
 #pragma unroll
     for (int i = 0; i < TM; i++) {
-        const int r = tr + i * RT;
+        const int r = row_of(i);
         if (m0 + r >= p.M) continue;
         T cr[TN], ci[TN];
 #pragma unroll
         for (int j = 0; j < TN; j++) {
-            const int c = tc + j * CT;
+            const int c = col_of(j);
             cr[j] = 0;
             ci[j] = 0;
             if (!p.beta_zero && n0 + c < p.N) load_rounded<T>(p.C, cRow[r] + cCol[c], p.tC, p.round_in, cr[j], ci[j]);
         }
 #pragma unroll
         for (int j = 0; j < TN; j++) {
-            const int c = tc + j * CT;
+            const int c = col_of(j);
             if (n0 + c >= p.N) continue;
             epilogue_store_c<T, CPLX>(p, acc[i][j][0], CPLX ? acc[i][j][NP - 1] : (T)0, cr[j], ci[j], dRow[r] + dCol[c]);
         }
