@@ -372,9 +372,10 @@ int tb_build_plan(const tb_tensor_view* A, const tb_tensor_view* B,
     const double macs = (double)outs * (double)(ksz > 0 ? ksz : 1) * (double)P->UA.size * (double)P->UB.size;
     int path = TB_PATH_GENERIC;
     /* few outputs and a long contraction: one block per output instead of
-     * one thread; also wherever one thread per output would not fill the
-     * GPU (under 148 x 256 outputs) and each would loop over >= 1024 terms */
-    if ((outs < 4096 && ksz >= 512 && outs * 16 < ksz) || (outs < 148 * 256 && ksz >= 1024))
+     * one thread; also wherever one thread per output would make about one
+     * wave of threads or less (under 148 x 1024 outputs) and each would loop
+     * over >= 1024 terms */
+    if ((outs < 4096 && ksz >= 512 && outs * 16 < ksz) || (outs < 148 * 1024 && ksz >= 1024))
         path = TB_PATH_REDUCE;
 
     int tc_ok = 0;

@@ -224,6 +224,8 @@ def test_planner_merges_contiguous_modes(tapp):
     (([55, 54, 53, 83, 6], [6, 54, 83, 53], [55, 83]), "reduce"),
     # 666 outputs x 5160 terms
     (([18, 86, 37, 60], [86, 60, 37], [18, 37]), "reduce"),
+    # D[a,h] = sum_k A[a,k,h] B[k,h]: 31 x 1794 outputs x 3634 terms (batched matrix-vector)
+    (([31, 3634, 1794], [3634, 1794], [31, 1794]), "reduce"),
     # 200 x 40 outputs x 30 terms: short contractions stay one thread per output
     (([200, 30, 40], [30, 40], [200, 40]), "generic"),
 ])
