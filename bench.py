@@ -72,6 +72,7 @@ def parse():
     ap.add_argument("--only-double", action="store_true", help="print only the binary64 / complex-double measurement")
     ap.add_argument("--only-batched", action="store_true", help="print only the batched-product measurement")
     ap.add_argument("--only-chain", action="store_true", help="print only the Tucker-chain measurement")
+    ap.add_argument("--only-tucker", action="store_true", help="print only the Tucker mode-n measurement")
     ap.add_argument("--slices", type=str, default="7,8", help="digit slices of the sliced binary64 runs")
     ap.add_argument("--double-ab", type=int, default=160, help="extent of a, b, e, f in the binary64 workload")
     ap.add_argument("--double-ij", type=int, default=40, help="extent of i, j in the binary64 workload")
@@ -408,6 +409,55 @@ def batched_measure(lib, torch, batches=64, n=512, steps=20):
             "speedup": t_s / t_b}
 
 
+def hbm_peak():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+TUCKER_CASES = [  # (core extents, contracted mode, rank, storage, precision)
+    ([128, 40, 128, 128], 1, 38, 0, 0),
+    ([128, 40, 128, 128], 0, 38, 0, 0),
+    ([128, 40, 128, 128], 1, 38, 0, 6),
+    ([77, 190, 133, 61], 2, 33, 0, 0),
+    ([96, 200, 90, 64], 3, 24, 1, -1),
+]
+
+
+def tucker_measure(lib, torch, steps=10, warmup=3):
+    """Tucker mode-n products D = 0.7 core x_n U + 0.3 C (the served mix's most common kind:
+    U is rank x extent, D has the rank at mode n), operands resident in HBM, uniform in [-1, 1].
+    Device time per product with CUDA events; algorithmic bytes = A + B + C + D."""
+    from tapp_b200.workloads import RequestSpec, case_from_spec
+    peak, peak_kind = hbm_peak()
+    stream = torch.cuda.current_stream().cuda_stream
+    out = []
+    for core, mode, R, storage, prec in TUCKER_CASES:
+        o = len(core)
+        d_ext = list(core)
+        d_ext[mode] = R
+        d_idx = list(range(o))
+        d_idx[mode] = o
+        spec = RequestSpec("tucker", storage, prec, (core, [R, core[mode]], d_ext, d_ext),
+                           (list(range(o)), [o, mode], d_idx, d_idx), 0.7, 0.3)
+        case = case_from_spec(np.random.default_rng(3), spec)
+        dev = [to_device(t, torch) for t in (case.A, case.B, case.C, case.D)]
+        ex = make_executor(lib, stream)
+        prod = Product(lib, case, [d[1] for d in dev], ex)
+        ms = time_device(torch, prod, steps, warmup, lambda: None)
+        nbytes = sum(spec.nbytes(k) for k in range(4))
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        out.append({"core": core, "mode": mode, "rank": R, "storage": ["f32", "f64"][storage], "precision": prec,
+                    "us": ms * 1e3, "gbs": gbs, "hbm_frac": gbs / peak, "tflops": spec.flops() / (ms * 1e-3) / 1e12})
+        prod.close()
+        lib.lib.TAPP_destroy_executor(ex)
+        del dev
+    return {"workload": "Tucker mode-n products D = 0.7 core x_n U + 0.3 C, operands in HBM (> L2)",
+            "hbm_peak_gbs": peak, "peak_kind": peak_kind, "cases": out}
+
+
 def chain_measure(lib, torch, r=64, n=256, reps=10):
     """Tucker reconstruction X[a,b,c] = sum_{i,j,k} G[i,j,k] U1[a,i] U2[b,j] U3[c,k] (core r^3,
     factors n x r, float32, F32F32_ACCUM_F32; synthetic, uniform in [-1, 1]) from pinned HOST
@@ -668,6 +718,10 @@ def run_b200(args):
         if rank == 0:
             print(json.dumps(chain_measure(lib, torch)), flush=True)
         return
+    if args.only_tucker:
+        if rank == 0:
+            print(json.dumps(tucker_measure(lib, torch)), flush=True)
+        return
     if args.only_batched:
         if rank == 0:
             print(json.dumps(batched_measure(lib, torch)), flush=True)
@@ -788,6 +842,7 @@ def run_b200(args):
         served = served_measure(lib, torch, args.served)
     batched = batched_measure(lib, torch) if world == 1 and not args.no_modes else None
     chain = chain_measure(lib, torch) if world == 1 and not args.no_modes else None
+    tucker = tucker_measure(lib, torch) if world == 1 and not args.no_modes else None
     double = None
     if world == 1 and not args.no_double:
         double = double_measure(lib, torch, slices)
@@ -808,7 +863,7 @@ def run_b200(args):
                            "l2": "inputs 256 MiB > 126 MB L2 (A,B,C,D 64 MiB each)",
                            "step": "pack A, pack B, tcgen05 GEMM + fused epilogue"},
                 "vs_plain_gpu": (value / world / plain) if plain else None,
-                "modes": modes, "batched": batched, "tucker_chain": chain, "double": double, "served": served, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu,
+                "modes": modes, "batched": batched, "tucker_chain": chain, "tucker": tucker, "double": double, "served": served, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu,
                 "clocks": clocks, "gpu_launches": gpu_launches}
         print(json.dumps(line), flush=True)
     prod.close()

@@ -504,14 +504,14 @@ __global__ void __launch_bounds__(256) k_narrow(NarrowParams np)
 // Streaming variant of k_narrow for A stored as T with no rounding: every
 // thread copies its own row of A into its own column of a shared-memory ring
 // with cp.async (S chunks of KC contracted values, S - 1 of them in flight
-// while one is multiplied), across tile boundaries, so the latency of HBM is
+// while one is multiplied; 48 KiB a block, so that two blocks share an SM), across tile boundaries, so the latency of HBM is
 // covered by the copies in flight instead of by registers. A thread only
 // reads what it copied itself: cp.async.wait_group orders the two, and no
 // block barrier is needed after the B panel is staged.
 template <typename T>
 struct StreamRing {
     static constexpr int KC = sizeof(T) == 4 ? 16 : 8;  // contracted values per chunk
-    static constexpr int S = 4;                         // chunks in the ring
+    static constexpr int S = 3;                         // chunks in the ring
     static constexpr size_t bytes = sizeof(T) * (size_t)KC * S * 256;
 };
 
@@ -687,12 +687,9 @@ __global__ void __launch_bounds__(256) k_narrow_stream(NarrowParams np)
             c = 0;
             ti++;
             if (oA >= 0 && np.stage_c) {
-                switch (c_pending) {
-                case 0: cp_async_wait<0>(); break;
-                case 1: cp_async_wait<1>(); break;
-                case 2: cp_async_wait<2>(); break;
-                default: cp_async_wait<3>(); break;
-                }
+                static_assert(S == 3, "the waits below cover c_pending = 0 .. S - 1");
+                if (c_pending == 0) cp_async_wait<0>();
+                else if (c_pending == 1) cp_async_wait<1>();
                 const bool d_as_t = p.tD == (sizeof(T) == 4 ? T_F32 : T_F64);
 #pragma unroll
                 for (int n = 0; n < NB; n++) {
