@@ -501,13 +501,14 @@ __global__ void __launch_bounds__(256) k_narrow(NarrowParams np)
     }
 }
 
-// Streaming variant of k_narrow for A stored as T with no rounding: every
-// thread copies its own row of A into its own column of a shared-memory ring
-// with cp.async (S chunks of KC contracted values, S - 1 of them in flight
-// while one is multiplied; 48 KiB a block, so that two blocks share an SM), across tile boundaries, so the latency of HBM is
-// covered by the copies in flight instead of by registers. A thread only
-// reads what it copied itself: cp.async.wait_group orders the two, and no
-// block barrier is needed after the B panel is staged.
+// Streaming variant of k_narrow for A stored as T: every thread copies its
+// own row of A into its own column of a shared-memory ring with cp.async (S
+// chunks of KC contracted values, S - 1 of them in flight while one is
+// multiplied, across tile boundaries; 48 KiB a block, so that two blocks
+// share an SM), so the latency of HBM is covered by the copies in flight
+// instead of by registers. Its row of C is copied the same way at the start
+// of each tile. A thread only reads what it copied itself: cp.async.wait_group
+// orders the two, and no block barrier is needed after the B panel is staged.
 template <typename T>
 struct StreamRing {
     static constexpr int KC = sizeof(T) == 4 ? 16 : 8;  // contracted values per chunk
