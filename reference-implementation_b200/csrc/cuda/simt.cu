@@ -381,6 +381,7 @@ static int64_t min_abs(const tb_modes& m, int w)
 // outputs. A loads coalesce when A's rows are contiguous (the common case);
 // row offsets decode with 32-bit multiply-high division.
 constexpr int NARROW_MAX_SMEM = 100 * 1024;
+constexpr int NARROW_COOP_SMEM = 227 * 1024;  // the cooperative variant's limit
 
 struct NarrowParams {
     Params p;
@@ -728,6 +729,213 @@ __global__ void __launch_bounds__(256) k_narrow_stream(NarrowParams np)
     cp_async_wait<0>();
 }
 
+// Variant of k_narrow_stream for products whose A is contiguous along the
+// contraction and whose D (and C) along the columns, such as mode-n products
+// on the first mode: a thread's own row would be read and written 4 bytes at
+// a time with every lane of a warp on a different line. Here each warp
+// copies its 32 rows cooperatively, consecutive lanes on consecutive
+// addresses: the A chunks into a ring laid out [slot][row][KC + 1] and the
+// rows of C into a staging buffer [row][NB + 1]; the thread of a row
+// multiplies as before, writes its results into its row of the staging
+// buffer, and the warp stores them to D the same cooperative way. Row offsets
+// of other lanes come by shuffles; __syncwarp orders the lanes' copies, reads
+// and writes (rows never leave their warp, so no block barrier is needed).
+constexpr int COOP_KC = 8;
+
+template <typename T, int NB, bool RND>
+__global__ void __launch_bounds__(256) k_narrow_coop(NarrowParams np)
+{
+    // chunks of 8 contracted values keep ring + staging buffer small enough
+    // for two blocks per SM
+    constexpr int KC = COOP_KC, S = StreamRing<T>::S, KP = KC + 1, NP1 = NB + 1;
+    const Params& p = np.p;
+    extern __shared__ __align__(16) unsigned char nsm[];
+    T* ring = (T*)nsm;                                                  // [S][256][KP]
+    T* Ts = ring + (size_t)S * 256 * KP;                                // [256][NP1]
+    T* Bs = Ts + (size_t)256 * NP1;                                     // [K][NB]
+    int64_t* kA = (int64_t*)(((uintptr_t)(Bs + (size_t)NB * p.K) + 15) & ~(uintptr_t)15);  // [K]
+    int64_t* nC = kA + p.K;                                             // [NB]
+    int64_t* nD = nC + NB;                                              // [NB]
+    const int t = threadIdx.x, lane = t & 31, wbase = t & ~31;
+    const int64_t l = blockIdx.y;
+    int64_t lA, lB, lC, lD, dummy;
+    decode(p.al, l, lA, dummy);
+    decode(p.bl, l, lB, dummy);
+    decode(p.cl, l, lC, lD);
+    for (int64_t k = t; k < p.K; k += 256) {
+        int64_t o;
+        decode(p.ak, k, o, dummy);
+        kA[k] = o + lA;
+    }
+    if (t < NB) {
+        int64_t oc = 0, od = 0;
+        if (t < p.N) decode(p.cn, t, oc, od);
+        nC[t] = oc + lC;
+        nD[t] = od + lD;
+    }
+    for (int64_t e = t; e < p.K * NB; e += 256) {
+        const int64_t k = e / NB;
+        const int n = (int)(e % NB);
+        T x = 0, xi = 0;
+        if (n < p.N) {
+            int64_t ob, ok;
+            decode(p.bn, n, ob, dummy);
+            decode(p.bk, k, ok, dummy);
+            load_rounded<T>(p.B, lB + ob + ok, p.tB, p.round_in, x, xi);
+        }
+        Bs[k * NB + n] = x;
+    }
+    __syncthreads();
+
+    const int64_t tiles = (p.M + 255) / 256;
+    if ((int64_t)blockIdx.x >= tiles) return;
+    const int64_t my_tiles = (tiles - 1 - blockIdx.x) / gridDim.x + 1;
+    const int nchunks = (int)((p.K + KC - 1) / KC);
+    const int64_t total = my_tiles * nchunks;
+    const T* A = (const T*)p.A;
+    const uint32_t ring_s = (uint32_t)__cvta_generic_to_shared(ring);
+    const uint32_t ts_s = (uint32_t)__cvta_generic_to_shared(Ts);
+
+    auto row_offsets = [&](int64_t i, int64_t& oA, int64_t& oC, int64_t& oD) {
+        const int64_t m = ((int64_t)blockIdx.x + i * gridDim.x) * 256 + t;
+        oA = oC = oD = -1;
+        if (m >= p.M) return;
+        oA = oC = oD = 0;
+        uint32_t r = (uint32_t)m;
+        for (int j = 0; j < p.am.n; j++) {
+            const uint32_t q = fdiv(r, np.fm[j]);
+            const int64_t c = (int64_t)(r - q * np.fm[j].d);
+            r = q;
+            oA += c * p.am.s0[j];
+            oC += c * p.cm.s0[j];
+            oD += c * p.cm.s1[j];
+        }
+    };
+    auto shfl64 = [](int64_t v, int src) { return (int64_t)__shfl_sync(0xffffffffu, (long long)v, src); };
+    // producer: the warp's copies of chunk g; every lane calls it with the same g
+    int64_t p_tile = -1, p_oA = -1;
+    int p_chunk = 0;
+    auto issue = [&](int64_t g) {
+        if (g < total) {
+            if (p_chunk == 0) {
+                p_tile++;
+                int64_t c_, d_;
+                row_offsets(p_tile, p_oA, c_, d_);
+            }
+            const int k0 = p_chunk * KC;
+            const uint32_t slot = ring_s + (uint32_t)(((g % S) * 256 + wbase) * KP) * sizeof(T);
+#pragma unroll 4
+            for (int f = lane; f < 32 * KC; f += 32) {
+                const int r = f / KC, kk = f % KC;
+                const int64_t oa = shfl64(p_oA, r);
+                if (oa >= 0 && k0 + kk < p.K) {
+                    const T* src = A + oa + kA[k0 + kk];
+                    const uint32_t dst = slot + (uint32_t)(r * KP + kk) * sizeof(T);
+                    if (sizeof(T) == 4) cp_async_elem4(dst, src);
+                    else cp_async_elem8(dst, src);
+                }
+            }
+            if (++p_chunk == nchunks) p_chunk = 0;
+        }
+        cp_async_commit();
+    };
+#pragma unroll
+    for (int g = 0; g < S - 1; g++) issue(g);
+
+    T acc[NB];
+    int64_t oA = -1, oC = -1, oD = -1;
+    int c = 0;
+    int64_t ti = 0;
+    const T al = (T)p.alpha, be = (T)p.beta;
+    const int c_pending = nchunks - 1 < S - 1 ? nchunks - 1 : S - 1;
+    T* trow = Ts + (size_t)t * NP1;
+    for (int64_t g = 0; g < total; g++) {
+        __syncwarp();  // the slot refilled below was read by every lane in the last round
+        if (c == 0) {
+            row_offsets(ti, oA, oC, oD);
+#pragma unroll
+            for (int n = 0; n < NB; n++) acc[n] = 0;
+            if (np.stage_c) {
+#pragma unroll 4
+                for (int f = lane; f < 32 * NB; f += 32) {
+                    const int r = f / NB, n = f % NB;
+                    const int64_t oc = shfl64(oC, r);
+                    if (oc >= 0 && n < p.N) {
+                        const T* src = (const T*)p.C + oc + nC[n];
+                        const uint32_t dst = ts_s + (uint32_t)((wbase + r) * NP1 + n) * sizeof(T);
+                        if (sizeof(T) == 4) cp_async_elem4(dst, src);
+                        else cp_async_elem8(dst, src);
+                    }
+                }
+            }
+        }
+        issue(g + S - 1);
+        cp_async_wait<S - 1>();
+        __syncwarp();  // the warp's copies of chunk g have landed
+        if (oA >= 0) {
+            const T* a = ring + (size_t)((g % S) * 256 + t) * KP;
+            const int k0 = c * KC;
+            const int kn = p.K - k0 < KC ? (int)(p.K - k0) : KC;
+#pragma unroll 2
+            for (int kk = 0; kk < kn; kk++) {
+                T x = a[kk];
+                if (RND) x = round_in<T>(x, p.round_in);
+                const T* b = Bs + (k0 + kk) * NB;
+                if (sizeof(T) == 4) {
+#pragma unroll
+                    for (int n = 0; n < NB; n += 4) {
+                        const float4 q = *(const float4*)((const float*)b + n);
+                        acc[n] = fma(x, (T)q.x, acc[n]);
+                        acc[n + 1] = fma(x, (T)q.y, acc[n + 1]);
+                        acc[n + 2] = fma(x, (T)q.z, acc[n + 2]);
+                        acc[n + 3] = fma(x, (T)q.w, acc[n + 3]);
+                    }
+                } else {
+#pragma unroll
+                    for (int n = 0; n < NB; n += 2) {
+                        const double2 q = *(const double2*)((const double*)b + n);
+                        acc[n] = fma(x, (T)q.x, acc[n]);
+                        acc[n + 1] = fma(x, (T)q.y, acc[n + 1]);
+                    }
+                }
+            }
+        }
+        if (++c == nchunks) {
+            c = 0;
+            ti++;
+            static_assert(S == 3, "the waits below cover c_pending = 0 .. S - 1");
+            if (np.stage_c) {
+                if (c_pending == 0) cp_async_wait<0>();
+                else if (c_pending == 1) cp_async_wait<1>();
+            }
+            __syncwarp();  // the warp's copies of C have landed
+            if (oA >= 0) {
+#pragma unroll
+                for (int n = 0; n < NB; n++) {
+                    T cv = np.stage_c ? trow[n] : (T)0;
+                    if (RND) cv = round_in<T>(cv, p.round_in);
+                    T v = p.beta_zero ? al * acc[n] : fma(be, cv, al * acc[n]);
+                    if (p.conjD && p.conjD_f32) v = (T)(float)v;  // op_D under the F64 precision rounds as conjf
+                    trow[n] = v;
+                }
+            }
+            __syncwarp();  // the warp's results are in the staging buffer
+            const bool d_as_t = p.tD == (sizeof(T) == 4 ? T_F32 : T_F64);
+#pragma unroll 4
+            for (int f = lane; f < 32 * NB; f += 32) {
+                const int r = f / NB, n = f % NB;
+                const int64_t od = shfl64(oD, r);
+                if (od >= 0 && n < p.N) {
+                    const T v = Ts[(size_t)(wbase + r) * NP1 + n];
+                    if (d_as_t) ((T*)p.D)[od + nD[n]] = v;
+                    else store_elem<T>(p.D, od + nD[n], p.tD, v, (T)0);
+                }
+            }
+        }
+    }
+    cp_async_wait<0>();
+}
+
 // Split of the contraction: enough CTAs to fill the GPU when the tiles do
 // not, each split at least 4 slices long, the workspace at most 256 MiB.
 struct Split {
@@ -891,7 +1099,7 @@ static int narrow_width(const tb_plan* P, const simt::Params& p)
 {
     if (P->compute != TB_R32 && P->compute != TB_R64) return 0;
     if (p.N > 64 || p.M < 1024 || p.M >= (1ll << 31) || p.L > 65535 || p.K < 1) return 0;
-    const int nb = p.N <= 8 ? 8 : p.N <= 16 ? 16 : p.N <= 32 ? 32 : p.N <= 48 ? 48 : 64;
+    const int nb = (int)((p.N + 7) / 8 * 8);  // widths in steps of 8: at most 7 padded columns
     const size_t es = P->compute == TB_R32 ? 4 : 8;
     const size_t smem = es * (size_t)nb * (size_t)p.K + 8 * ((size_t)p.K + 2 * (size_t)nb);
     if (smem > (size_t)simt::NARROW_MAX_SMEM) return 0;
@@ -908,10 +1116,10 @@ static cudaError_t launch_narrow_t(simt::NarrowParams& np, cudaStream_t s)
     size_t smem = sizeof(T) * NB * (size_t)p.K + 8 * ((size_t)p.K + 2 * NB);
     // A read as stored: the streaming kernel (cp.async ring); else the
     // register-prefetch kernel, which converts and rounds A at load. Not for
-    // binary64 at width 64 (its accumulators leave no registers) nor binary64
+    // binary64 wider than 48 (its accumulators leave no registers) nor binary64
     // products whose D is contiguous along the columns (each thread then
     // writes a row of its own, and the ring only costs occupancy).
-    constexpr bool stream_ok = !(sizeof(T) == 8 && NB == 64);
+    constexpr bool stream_ok = !(sizeof(T) == 8 && NB > 48);
     const int t_own = sizeof(T) == 4 ? T_F32 : T_F64;
     const bool plain_a = p.tA == t_own && p.round_in == TB_ROUND_NONE;
     // rounding after the copy is the rounding load's only for binary32 storage
@@ -937,13 +1145,27 @@ static cudaError_t launch_narrow_t(simt::NarrowParams& np, cudaStream_t s)
             smem += cb;
         }
     }
-    const int variant = stream ? 2 + (int)rnd : plain_a ? 1 : 0;
-    static int attr_done[64][4];
+    // A contiguous along the contraction and D along the columns: the
+    // cooperative variant (binary32; C staged whenever it is read)
+    int variant = stream ? 2 + (int)rnd : plain_a ? 1 : 0;
+    if constexpr (sizeof(T) == 4) {
+        const size_t coop_smem = sizeof(T) * (size_t)StreamRing<T>::S * 256 * (COOP_KC + 1) +
+                                 sizeof(T) * 256 * (NB + 1) + sizeof(T) * NB * (size_t)p.K + 16 +
+                                 8 * ((size_t)p.K + 2 * NB);
+        const bool c_ok = p.beta_zero || (p.tC == t_own && (uintptr_t)p.C % sizeof(T) == 0);
+        if (stream && !p.a_rows_fast && !p.d_rows_fast && c_ok && coop_smem <= NARROW_COOP_SMEM) {
+            kern = rnd ? k_narrow_coop<T, NB, true> : k_narrow_coop<T, NB, false>;
+            np.stage_c = !p.beta_zero;
+            smem = coop_smem;
+            variant = 4 + (int)rnd;
+        }
+    }
+    static int attr_done[64][6];
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64 || !attr_done[dev][variant]) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             NARROW_MAX_SMEM + (int)StreamRing<T>::bytes);
+                                             variant >= 4 ? NARROW_COOP_SMEM : NARROW_MAX_SMEM + (int)StreamRing<T>::bytes);
         if (e != cudaSuccess) return e;
         if (dev >= 0 && dev < 64) attr_done[dev][variant] = 1;
     }
@@ -976,16 +1198,22 @@ cudaError_t launch_simt(const tb_plan* P, const tb_ptrs* d, cudaStream_t s)
             switch (nb) {
             case 8: return launch_narrow_t<float, 8>(np, s);
             case 16: return launch_narrow_t<float, 16>(np, s);
+            case 24: return launch_narrow_t<float, 24>(np, s);
             case 32: return launch_narrow_t<float, 32>(np, s);
+            case 40: return launch_narrow_t<float, 40>(np, s);
             case 48: return launch_narrow_t<float, 48>(np, s);
+            case 56: return launch_narrow_t<float, 56>(np, s);
             default: return launch_narrow_t<float, 64>(np, s);
             }
         }
         switch (nb) {
         case 8: return launch_narrow_t<double, 8>(np, s);
         case 16: return launch_narrow_t<double, 16>(np, s);
+        case 24: return launch_narrow_t<double, 24>(np, s);
         case 32: return launch_narrow_t<double, 32>(np, s);
+        case 40: return launch_narrow_t<double, 40>(np, s);
         case 48: return launch_narrow_t<double, 48>(np, s);
+        case 56: return launch_narrow_t<double, 56>(np, s);
         default: return launch_narrow_t<double, 64>(np, s);
         }
     }

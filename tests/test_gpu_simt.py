@@ -187,3 +187,39 @@ def test_hadamard_long_contraction_reduction(tapp, oracle, gpu, storage, prec):
     assert "path=reduce" in describe(tapp, case, ex)
     check_against_f64(tapp, oracle, case, device=True, executor=ex)
     tapp.lib.TAPP_destroy_executor(ex)
+
+
+@pytest.mark.parametrize("prec", [0, 6])
+@pytest.mark.parametrize("rank", [8, 24, 40, 60])
+def test_first_mode_products_beta_zero_and_aliased_c(tapp, oracle, gpu, prec, rank):
+    """Mode-n products on the first mode (A contiguous along the contraction,
+    D along the rank: the cooperative streaming kernel) with beta = 0, and
+    with C given as D's own buffer, whose result must equal the one from a
+    separate copy of C bit for bit (rows are read and written by one warp)."""
+    import ctypes as C
+    import torch
+    from tapp_b200.case import scalar
+    rng = np.random.default_rng(200 + rank + prec)
+    core = [60, 77, 43]
+    d_ext = [rank, 77, 43]
+    case = spec_case(rng, 0, prec, (core, [rank, 60], d_ext, d_ext), ([0, 1, 2], [3, 0], [3, 1, 2], [3, 1, 2]),
+                     "tucker")
+    zero = case.copy()
+    zero.beta = scalar(0, 0.0)
+    ex = tapp.create_executor()
+    assert "path=simt" in describe(tapp, case, ex)
+    check_against_f64(tapp, oracle, zero, device=True, executor=ex)
+    check_against_f64(tapp, oracle, case, device=True, executor=ex)
+    infos = [tapp.tensor_info(t.dtype, t.extents, t.strides)[1] for t in (case.A, case.B, case.C, case.D)]
+    _, plan = tapp.create_product(0, [0, 0, 0, 0], infos, [case.A.idx, case.B.idx, case.C.idx, case.D.idx], prec)
+    dev = [torch.from_numpy(t.buf.view(np.uint8).copy()).cuda() for t in (case.A, case.B, case.C, case.D)]
+    aliased = dev[2].clone()  # D's buffer holding C's values
+    st = tapp_b200.intptr(0)
+    call = lambda Cp, Dp: tapp.lib.TAPP_execute_product(plan, ex, C.byref(st), case.alpha.ctypes.data, dev[0].data_ptr(),
+                                                        dev[1].data_ptr(), case.beta.ctypes.data, Cp, Dp)
+    assert call(dev[2].data_ptr(), dev[3].data_ptr()) == 0
+    assert call(aliased.data_ptr(), aliased.data_ptr()) == 0
+    torch.cuda.synchronize()
+    assert torch.equal(aliased, dev[3])
+    tapp.lib.TAPP_destroy_tensor_product(plan)
+    tapp.lib.TAPP_destroy_executor(ex)
