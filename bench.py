@@ -423,6 +423,7 @@ TUCKER_CASES = [  # (core extents, contracted mode, rank, storage, precision)
     ([128, 40, 128, 128], 1, 38, 0, 6),
     ([77, 190, 133, 61], 2, 33, 0, 0),
     ([96, 200, 90, 64], 3, 24, 1, -1),
+    ([128, 40, 128, 128], 1, 24, 2, -1),
 ]
 
 
@@ -449,7 +450,7 @@ def tucker_measure(lib, torch, steps=10, warmup=3):
         ms = time_device(torch, prod, steps, warmup, lambda: None)
         nbytes = sum(spec.nbytes(k) for k in range(4))
         gbs = nbytes / (ms * 1e-3) / 1e9
-        out.append({"core": core, "mode": mode, "rank": R, "storage": ["f32", "f64"][storage], "precision": prec,
+        out.append({"core": core, "mode": mode, "rank": R, "storage": ["f32", "f64", "c32", "c64"][storage], "precision": prec,
                     "us": ms * 1e3, "gbs": gbs, "hbm_frac": gbs / peak, "tflops": spec.flops() / (ms * 1e-3) / 1e12})
         prod.close()
         lib.lib.TAPP_destroy_executor(ex)

@@ -936,6 +936,156 @@ __global__ void __launch_bounds__(256) k_narrow_coop(NarrowParams np)
     cp_async_wait<0>();
 }
 
+// Complex-float variant of k_narrow_stream (A stored as complex float, rows
+// contiguous in A and D, at most 32 columns): a ring of complex values per
+// thread, B as complex pairs in shared memory, four FMAs per product in the
+// order of the tiled kernel, op_A/op_B conjugation at load, and the tiled
+// kernel's epilogue (alpha, beta, op_C, op_D) with C loaded eight at a time.
+template <int NB>
+__global__ void __launch_bounds__(256) k_narrow_cstream(NarrowParams np)
+{
+    constexpr int KC = 8, S = 3;
+    const Params& p = np.p;
+    extern __shared__ __align__(16) unsigned char nsm[];
+    float2* ring = (float2*)nsm;                 // [S][KC][256]
+    float2* Bs = ring + S * KC * 256;            // [K][NB]
+    int64_t* kA = (int64_t*)(Bs + (size_t)NB * p.K);  // [K]
+    int64_t* nC = kA + p.K;                      // [NB]
+    int64_t* nD = nC + NB;                       // [NB]
+    const int t = threadIdx.x;
+    const int64_t l = blockIdx.y;
+    int64_t lA, lB, lC, lD, dummy;
+    decode(p.al, l, lA, dummy);
+    decode(p.bl, l, lB, dummy);
+    decode(p.cl, l, lC, lD);
+    for (int64_t k = t; k < p.K; k += 256) {
+        int64_t o;
+        decode(p.ak, k, o, dummy);
+        kA[k] = o + lA;
+    }
+    if (t < NB) {
+        int64_t oc = 0, od = 0;
+        if (t < p.N) decode(p.cn, t, oc, od);
+        nC[t] = oc + lC;
+        nD[t] = od + lD;
+    }
+    for (int64_t e = t; e < p.K * NB; e += 256) {
+        const int64_t k = e / NB;
+        const int n = (int)(e % NB);
+        float x = 0, xi = 0;
+        if (n < p.N) {
+            int64_t ob, ok;
+            decode(p.bn, n, ob, dummy);
+            decode(p.bk, k, ok, dummy);
+            load_rounded<float>(p.B, lB + ob + ok, p.tB, p.round_in, x, xi);
+            if (p.conjB) xi = -xi;
+        }
+        Bs[k * NB + n] = make_float2(x, xi);
+    }
+    __syncthreads();
+
+    const int64_t tiles = (p.M + 255) / 256;
+    if ((int64_t)blockIdx.x >= tiles) return;
+    const int64_t my_tiles = (tiles - 1 - blockIdx.x) / gridDim.x + 1;
+    const int nchunks = (int)((p.K + KC - 1) / KC);
+    const int64_t total = my_tiles * nchunks;
+    const float* A = (const float*)p.A;
+    const uint32_t ring_base = (uint32_t)__cvta_generic_to_shared(ring) + (uint32_t)t * sizeof(float2);
+    auto row_offsets = [&](int64_t i, int64_t& oA, int64_t& oC, int64_t& oD) {
+        const int64_t m = ((int64_t)blockIdx.x + i * gridDim.x) * 256 + t;
+        oA = oC = oD = -1;
+        if (m >= p.M) return;
+        oA = oC = oD = 0;
+        uint32_t r = (uint32_t)m;
+        for (int j = 0; j < p.am.n; j++) {
+            const uint32_t q = fdiv(r, np.fm[j]);
+            const int64_t c = (int64_t)(r - q * np.fm[j].d);
+            r = q;
+            oA += c * p.am.s0[j];
+            oC += c * p.cm.s0[j];
+            oD += c * p.cm.s1[j];
+        }
+    };
+    int64_t p_tile = -1, p_oA = -1;
+    int p_chunk = 0;
+    auto issue = [&](int64_t g) {
+        if (g < total) {
+            if (p_chunk == 0) {
+                p_tile++;
+                int64_t c_, d_;
+                row_offsets(p_tile, p_oA, c_, d_);
+            }
+            if (p_oA >= 0) {
+                const int k0 = p_chunk * KC;
+                const uint32_t dst = ring_base + (uint32_t)((g % S) * KC * 256) * sizeof(float2);
+#pragma unroll
+                for (int kk = 0; kk < KC; kk++)
+                    if (k0 + kk < p.K) cp_async_elem8(dst + kk * 256 * sizeof(float2), A + 2 * (p_oA + kA[k0 + kk]));
+            }
+            if (++p_chunk == nchunks) p_chunk = 0;
+        }
+        cp_async_commit();
+    };
+#pragma unroll
+    for (int g = 0; g < S - 1; g++) issue(g);
+
+    float ar_[NB], ai_[NB];
+    int64_t oA = -1, oC = -1, oD = -1;
+    int c = 0;
+    int64_t ti = 0;
+    for (int64_t g = 0; g < total; g++) {
+        if (c == 0) {
+            row_offsets(ti, oA, oC, oD);
+#pragma unroll
+            for (int n = 0; n < NB; n++) ar_[n] = ai_[n] = 0.f;
+        }
+        issue(g + S - 1);
+        cp_async_wait<S - 1>();
+        if (oA >= 0) {
+            const float2* a = ring + (size_t)(g % S) * KC * 256 + t;
+            const int k0 = c * KC;
+            const int kn = p.K - k0 < KC ? (int)(p.K - k0) : KC;
+#pragma unroll 2
+            for (int kk = 0; kk < kn; kk++) {
+                const float2 x = a[kk * 256];
+                const float xr = x.x, xi = p.conjA ? -x.y : x.y;
+                const float4* b = (const float4*)(Bs + (k0 + kk) * NB);
+#pragma unroll
+                for (int n = 0; n < NB; n += 2) {
+                    const float4 q = b[n / 2];
+                    ar_[n] = fmaf(xr, q.x, ar_[n]);
+                    ar_[n] = fmaf(-xi, q.y, ar_[n]);
+                    ai_[n] = fmaf(xr, q.y, ai_[n]);
+                    ai_[n] = fmaf(xi, q.x, ai_[n]);
+                    ar_[n + 1] = fmaf(xr, q.z, ar_[n + 1]);
+                    ar_[n + 1] = fmaf(-xi, q.w, ar_[n + 1]);
+                    ai_[n + 1] = fmaf(xr, q.w, ai_[n + 1]);
+                    ai_[n + 1] = fmaf(xi, q.z, ai_[n + 1]);
+                }
+            }
+        }
+        if (++c == nchunks) {
+            c = 0;
+            ti++;
+            if (oA >= 0) {
+#pragma unroll
+                for (int gq = 0; gq < NB; gq += 8) {
+                    float cr[8], ci[8];
+#pragma unroll
+                    for (int j = 0; j < 8; j++) {
+                        cr[j] = ci[j] = 0.f;
+                        if (!p.beta_zero && gq + j < p.N) load_rounded<float>(p.C, oC + nC[gq + j], p.tC, p.round_in, cr[j], ci[j]);
+                    }
+#pragma unroll
+                    for (int j = 0; j < 8; j++)
+                        if (gq + j < p.N) epilogue_store_c<float, true>(p, ar_[gq + j], ai_[gq + j], cr[j], ci[j], oD + nD[gq + j]);
+                }
+            }
+        }
+    }
+    cp_async_wait<0>();
+}
+
 // Split of the contraction: enough CTAs to fill the GPU when the tiles do
 // not, each split at least 4 slices long, the workspace at most 256 MiB.
 struct Split {
@@ -1097,7 +1247,13 @@ size_t simt_scratch_bytes(const tb_plan* P)
 // padded width of the narrow kernel for a turned view, or 0 when it does not apply
 static int narrow_width(const tb_plan* P, const simt::Params& p)
 {
-    if (P->compute != TB_R32 && P->compute != TB_R64) return 0;
+    // complex float: the streaming kernel only (A read as stored, rows
+    // contiguous in A and D, at most 32 columns)
+    const bool cplx = P->compute == TB_C32;
+    if (cplx && (p.N > 32 || p.tA != T_C32 || p.round_in != TB_ROUND_NONE || !p.a_rows_fast || !p.d_rows_fast ||
+                 (uintptr_t)p.A % 8 != 0))
+        return 0;
+    if (P->compute != TB_R32 && P->compute != TB_R64 && !cplx) return 0;
     if (p.N > 64 || p.M < 1024 || p.M >= (1ll << 31) || p.L > 65535 || p.K < 1) return 0;
     const int nb = (int)((p.N + 7) / 8 * 8);  // widths in steps of 8: at most 7 padded columns
     const size_t es = P->compute == TB_R32 ? 4 : 8;
@@ -1182,6 +1338,34 @@ static cudaError_t launch_narrow_t(simt::NarrowParams& np, cudaStream_t s)
     return cudaGetLastError();
 }
 
+template <int NB>
+static cudaError_t launch_narrow_c(simt::NarrowParams& np, cudaStream_t s)
+{
+    using namespace simt;
+    const Params& p = np.p;
+    const size_t smem = sizeof(float2) * (size_t)(3 * 8 * 256) + sizeof(float2) * NB * (size_t)p.K +
+                        8 * ((size_t)p.K + 2 * NB);
+    auto kern = k_narrow_cstream<NB>;
+    static int attr_done[64];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64 || !attr_done[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             NARROW_MAX_SMEM + (int)(sizeof(float2) * 3 * 8 * 256));
+        if (e != cudaSuccess) return e;
+        if (dev >= 0 && dev < 64) attr_done[dev] = 1;
+    }
+    const int64_t tiles = (p.M + 255) / 256;
+    int per_sm = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem) != cudaSuccess || per_sm < 1) per_sm = 1;
+    int64_t gx = ((int64_t)148 * per_sm + p.L - 1) / p.L;
+    if (gx > tiles) gx = tiles;
+    if (gx < 1) gx = 1;
+    kern<<<dim3((unsigned)gx, (unsigned)p.L), 256, smem, s>>>(np);
+    count_launch();
+    return cudaGetLastError();
+}
+
 cudaError_t launch_simt(const tb_plan* P, const tb_ptrs* d, cudaStream_t s)
 {
     using namespace simt;
@@ -1194,6 +1378,14 @@ cudaError_t launch_simt(const tb_plan* P, const tb_ptrs* d, cudaStream_t s)
         np.p = p;
         np.nb = nb;
         for (int j = 0; j < p.am.n; j++) np.fm[j] = make_fastdiv((uint32_t)p.am.ext[j]);
+        if (P->compute == TB_C32) {
+            switch (nb) {
+            case 8: return launch_narrow_c<8>(np, s);
+            case 16: return launch_narrow_c<16>(np, s);
+            case 24: return launch_narrow_c<24>(np, s);
+            default: return launch_narrow_c<32>(np, s);
+            }
+        }
         if (P->compute == TB_R32) {
             switch (nb) {
             case 8: return launch_narrow_t<float, 8>(np, s);

@@ -223,3 +223,22 @@ def test_first_mode_products_beta_zero_and_aliased_c(tapp, oracle, gpu, prec, ra
     assert torch.equal(aliased, dev[3])
     tapp.lib.TAPP_destroy_tensor_product(plan)
     tapp.lib.TAPP_destroy_executor(ex)
+
+
+@pytest.mark.parametrize("ops", [(0, 0, 0, 0), (1, 1, 1, 1), (1, 0, 0, 1)])
+@pytest.mark.parametrize("rank", [6, 12, 30])
+def test_complex_mode_n_products_streaming(tapp, oracle, gpu, ops, rank):
+    """Complex-float mode-n products on an inner mode (rows contiguous in A and
+    D, at most 32 columns: the complex streaming kernel), with op_A, op_B,
+    op_C and op_D conjugation under the DEFAULT precision."""
+    rng = np.random.default_rng(300 + rank + 7 * sum(ops))
+    core = [70, 45, 60]
+    d_ext = [70, rank, 60]
+    case = spec_case(rng, 2, -1, (core, [rank, 45], d_ext, d_ext), ([0, 1, 2], [3, 1], [0, 3, 2], [0, 3, 2]), "tucker")
+    for t, o in zip((case.A, case.B, case.C, case.D), ops):
+        t.op = o
+    ex = tapp.create_executor()
+    assert "path=simt" in describe(tapp, case, ex)
+    check_against_f64(tapp, oracle, case, device=True, executor=ex)
+    check_against_f64(tapp, oracle, case, device=False, executor=ex)
+    tapp.lib.TAPP_destroy_executor(ex)
