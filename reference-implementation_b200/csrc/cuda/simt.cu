@@ -64,6 +64,7 @@ struct Params {
     int32_t tiles_m, tiles_n;
     int64_t k_chunk;   // contraction length of one split (multiple of BK)
     void* ws;          // split sums [split][l][m][n][plane], or NULL: epilogue in place
+    int32_t a_vec, b_vec;  // binary32 operand read four elements at a time (see vec4_side)
 };
 
 // D = op_D(alpha * acc + beta * op_C(C)) for one element whose C value
@@ -165,8 +166,43 @@ k_simt(Params p)
         }
     };
     constexpr int A_PER = BM * BK / NT, B_PER = BN * BK / NT;
+    // VA / VB: with a_vec / b_vec set, four neighbours along the operand's
+    // contiguous mode come in one 16-byte load
+    constexpr bool VA = V4 && A_PER % 4 == 0, VB = V4 && B_PER % 4 == 0;
     T ra[A_PER][NP], rb[B_PER][NP];
+    // element (r, kk) of group u of four: along rows or along the contraction
+    auto vec_rk = [&](int u, bool rows_fast, int rows, int& r, int& kk) {
+        const int e = t + NT * u;
+        if (rows_fast) {
+            r = (e % (rows / 4)) * 4;
+            kk = e / (rows / 4);
+        } else {
+            kk = (e % (BK / 4)) * 4;
+            r = e / (BK / 4);
+        }
+    };
+    auto load4 = [&](const void* base, int64_t off, bool in, T* dst) {
+        float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (in) q = __ldg((const float4*)((const float*)base + off));
+        dst[0] = q.x; dst[1] = q.y; dst[2] = q.z; dst[3] = q.w;
+        if (p.round_in != TB_ROUND_NONE)
+            for (int h = 0; h < 4; h++) dst[h] = round_in<T>(dst[h], p.round_in);
+    };
     auto load_slice = [&](int64_t k0, int buf) {
+        if constexpr (VA) {
+            if (p.a_vec) {
+#pragma unroll
+                for (int u = 0; u < A_PER / 4; u++) {
+                    int r, kk;
+                    vec_rk(u, p.a_rows_fast, BM, r, kk);
+                    T v[4];
+                    load4(p.A, aRow[r] + aK[buf][kk], m0 + r < p.M && k0 + kk < kend, v);
+#pragma unroll
+                    for (int h = 0; h < 4; h++) ra[4 * u + h][0] = v[h];
+                }
+                goto b_side;
+            }
+        }
 #pragma unroll
         for (int u = 0; u < A_PER; u++) {
             const int e = t + NT * u;
@@ -177,6 +213,21 @@ k_simt(Params p)
                 load_rounded<T>(p.A, aRow[r] + aK[buf][kk], p.tA, p.round_in, x, xi);
             ra[u][0] = x;
             if (CPLX) ra[u][NP - 1] = p.conjA ? -xi : xi;
+        }
+    b_side:
+        if constexpr (VB) {
+            if (p.b_vec) {
+#pragma unroll
+                for (int u = 0; u < B_PER / 4; u++) {
+                    int r, kk;
+                    vec_rk(u, p.b_rows_fast, BN, r, kk);
+                    T v[4];
+                    load4(p.B, bRow[r] + bK[buf][kk], n0 + r < p.N && k0 + kk < kend, v);
+#pragma unroll
+                    for (int h = 0; h < 4; h++) rb[4 * u + h][0] = v[h];
+                }
+                return;
+            }
         }
 #pragma unroll
         for (int u = 0; u < B_PER; u++) {
@@ -191,6 +242,23 @@ k_simt(Params p)
         }
     };
     auto store_slice = [&](int buf) {
+        if constexpr (VA) {
+            if (p.a_vec) {
+#pragma unroll
+                for (int u = 0; u < A_PER / 4; u++) {
+                    int r, kk;
+                    vec_rk(u, p.a_rows_fast, BM, r, kk);
+                    if (p.a_rows_fast) {
+                        *(float4*)&As[buf][0][kk][r] =
+                            make_float4(ra[4 * u][0], ra[4 * u + 1][0], ra[4 * u + 2][0], ra[4 * u + 3][0]);
+                    } else {
+#pragma unroll
+                        for (int h = 0; h < 4; h++) As[buf][0][kk + h][r] = ra[4 * u + h][0];
+                    }
+                }
+                goto b_store;
+            }
+        }
 #pragma unroll
         for (int u = 0; u < A_PER; u++) {
             const int e = t + NT * u;
@@ -198,6 +266,24 @@ k_simt(Params p)
             const int kk = p.a_rows_fast ? e / BM : e % BK;
 #pragma unroll
             for (int c = 0; c < NP; c++) As[buf][c][kk][r] = ra[u][c];
+        }
+    b_store:
+        if constexpr (VB) {
+            if (p.b_vec) {
+#pragma unroll
+                for (int u = 0; u < B_PER / 4; u++) {
+                    int r, kk;
+                    vec_rk(u, p.b_rows_fast, BN, r, kk);
+                    if (p.b_rows_fast) {
+                        *(float4*)&Bs[buf][0][kk][r] =
+                            make_float4(rb[4 * u][0], rb[4 * u + 1][0], rb[4 * u + 2][0], rb[4 * u + 3][0]);
+                    } else {
+#pragma unroll
+                        for (int h = 0; h < 4; h++) Bs[buf][0][kk + h][r] = rb[4 * u + h][0];
+                    }
+                }
+                return;
+            }
         }
 #pragma unroll
         for (int u = 0; u < B_PER; u++) {
@@ -1186,6 +1272,28 @@ static auto with_cfg(int compute, int tile, F&& f)
 
 }  // namespace simt
 
+// Whether a binary32 operand can be read four elements at a time: its
+// contiguous mode (the first row mode when rows_fast, else the first
+// contracted mode) has stride 1 and an extent divisible by 4, every other
+// stride keeps 4-element alignment and the base is 16-byte aligned, so the
+// four neighbours of an aligned group lie in one 16-byte word (the extents
+// then make M or K a multiple of 4, and a group is wholly in range or not).
+static bool vec4_side(const simt::Modes& rows, const simt::Modes& ks, const simt::Modes& ls, int rows_fast,
+                      const void* base, int t)
+{
+    if (t != T_F32 || ((uintptr_t)base & 15) != 0) return false;
+    const simt::Modes& f = rows_fast ? rows : ks;
+    const simt::Modes& o = rows_fast ? ks : rows;
+    if (f.n < 1 || f.s0[0] != 1 || f.ext[0] % 4 != 0) return false;
+    for (int j = 1; j < f.n; j++)
+        if (f.s0[j] % 4 != 0) return false;
+    for (int j = 0; j < o.n; j++)
+        if (o.s0[j] % 4 != 0) return false;
+    for (int j = 0; j < ls.n; j++)
+        if (ls.s0[j] % 4 != 0) return false;
+    return true;
+}
+
 // the launch parameters of a plan, turned so that M >= N
 static void simt_params(const tb_plan* P, const tb_ptrs* d, simt::Params& p)
 {
@@ -1230,6 +1338,10 @@ static void simt_params(const tb_plan* P, const tb_ptrs* d, simt::Params& p)
     p.a_rows_fast = min_abs(Mm, wa) < min_abs(P->K, wa);
     p.b_rows_fast = min_abs(Nm, wb) < min_abs(P->K, wb);
     p.d_rows_fast = min_abs(Mm, 3) <= min_abs(Nm, 3);
+    if (P->compute == TB_R32) {
+        p.a_vec = vec4_side(p.am, p.ak, p.al, p.a_rows_fast, p.A, p.tA);
+        p.b_vec = vec4_side(p.bn, p.bk, p.bl, p.b_rows_fast, p.B, p.tB);
+    }
 }
 
 static int narrow_width(const tb_plan* P, const simt::Params& p);
