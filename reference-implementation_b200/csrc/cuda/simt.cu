@@ -64,7 +64,7 @@ struct Params {
     int32_t tiles_m, tiles_n;
     int64_t k_chunk;   // contraction length of one split (multiple of BK)
     void* ws;          // split sums [split][l][m][n][plane], or NULL: epilogue in place
-    int32_t a_vec, b_vec;  // binary32 operand read four elements at a time (see vec4_side)
+    int32_t a_vec, b_vec;  // operand read 16 bytes at a time (see vec_side)
 };
 
 // D = op_D(alpha * acc + beta * op_C(C)) for one element whose C value
@@ -166,39 +166,46 @@ k_simt(Params p)
         }
     };
     constexpr int A_PER = BM * BK / NT, B_PER = BN * BK / NT;
-    // VA / VB: with a_vec / b_vec set, four neighbours along the operand's
-    // contiguous mode come in one 16-byte load
-    constexpr bool VA = V4 && A_PER % 4 == 0, VB = V4 && B_PER % 4 == 0;
+    // VA / VB: with a_vec / b_vec set, VW neighbours along the operand's
+    // contiguous mode (4 binary32 or 2 binary64) come in one 16-byte load
+    constexpr int VW = 16 / sizeof(T);
+    constexpr bool VA = !CPLX && A_PER % VW == 0, VB = !CPLX && B_PER % VW == 0;
     T ra[A_PER][NP], rb[B_PER][NP];
-    // element (r, kk) of group u of four: along rows or along the contraction
+    // element (r, kk) of group u of VW: along rows or along the contraction
     auto vec_rk = [&](int u, bool rows_fast, int rows, int& r, int& kk) {
         const int e = t + NT * u;
         if (rows_fast) {
-            r = (e % (rows / 4)) * 4;
-            kk = e / (rows / 4);
+            r = (e % (rows / VW)) * VW;
+            kk = e / (rows / VW);
         } else {
-            kk = (e % (BK / 4)) * 4;
-            r = e / (BK / 4);
+            kk = (e % (BK / VW)) * VW;
+            r = e / (BK / VW);
         }
     };
-    auto load4 = [&](const void* base, int64_t off, bool in, T* dst) {
-        float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (in) q = __ldg((const float4*)((const float*)base + off));
-        dst[0] = q.x; dst[1] = q.y; dst[2] = q.z; dst[3] = q.w;
+    auto loadv = [&](const void* base, int64_t off, bool in, T* dst) {
+        if constexpr (sizeof(T) == 4) {
+            float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (in) q = __ldg((const float4*)((const float*)base + off));
+            dst[0] = q.x; dst[1] = q.y; dst[2] = q.z; dst[3] = q.w;
+        } else {
+            double2 q = make_double2(0.0, 0.0);
+            if (in) q = __ldg((const double2*)((const double*)base + off));
+            dst[0] = q.x; dst[1] = q.y;
+        }
         if (p.round_in != TB_ROUND_NONE)
-            for (int h = 0; h < 4; h++) dst[h] = round_in<T>(dst[h], p.round_in);
+            for (int h = 0; h < VW; h++) dst[h] = round_in<T>(dst[h], p.round_in);
     };
     auto load_slice = [&](int64_t k0, int buf) {
         if constexpr (VA) {
             if (p.a_vec) {
 #pragma unroll
-                for (int u = 0; u < A_PER / 4; u++) {
+                for (int u = 0; u < A_PER / VW; u++) {
                     int r, kk;
                     vec_rk(u, p.a_rows_fast, BM, r, kk);
-                    T v[4];
-                    load4(p.A, aRow[r] + aK[buf][kk], m0 + r < p.M && k0 + kk < kend, v);
+                    T v[VW];
+                    loadv(p.A, aRow[r] + aK[buf][kk], m0 + r < p.M && k0 + kk < kend, v);
 #pragma unroll
-                    for (int h = 0; h < 4; h++) ra[4 * u + h][0] = v[h];
+                    for (int h = 0; h < VW; h++) ra[VW * u + h][0] = v[h];
                 }
                 goto b_side;
             }
@@ -218,13 +225,13 @@ k_simt(Params p)
         if constexpr (VB) {
             if (p.b_vec) {
 #pragma unroll
-                for (int u = 0; u < B_PER / 4; u++) {
+                for (int u = 0; u < B_PER / VW; u++) {
                     int r, kk;
                     vec_rk(u, p.b_rows_fast, BN, r, kk);
-                    T v[4];
-                    load4(p.B, bRow[r] + bK[buf][kk], n0 + r < p.N && k0 + kk < kend, v);
+                    T v[VW];
+                    loadv(p.B, bRow[r] + bK[buf][kk], n0 + r < p.N && k0 + kk < kend, v);
 #pragma unroll
-                    for (int h = 0; h < 4; h++) rb[4 * u + h][0] = v[h];
+                    for (int h = 0; h < VW; h++) rb[VW * u + h][0] = v[h];
                 }
                 return;
             }
@@ -245,15 +252,18 @@ k_simt(Params p)
         if constexpr (VA) {
             if (p.a_vec) {
 #pragma unroll
-                for (int u = 0; u < A_PER / 4; u++) {
+                for (int u = 0; u < A_PER / VW; u++) {
                     int r, kk;
                     vec_rk(u, p.a_rows_fast, BM, r, kk);
-                    if (p.a_rows_fast) {
+                    if (V4 && p.a_rows_fast) {
                         *(float4*)&As[buf][0][kk][r] =
-                            make_float4(ra[4 * u][0], ra[4 * u + 1][0], ra[4 * u + 2][0], ra[4 * u + 3][0]);
+                            make_float4(ra[VW * u][0], ra[VW * u + 1][0], ra[VW * u + 2][0], ra[VW * u + 3][0]);
+                    } else if (p.a_rows_fast) {
+#pragma unroll
+                        for (int h = 0; h < VW; h++) As[buf][0][kk][r + h] = ra[VW * u + h][0];
                     } else {
 #pragma unroll
-                        for (int h = 0; h < 4; h++) As[buf][0][kk + h][r] = ra[4 * u + h][0];
+                        for (int h = 0; h < VW; h++) As[buf][0][kk + h][r] = ra[VW * u + h][0];
                     }
                 }
                 goto b_store;
@@ -271,15 +281,18 @@ k_simt(Params p)
         if constexpr (VB) {
             if (p.b_vec) {
 #pragma unroll
-                for (int u = 0; u < B_PER / 4; u++) {
+                for (int u = 0; u < B_PER / VW; u++) {
                     int r, kk;
                     vec_rk(u, p.b_rows_fast, BN, r, kk);
-                    if (p.b_rows_fast) {
+                    if (V4 && p.b_rows_fast) {
                         *(float4*)&Bs[buf][0][kk][r] =
-                            make_float4(rb[4 * u][0], rb[4 * u + 1][0], rb[4 * u + 2][0], rb[4 * u + 3][0]);
+                            make_float4(rb[VW * u][0], rb[VW * u + 1][0], rb[VW * u + 2][0], rb[VW * u + 3][0]);
+                    } else if (p.b_rows_fast) {
+#pragma unroll
+                        for (int h = 0; h < VW; h++) Bs[buf][0][kk][r + h] = rb[VW * u + h][0];
                     } else {
 #pragma unroll
-                        for (int h = 0; h < 4; h++) Bs[buf][0][kk + h][r] = rb[4 * u + h][0];
+                        for (int h = 0; h < VW; h++) Bs[buf][0][kk + h][r] = rb[VW * u + h][0];
                     }
                 }
                 return;
@@ -1272,25 +1285,26 @@ static auto with_cfg(int compute, int tile, F&& f)
 
 }  // namespace simt
 
-// Whether a binary32 operand can be read four elements at a time: its
-// contiguous mode (the first row mode when rows_fast, else the first
-// contracted mode) has stride 1 and an extent divisible by 4, every other
-// stride keeps 4-element alignment and the base is 16-byte aligned, so the
-// four neighbours of an aligned group lie in one 16-byte word (the extents
-// then make M or K a multiple of 4, and a group is wholly in range or not).
-static bool vec4_side(const simt::Modes& rows, const simt::Modes& ks, const simt::Modes& ls, int rows_fast,
-                      const void* base, int t)
+// Whether a real operand stored as the compute type can be read w elements
+// at a time (w = 4 binary32, 2 binary64): its contiguous mode (the first row
+// mode when rows_fast, else the first contracted mode) has stride 1 and an
+// extent divisible by w, every other stride keeps w-element alignment and the
+// base is 16-byte aligned, so the w neighbours of an aligned group lie in one
+// 16-byte word (the extents then make M or K a multiple of w, and a group is
+// wholly in range or not).
+static bool vec_side(const simt::Modes& rows, const simt::Modes& ks, const simt::Modes& ls, int rows_fast,
+                     const void* base, int t, int want_t, int w)
 {
-    if (t != T_F32 || ((uintptr_t)base & 15) != 0) return false;
+    if (t != want_t || ((uintptr_t)base & 15) != 0) return false;
     const simt::Modes& f = rows_fast ? rows : ks;
     const simt::Modes& o = rows_fast ? ks : rows;
-    if (f.n < 1 || f.s0[0] != 1 || f.ext[0] % 4 != 0) return false;
+    if (f.n < 1 || f.s0[0] != 1 || f.ext[0] % w != 0) return false;
     for (int j = 1; j < f.n; j++)
-        if (f.s0[j] % 4 != 0) return false;
+        if (f.s0[j] % w != 0) return false;
     for (int j = 0; j < o.n; j++)
-        if (o.s0[j] % 4 != 0) return false;
+        if (o.s0[j] % w != 0) return false;
     for (int j = 0; j < ls.n; j++)
-        if (ls.s0[j] % 4 != 0) return false;
+        if (ls.s0[j] % w != 0) return false;
     return true;
 }
 
@@ -1338,9 +1352,10 @@ static void simt_params(const tb_plan* P, const tb_ptrs* d, simt::Params& p)
     p.a_rows_fast = min_abs(Mm, wa) < min_abs(P->K, wa);
     p.b_rows_fast = min_abs(Nm, wb) < min_abs(P->K, wb);
     p.d_rows_fast = min_abs(Mm, 3) <= min_abs(Nm, 3);
-    if (P->compute == TB_R32) {
-        p.a_vec = vec4_side(p.am, p.ak, p.al, p.a_rows_fast, p.A, p.tA);
-        p.b_vec = vec4_side(p.bn, p.bk, p.bl, p.b_rows_fast, p.B, p.tB);
+    if (P->compute == TB_R32 || P->compute == TB_R64) {
+        const int want = P->compute == TB_R32 ? T_F32 : T_F64, w = P->compute == TB_R32 ? 4 : 2;
+        p.a_vec = vec_side(p.am, p.ak, p.al, p.a_rows_fast, p.A, p.tA, want, w);
+        p.b_vec = vec_side(p.bn, p.bk, p.bl, p.b_rows_fast, p.B, p.tB, want, w);
     }
 }
 

@@ -244,17 +244,18 @@ def test_complex_mode_n_products_streaming(tapp, oracle, gpu, ops, rank):
     tapp.lib.TAPP_destroy_executor(ex)
 
 
+@pytest.mark.parametrize("storage,prec", [(0, 0), (1, -1)])
 @pytest.mark.parametrize("a_t,b_t", [(False, False), (True, False), (False, True), (True, True)])
-def test_f32_gemm_vector_loads(tapp, oracle, gpu, a_t, b_t):
-    """Binary32 matrix products D[m,n] = A B + C whose operands are dense with
-    extents divisible by 4 (the tiled kernel reads them four elements at a
-    time, along rows or along the contraction), with ragged tiles (600 rows,
-    200 columns) and a contraction of 1000."""
-    rng = np.random.default_rng(400 + 2 * a_t + b_t)
+def test_gemm_vector_loads(tapp, oracle, gpu, storage, prec, a_t, b_t):
+    """Binary32 and binary64 matrix products D[m,n] = A B + C whose operands
+    are dense with extents divisible by 4 (the tiled kernel reads them 16
+    bytes at a time, along rows or along the contraction), with ragged tiles
+    (600 rows, 200 columns) and a contraction of 1000."""
+    rng = np.random.default_rng(400 + 2 * a_t + b_t + 10 * storage)
     M, N, K = 600, 200, 1000
     A = ([K, M], [2, 0]) if a_t else ([M, K], [0, 2])
     B = ([N, K], [1, 2]) if b_t else ([K, N], [2, 1])
-    case = spec_case(rng, 0, 0, (A[0], B[0], [M, N], [M, N]), (A[1], B[1], [0, 1], [0, 1]))
+    case = spec_case(rng, storage, prec, (A[0], B[0], [M, N], [M, N]), (A[1], B[1], [0, 1], [0, 1]))
     ex = tapp.create_executor()
     assert "path=simt" in describe(tapp, case, ex)
     check_against_f64(tapp, oracle, case, device=True, executor=ex)
