@@ -299,6 +299,23 @@ def make_executor(lib, stream, f32_mode=0, path=0, async_=True, status=False):
     return ex
 
 
+def replica_max(dist, value, device):
+    """The largest of a per-rank scalar over the ranks (the slowest replica's
+    time); the value itself with one rank (dist None)."""
+    if dist is None:
+        return value
+    import torch
+    x = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(x, op=dist.ReduceOp.MAX)
+    return float(x.item())
+
+
+def replica_tflops(world, flops_per_rank, seconds):
+    """Whole-job throughput of `world` replicas that each did `flops_per_rank`
+    in at most `seconds` (weak scaling: the work per rank is fixed)."""
+    return world * flops_per_rank / seconds / 1e12
+
+
 def time_device(torch, fn, steps, warmup, barrier, window=None):
     """Mean device time of one step in ms: `warmup` untimed steps, then
     `steps` steps between CUDA events on the current stream, bracketed by a
@@ -753,12 +770,8 @@ def run_b200(args):
         if dist is not None:
             dist.destroy_process_group()
         return
-    t_max = t_ms
-    if dist is not None:
-        x = torch.tensor([t_ms], device="cuda")
-        dist.all_reduce(x, op=dist.ReduceOp.MAX)
-        t_max = float(x.item())
-    value = world * FLOPS / (t_max * 1e-3) / 1e12
+    t_max = replica_max(dist, t_ms, "cuda")
+    value = replica_tflops(world, FLOPS, t_max * 1e-3)
 
     # ---------------- dominant kernel: GEMM duration per launch ----------------
     ex_s = make_executor(lib, stream, async_=False, status=True)
@@ -826,13 +839,10 @@ def run_b200(args):
         prod_h()
     torch.cuda.synchronize()
     e2e_s = (time.perf_counter() - t0) / e2e_steps
-    if dist is not None:
-        x = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(x, op=dist.ReduceOp.MAX)
-        e2e_s = float(x.item())
+    e2e_s = replica_max(dist, e2e_s, "cuda")
     h2d = sum(t.buf.nbytes for t in (case.A, case.B, case.C))
     d2h = case.D.buf.nbytes
-    e2e = {"value": world * FLOPS / e2e_s / 1e12, "unit": "TFLOP/s", "h2d_bytes_per_step": h2d,
+    e2e = {"value": replica_tflops(world, FLOPS, e2e_s), "unit": "TFLOP/s", "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1e3,
            "how": "TAPP_execute_product on pinned host buffers, synchronous; wall clock per call"}
     prod_h.close()
