@@ -112,6 +112,20 @@ TAPP_EXPORT size_t tapp_b200_describe_plan(TAPP_tensor_product plan, TAPP_execut
 TAPP_EXPORT long long tapp_b200_kernel_launches(void);
 
 /*
+ * Self-test of the bounded waits of the library's kernels (no counterpart in
+ * the reference). On the current device, one kernel waits, with the waits
+ * the tensor-core kernels use, on a flag that nothing raises and on an
+ * mbarrier phase that nothing completes, limit_ms each. A wait that runs out
+ * raises the kernel's abort word and returns, so the kernel ends and the
+ * context stays usable; this is how a stalled product turns into an error
+ * instead of a hang. *flag_wait_expired / *barrier_wait_expired are set to 1
+ * when the wait gave up and raised the abort word, 0 otherwise.
+ * Returns 0, TAPP_B200_ERR_INVALID (NULL outputs, limit_ms outside
+ * (0, 10000]) or TAPP_B200_ERR_CUDA.
+ */
+TAPP_EXPORT TAPP_error tapp_b200_selftest_waits(double limit_ms, int* flag_wait_expired, int* barrier_wait_expired);
+
+/*
  * TAPP_execute_product for callers that cannot allocate device memory while
  * they run a product: code running inside an allocator or memory manager,
  * or a program that has handed the whole device to its own pool. There is no

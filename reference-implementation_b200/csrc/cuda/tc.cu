@@ -489,9 +489,11 @@ __device__ __forceinline__ unsigned long long now_ns()
     return t;
 }
 
-// Waits for the phase of `parity` to complete; gives up after WAIT_NS (or at
-// once when another role already gave up) and returns false.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag)
+// Waits for the phase of `parity` to complete; gives up after limit_ns (4 s
+// in the kernels; or at once when another role already gave up), raises
+// *abort_flag and returns false.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
+                                          unsigned long long limit_ns = WAIT_NS)
 {
     if (mbar_try(bar, parity)) return true;
     const unsigned long long t0 = now_ns();
@@ -499,7 +501,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volati
         if (mbar_try(bar, parity)) return true;
         if ((i & 255) == 0) {
             if (*abort_flag) return false;
-            if (now_ns() - t0 > WAIT_NS) {
+            if (now_ns() - t0 > limit_ns) {
                 *abort_flag = 1;
                 return false;
             }
@@ -509,7 +511,8 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volati
 
 // Waits until another CTA raised *flag (acquire, GPU scope); gives up like
 // mbar_wait.
-__device__ __forceinline__ bool flag_wait(const int* flag, volatile int* abort_flag)
+__device__ __forceinline__ bool flag_wait(const int* flag, volatile int* abort_flag,
+                                          unsigned long long limit_ns = WAIT_NS)
 {
     const unsigned long long t0 = now_ns();
     for (uint32_t i = 0;; i++) {
@@ -518,12 +521,32 @@ __device__ __forceinline__ bool flag_wait(const int* flag, volatile int* abort_f
         if (v) return true;
         if ((i & 63) == 63) {
             if (*abort_flag) return false;
-            if (now_ns() - t0 > WAIT_NS) {
+            if (now_ns() - t0 > limit_ns) {
                 *abort_flag = 1;
                 return false;
             }
         }
     }
+}
+
+// Self-test of the bounded waits: one thread waits, with the kernels' own
+// flag_wait and mbar_wait, on a flag that nothing raises and on the first
+// phase of an mbarrier that nothing completes, limit_ns each. Both must give
+// up and raise the abort word; out = {flag wait returned, abort word after
+// it, barrier wait returned, abort word after it}.
+__global__ void k_wait_selftest(const int* flag, int* out, unsigned long long limit_ns)
+{
+    __shared__ uint64_t bar;
+    __shared__ int abort_word;
+    if (threadIdx.x != 0) return;
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    abort_word = 0;
+    out[0] = flag_wait(flag, &abort_word, limit_ns) ? 1 : 0;
+    out[1] = abort_word;
+    abort_word = 0;
+    out[2] = mbar_wait(&bar, 0, &abort_word, limit_ns) ? 1 : 0;
+    out[3] = abort_word;
 }
 
 __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* tm, uint64_t* bar, int c0, int c1, int c2)
@@ -2156,6 +2179,25 @@ int tbk_run_plan_tc_noalloc(const tb_plan* P, const tb_ptrs* d, void* stream, in
     e = launch_gemm(kind, false, grid, tmA, tmB, gp, idesc, tmC, tmD, s);
     count_launch();
     (*kernels)++;
+    return (int)e;
+}
+
+// Runs k_wait_selftest with waits of limit_ns and copies its four words to
+// out (synchronises; the flag and the words are allocated for the call).
+int tbk_wait_selftest(unsigned long long limit_ns, int* out)
+{
+    int* d = nullptr;
+    cudaError_t e = cudaMalloc((void**)&d, 8 * sizeof(int));
+    if (e != cudaSuccess) return (int)e;
+    e = cudaMemset(d, 0, 8 * sizeof(int));
+    if (e == cudaSuccess) {
+        tb::tc::k_wait_selftest<<<1, 32>>>(d, d + 4, limit_ns);
+        tb::count_launch();
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(out, d + 4, 4 * sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(d);
     return (int)e;
 }
 

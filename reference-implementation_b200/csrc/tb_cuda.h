@@ -20,6 +20,7 @@ enum { TBK_H2D = 0, TBK_D2H = 1, TBK_D2D = 2 };
 enum { TBK_ERR_NOMEM = 2 };  /* cudaErrorMemoryAllocation */
 
 int tbk_device_count(int* count);
+int tbk_wait_selftest(unsigned long long limit_ns, int* out);
 int tbk_pointer_kind(const void* p, int* kind, int* device);
 /* as tbk_pointer_kind; for device and managed memory also the allocation
  * holding p, [start, start + size) */

@@ -245,3 +245,16 @@ def test_planner_long_contraction_few_outputs(tapp, dims, path):
     plan, infos = _plan(tapp, case)
     assert f"path={path}" in tapp.describe(plan), tapp.describe(plan)
     tapp.lib.TAPP_destroy_tensor_product(plan)
+
+
+def test_wait_selftest_argument_checks(tapp):
+    """tapp_b200_selftest_waits refuses NULL outputs and limits outside
+    (0, 10 s] before touching a device."""
+    f = tapp.lib.tapp_b200_selftest_waits
+    f.restype = C.c_int
+    f.argtypes = [C.c_double, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    a, b = C.c_int(0), C.c_int(0)
+    assert f(100.0, None, C.byref(b)) == tapp_b200.ERR_INVALID
+    assert f(100.0, C.byref(a), None) == tapp_b200.ERR_INVALID
+    for bad in (0.0, -1.0, 1e9, float("nan")):
+        assert f(bad, C.byref(a), C.byref(b)) == tapp_b200.ERR_INVALID
