@@ -73,3 +73,42 @@ def test_reference_arm_runs_on_rank_zero_only(monkeypatch):
 
     monkeypatch.setattr(bench, "cpu_reference_run", must_not_run)
     assert bench.run_reference(SimpleNamespace(steps=2, warmup=1, gpus=2)) is None
+
+
+def _rank_leaving(rank: int, world: int, port: int, q) -> None:
+    """Rank 1 leaves after joining the group, before the collective; rank 0
+    must get an error from its next collective within the group's timeout."""
+    from datetime import timedelta
+    import time
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    import bench
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=5))
+    if rank == 1:
+        os._exit(0)  # gone without a word, between steps
+    t0 = time.monotonic()
+    try:
+        bench.replica_max(dist, 1.0, "cpu")
+        q.put(("no error", time.monotonic() - t0))
+    except Exception as e:  # the peer's departure surfaces as an error, not a hang
+        q.put(("error", time.monotonic() - t0, type(e).__name__))
+    q.close()
+    q.join_thread()  # the result is in the pipe before the process ends
+    os._exit(0)
+
+
+def test_departed_rank_ends_the_next_collective_with_an_error():
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_leaving, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = q.get(timeout=120)
+    for p in procs:
+        p.join(30)
+        if p.is_alive():
+            p.kill()
+    assert got[0] == "error", got
+    assert got[1] < 60.0, got
