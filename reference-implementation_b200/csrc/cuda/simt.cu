@@ -1391,58 +1391,78 @@ static int narrow_width(const tb_plan* P, const simt::Params& p)
     return nb;
 }
 
+// Which narrow kernel a turned view runs, and what it stages: one decision
+// for the launcher and for tapp_b200_describe_plan.
+//   NK_REG     k_narrow: register prefetch, conversion and rounding at load
+//   NK_STREAM  k_narrow_stream: A read as stored (binary32, also under the
+//              16-bit precisions, which round after the copy; binary64 up to
+//              width 48 with D contiguous along its rows)
+//   NK_COOP    k_narrow_coop: binary32 streaming with A contiguous along the
+//              contraction and D along the columns (C staged whenever read)
+enum { NK_REG = 1, NK_STREAM = 2, NK_COOP = 3 };
+struct NarrowChoice {
+    int kind;
+    bool rnd, stage_c;
+    size_t smem;
+};
+
+static NarrowChoice narrow_choice(const simt::Params& p, int nb, size_t es)
+{
+    using namespace simt;
+    NarrowChoice c;
+    const bool f32 = es == 4;
+    const size_t ring = f32 ? StreamRing<float>::bytes : StreamRing<double>::bytes;
+    size_t smem = es * (size_t)nb * (size_t)p.K + 8 * ((size_t)p.K + 2 * (size_t)nb);
+    // binary64 wider than 48 leaves no registers for the ring's bookkeeping;
+    // binary64 with D contiguous along the columns: each thread would write a
+    // row of its own, and the ring only costs occupancy
+    const bool stream_ok = f32 || nb <= 48;
+    const int t_own = f32 ? T_F32 : T_F64;
+    c.rnd = p.round_in != TB_ROUND_NONE;  // rounding after the copy is the rounding load's for binary32 only
+    const bool stream = stream_ok && p.tA == t_own && (!c.rnd || f32) && (uintptr_t)p.A % es == 0 &&
+                        (f32 || p.d_rows_fast);
+    c.kind = stream ? NK_STREAM : NK_REG;
+    c.stage_c = false;
+    if (stream) {
+        smem += ring;
+        const size_t cb = es * (size_t)nb * 256;
+        if (!p.beta_zero && p.tC == t_own && (uintptr_t)p.C % es == 0 && smem + cb <= (size_t)NARROW_MAX_SMEM + ring) {
+            c.stage_c = true;
+            smem += cb;
+        }
+    }
+    if (f32 && stream && !p.a_rows_fast && !p.d_rows_fast) {
+        const size_t coop_smem = es * (size_t)StreamRing<float>::S * 256 * (COOP_KC + 1) + es * 256 * (nb + 1) +
+                                 es * (size_t)nb * (size_t)p.K + 16 + 8 * ((size_t)p.K + 2 * (size_t)nb);
+        const bool c_ok = p.beta_zero || (p.tC == t_own && (uintptr_t)p.C % es == 0);
+        if (c_ok && coop_smem <= NARROW_COOP_SMEM) {
+            c.kind = NK_COOP;
+            c.stage_c = !p.beta_zero;
+            smem = coop_smem;
+        }
+    }
+    c.smem = smem;
+    return c;
+}
+
 template <typename T, int NB>
 static cudaError_t launch_narrow_t(simt::NarrowParams& np, cudaStream_t s)
 {
     using namespace simt;
     const Params& p = np.p;
-    size_t smem = sizeof(T) * NB * (size_t)p.K + 8 * ((size_t)p.K + 2 * NB);
-    // A read as stored: the streaming kernel (cp.async ring); else the
-    // register-prefetch kernel, which converts and rounds A at load. Not for
-    // binary64 wider than 48 (its accumulators leave no registers) nor binary64
-    // products whose D is contiguous along the columns (each thread then
-    // writes a row of its own, and the ring only costs occupancy).
-    constexpr bool stream_ok = !(sizeof(T) == 8 && NB > 48);
-    const int t_own = sizeof(T) == 4 ? T_F32 : T_F64;
-    const bool plain_a = p.tA == t_own && p.round_in == TB_ROUND_NONE;
-    // rounding after the copy is the rounding load's only for binary32 storage
-    const bool rnd = p.round_in != TB_ROUND_NONE;
-    const bool stream = stream_ok && p.tA == t_own && (!rnd || sizeof(T) == 4) && (uintptr_t)p.A % sizeof(T) == 0 &&
-                        (sizeof(T) == 4 || p.d_rows_fast);
+    const NarrowChoice ch = narrow_choice(p, NB, sizeof(T));
+    const bool plain_a = p.tA == (sizeof(T) == 4 ? T_F32 : T_F64) && p.round_in == TB_ROUND_NONE;
     void (*kern)(NarrowParams) = plain_a ? k_narrow<T, NB, true> : k_narrow<T, NB, false>;
-    if constexpr (stream_ok) {
-        if constexpr (sizeof(T) == 4) {
-            if (stream) kern = rnd ? k_narrow_stream<T, NB, true> : k_narrow_stream<T, NB, false>;
-        } else {
-            if (stream) kern = k_narrow_stream<T, NB, false>;
-        }
-    }
-    // C staged when it is read as stored and the shared memory allows
-    np.stage_c = 0;
-    if (stream) {
-        smem += StreamRing<T>::bytes;
-        const size_t cb = sizeof(T) * NB * 256;
-        if (!p.beta_zero && p.tC == t_own && (uintptr_t)p.C % sizeof(T) == 0 &&
-            smem + cb <= (size_t)NARROW_MAX_SMEM + StreamRing<T>::bytes) {
-            np.stage_c = 1;
-            smem += cb;
-        }
-    }
-    // A contiguous along the contraction and D along the columns: the
-    // cooperative variant (binary32; C staged whenever it is read)
-    int variant = stream ? 2 + (int)rnd : plain_a ? 1 : 0;
     if constexpr (sizeof(T) == 4) {
-        const size_t coop_smem = sizeof(T) * (size_t)StreamRing<T>::S * 256 * (COOP_KC + 1) +
-                                 sizeof(T) * 256 * (NB + 1) + sizeof(T) * NB * (size_t)p.K + 16 +
-                                 8 * ((size_t)p.K + 2 * NB);
-        const bool c_ok = p.beta_zero || (p.tC == t_own && (uintptr_t)p.C % sizeof(T) == 0);
-        if (stream && !p.a_rows_fast && !p.d_rows_fast && c_ok && coop_smem <= NARROW_COOP_SMEM) {
-            kern = rnd ? k_narrow_coop<T, NB, true> : k_narrow_coop<T, NB, false>;
-            np.stage_c = !p.beta_zero;
-            smem = coop_smem;
-            variant = 4 + (int)rnd;
-        }
+        if (ch.kind == NK_STREAM) kern = ch.rnd ? k_narrow_stream<T, NB, true> : k_narrow_stream<T, NB, false>;
+        if (ch.kind == NK_COOP) kern = ch.rnd ? k_narrow_coop<T, NB, true> : k_narrow_coop<T, NB, false>;
+    } else if constexpr (NB <= 48) {
+        if (ch.kind == NK_STREAM) kern = k_narrow_stream<T, NB, false>;
     }
+    np.stage_c = ch.stage_c ? 1 : 0;
+    const size_t smem = ch.smem;
+    const bool stream = ch.kind != NK_REG;
+    const int variant = ch.kind == NK_COOP ? 4 + (int)ch.rnd : ch.kind == NK_STREAM ? 2 + (int)ch.rnd : plain_a ? 1 : 0;
     static int attr_done[64][6];
     int dev = 0;
     cudaGetDevice(&dev);
@@ -1540,3 +1560,20 @@ cudaError_t launch_simt(const tb_plan* P, const tb_ptrs* d, cudaStream_t s)
 }
 
 }  // namespace tb
+
+// The CUDA-core kernel a plan of the simt path runs, for operands aligned to
+// their element size (the launcher falls back to the register-prefetch or
+// tiled kernel for others): 0 tiled, 1 narrow with register prefetch, 2
+// narrow streaming, 3 narrow cooperative, 4 complex narrow streaming. No
+// device call.
+extern "C" int tbk_simt_kernel(const tb_plan* P)
+{
+    using namespace tb;
+    simt::Params p;
+    tb_ptrs d = {nullptr, nullptr, nullptr, nullptr};
+    simt_params(P, &d, p);
+    const int nb = narrow_width(P, p);
+    if (!nb) return 0;
+    if (P->compute == TB_C32) return 4;
+    return narrow_choice(p, nb, P->compute == TB_R32 ? 4 : 8).kind;
+}

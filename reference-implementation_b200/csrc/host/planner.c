@@ -466,6 +466,11 @@ size_t tb_describe(const tb_plan* p, size_t maxlen, char* out)
              p->beta_zero);
     if (p->path == TB_PATH_TC) at = put(out, maxlen, at, " tc_mode=%s", tcm[p->tc_mode]);
     if (p->path == TB_PATH_SLICED) at = put(out, maxlen, at, " slices=%d", p->slices);
+    if (p->path == TB_PATH_SIMT) {
+        static const char* kern[] = {"tiled", "narrow", "narrow_stream", "narrow_coop", "narrow_cstream"};
+        const int k = tbk_simt_kernel(p);
+        if (k >= 0 && k <= 4) at = put(out, maxlen, at, " kernel=%s", kern[k]);
+    }
     at = put_modes(out, maxlen, at, "F", &p->F);
     at = put_modes(out, maxlen, at, "K", &p->K);
     at = put_modes(out, maxlen, at, "UA", &p->UA);

@@ -258,3 +258,40 @@ def test_wait_selftest_argument_checks(tapp):
     assert f(100.0, C.byref(a), None) == tapp_b200.ERR_INVALID
     for bad in (0.0, -1.0, 1e9, float("nan")):
         assert f(bad, C.byref(a), C.byref(b)) == tapp_b200.ERR_INVALID
+
+
+@pytest.mark.parametrize("core,mode,rank,storage,prec,kernel", [
+    ([64, 40, 32, 32], 1, 38, 0, 0, "narrow_stream"),     # rows contiguous in A and D
+    ([64, 40, 32, 32], 0, 38, 0, 0, "narrow_coop"),       # A along the contraction, D along the rank
+    ([64, 40, 32, 32], 1, 24, 0, 6, "narrow_stream"),     # bf16 precision: rounding after the copy
+    ([64, 40, 32, 32], 1, 24, 1, -1, "narrow_stream"),    # binary64, rows contiguous
+    ([64, 40, 32, 32], 0, 38, 1, -1, "narrow"),           # binary64 with D along the rank
+    ([64, 40, 32, 32], 1, 60, 1, -1, "narrow"),           # binary64 wider than 48
+    ([64, 40, 32, 32], 1, 24, 2, -1, "narrow_cstream"),   # complex float
+    ([64, 40, 32, 32], 1, 24, 3, -1, "tiled"),            # complex double
+])
+def test_planner_reports_the_cuda_core_kernel(tapp, core, mode, rank, storage, prec, kernel):
+    """tapp_b200_describe_plan names the CUDA-core kernel a mode-n product of
+    the simt path runs, from its layout, types and width."""
+    from tapp_b200.workloads import RequestSpec, case_from_spec
+    o = len(core)
+    d_ext = list(core)
+    d_ext[mode] = rank
+    d_idx = list(range(o))
+    d_idx[mode] = o
+    case = case_from_spec(np.random.default_rng(0), RequestSpec("tucker", storage, prec, (core, [rank, core[mode]], d_ext, d_ext),
+                                                                (list(range(o)), [o, mode], d_idx, d_idx), 0.7, 0.3))
+    plan, infos = _plan(tapp, case)
+    d = tapp.describe(plan)
+    assert "path=simt" in d and f" kernel={kernel} " in d, d
+    tapp.lib.TAPP_destroy_tensor_product(plan)
+
+
+def test_planner_reports_tiled_kernel_for_wide_products(tapp):
+    A = alloc(0, [512, 256], [1, 512], [0, 2])
+    B = alloc(0, [256, 384], [1, 256], [2, 1])
+    Cc = alloc(0, [512, 384], [1, 512], [0, 1])
+    D = alloc(0, [512, 384], [1, 512], [0, 1])
+    plan, infos = _plan(tapp, Case(A, B, Cc, D, scalar(0, 1.0), scalar(0, 1.0), 0))
+    assert " kernel=tiled " in tapp.describe(plan)
+    tapp.lib.TAPP_destroy_tensor_product(plan)
