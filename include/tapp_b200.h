@@ -112,6 +112,14 @@ TAPP_EXPORT size_t tapp_b200_describe_plan(TAPP_tensor_product plan, TAPP_execut
 TAPP_EXPORT long long tapp_b200_kernel_launches(void);
 
 /*
+ * Number of memory allocations (device memory from the library's pool or
+ * cudaMalloc, page-locked host staging) this library asked CUDA for since
+ * the process started (all threads, all devices). A diagnostic: it lets a
+ * caller check that a code path allocated nothing.
+ */
+TAPP_EXPORT long long tapp_b200_device_allocations(void);
+
+/*
  * Self-test of the bounded waits of the library's kernels (no counterpart in
  * the reference). On the current device, one kernel waits, with the waits
  * the tensor-core kernels use, on a flag that nothing raises and on an
@@ -134,14 +142,19 @@ TAPP_EXPORT TAPP_error tapp_b200_selftest_waits(double limit_ms, int* flag_wait_
  * Runs the tensor-core path (BF16BF16_ACCUM_F32, F16F16_ACCUM_F32/_F16, or
  * F32 with TAPP_B200_ATTR_F32_MODE = 1) with its packed-operand scratch in a
  * fixed 32 MiB device array of the library (held on every GPU that loads the
- * library until the process exits); it calls no device or host allocator.
- * A, B, C and D must be device pointers (TAPP_B200_ERR_INVALID otherwise);
- * other precisions return TAPP_B200_ERR_UNSUPPORTED; products whose operand
- * panels need more than the array holds return TAPP_B200_ERR_SCRATCH without
- * launching anything. The first call on a device looks up the array's device
- * address with that device current: make it before any stream capture.
- * Every call shares the array, so calls whose work overlaps on the GPU race.
- * Codes and validation are otherwise those of TAPP_execute_product.
+ * library until the process exits); the library calls no device allocator
+ * (and no host allocator) on this path. A, B, C and D must be device
+ * pointers (TAPP_B200_ERR_INVALID otherwise); other precisions return
+ * TAPP_B200_ERR_UNSUPPORTED; products whose operand panels need more than the
+ * array holds return TAPP_B200_ERR_SCRATCH without launching anything. The
+ * first call on a device (and the first after a cudaDeviceReset) looks up the
+ * array's device address with that device current: make it before any stream
+ * capture. Every call shares the array, so calls whose work overlaps on the
+ * GPU race. With an asynchronous executor the call returns before its kernels
+ * run and cannot read their error word: a bounded wait that expired there is
+ * reported (TAPP_B200_ERR_CUDA) by the next synchronous call of this entry
+ * point on that device. Codes and validation are otherwise those of
+ * TAPP_execute_product.
  */
 TAPP_EXPORT TAPP_error tapp_b200_execute_product_noalloc(TAPP_tensor_product plan, TAPP_executor exec,
                                                          const void* alpha, const void* A, const void* B,

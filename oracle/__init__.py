@@ -25,14 +25,16 @@ class _OTensor(C.Structure):
                 ("idx", C.POINTER(C.c_int64))]
 
 
-def build(with_reference: bool = False) -> None:
-    """Compile the oracle (and the reference, if its sources are present)."""
+def build(reference_dir: str | None = None) -> None:
+    """Compile the oracle; with `reference_dir` (or TAPP_REFERENCE_DIR) naming
+    a checkout of the reference whose sources are present, also build the
+    reference itself into _ref/."""
     targets = ["all"]
-    if with_reference and os.path.isdir(os.environ.get("TAPP_REFERENCE_DIR", "/root/reference")):
-        targets.append("ref")
     env = dict(os.environ)
-    if "TAPP_REFERENCE_DIR" in env:
-        env["REF"] = env["TAPP_REFERENCE_DIR"]
+    ref = reference_dir or env.get("TAPP_REFERENCE_DIR")
+    if ref and os.path.isfile(os.path.join(ref, "reference_implementation", "src", "product.c")):
+        targets.append("ref")
+        env["REF"] = ref
     subprocess.run(["make", "-s", "-C", HERE] + targets, check=True, env=env)
 
 

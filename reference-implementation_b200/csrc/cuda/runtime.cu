@@ -13,8 +13,10 @@
 namespace tb {
 
 static std::atomic<long long> g_launches{0};
+static std::atomic<long long> g_allocations{0};
 
 void count_launch(int n) { g_launches += n; }
+void count_allocation() { g_allocations++; }
 
 // One device word per GPU that kernels set when a bounded wait expires; the
 // host reads and clears it after synchronous executions.
@@ -28,6 +30,7 @@ int* device_error_word()
     std::lock_guard<std::mutex> lk(g_err_mutex);
     if (!g_err_word[dev]) {
         int* p = nullptr;
+        count_allocation();
         if (cudaMalloc(&p, sizeof(int)) != cudaSuccess) return nullptr;
         if (cudaMemset(p, 0, sizeof(int)) != cudaSuccess) return nullptr;
         g_err_word[dev] = p;
@@ -47,6 +50,7 @@ cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t s)
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
+    count_allocation();
     if (dev < 0 || dev >= 64) return cudaMallocAsync(p, bytes, s);
     {
         std::lock_guard<std::mutex> lk(g_pool_mutex);
@@ -91,6 +95,7 @@ cudaError_t stage_copy(void* dev_dst, const void* src, size_t bytes, cudaStream_
     std::lock_guard<std::mutex> lk(g_ring_mutex);
     StageRing& r = g_ring[dev];
     if (!r.host) {
+        count_allocation();
         e = cudaMallocHost((void**)&r.host, RING_SLOTS * RING_SLOT_BYTES);
         if (e != cudaSuccess) {
             r.host = nullptr;
@@ -329,7 +334,11 @@ int tbk_host_func(void* stream, void (*fn)(void*), void* arg)
     return (int)cudaLaunchHostFunc((cudaStream_t)stream, fn, arg);
 }
 
-int tbk_host_alloc(void** p, size_t bytes) { return (int)cudaMallocHost(p, bytes); }
+int tbk_host_alloc(void** p, size_t bytes)
+{
+    tb::count_allocation();
+    return (int)cudaMallocHost(p, bytes);
+}
 int tbk_host_free(void* p) { return (int)cudaFreeHost(p); }
 
 size_t tbk_group_bytes(int n) { return tb::group_descriptor_bytes(n); }
@@ -356,6 +365,7 @@ int tbk_run_group(const tb_plan* const* plans, const tb_ptrs* ptrs, int n, void*
 }
 
 long long tbk_launch_count(void) { return tb::g_launches.load(); }
+long long tbk_allocation_count(void) { return tb::g_allocations.load(); }
 
 int tbk_check_device_error(void)
 {

@@ -16,6 +16,8 @@ enum { T_F32 = 0, T_F64 = 1, T_C32 = 2, T_C64 = 3, T_F16 = 4, T_BF16 = 5 };
 namespace tb {
 
 void count_launch(int n = 1);
+// counts one device or page-locked host allocation the library asks CUDA for
+void count_allocation();
 // stream-ordered allocation from the library's own device pool (runtime.cu)
 cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t s);
 

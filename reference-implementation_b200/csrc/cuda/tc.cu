@@ -2011,12 +2011,17 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
 //   - The array's device address is looked up once per device, with that
 //     device current, on the first call there (cudaGetSymbolAddress; the name
 //     of a __device__ array is only a host-side stand-in, not an address the
-//     GPU can use). Make that first call before any stream capture.
+//     GPU can use), and again on the first call after a cudaDeviceReset gave
+//     the device a new context. Make that first call before any stream
+//     capture.
 //   - All calls share the array and it keeps the last call's contents; calls
 //     whose work overlaps on the GPU (other streams, or several host threads)
 //     race on it. The pack kernels write every panel element the GEMM reads,
 //     padding included; only the error word has to start at zero and is
 //     cleared at set-up and after each reported error.
+//   - A synchronous call reads the error word after its kernels; an
+//     asynchronous call cannot, so a wait that expired in it is reported by
+//     the next synchronous call on the same device.
 namespace tb {
 namespace tc {
 
@@ -2026,9 +2031,39 @@ constexpr size_t NOALLOC_RESERVED = 256;              // error word + padding at
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH];
 
 static void* g_noalloc_ptr[64];
+static unsigned long long g_noalloc_ctx[64];  // id of the context the address belongs to
 static std::mutex g_noalloc_mutex;
 
-// device address of the array on the current device (set-up on first use)
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
+
+// Unique id of the current context (0 when the driver cannot tell). A
+// cudaDeviceReset ends the context and the next one gets a new id, so an
+// address looked up in the old one is not reused.
+static unsigned long long current_ctx_id()
+{
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = (CtxGetCurrentFn)p;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = (CtxGetIdFn)p;
+    });
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS)
+        return 0;
+    return id;
+}
+
+// device address of the array on the current device (set-up on first use in
+// each context of the device)
 static cudaError_t noalloc_base(void** out)
 {
     int dev = 0;
@@ -2036,13 +2071,17 @@ static cudaError_t noalloc_base(void** out)
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
     std::lock_guard<std::mutex> lk(g_noalloc_mutex);
-    if (!g_noalloc_ptr[dev]) {
+    // 0 when the driver cannot name the context: the address is then kept
+    // for the life of the process
+    const unsigned long long ctx = g_noalloc_ptr[dev] ? current_ctx_id() : 0;
+    if (!g_noalloc_ptr[dev] || (ctx != 0 && g_noalloc_ctx[dev] != ctx)) {
         void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);  // makes the device's context current
         if (e != cudaSuccess) return e;
         e = cudaMemset(p, 0, NOALLOC_RESERVED);  // error word starts at zero
         if (e != cudaSuccess) return e;
         g_noalloc_ptr[dev] = p;
+        g_noalloc_ctx[dev] = current_ctx_id();
     }
     *out = g_noalloc_ptr[dev];
     return cudaSuccess;
@@ -2187,6 +2226,7 @@ int tbk_run_plan_tc_noalloc(const tb_plan* P, const tb_ptrs* d, void* stream, in
 int tbk_wait_selftest(unsigned long long limit_ns, int* out)
 {
     int* d = nullptr;
+    tb::count_allocation();
     cudaError_t e = cudaMalloc((void**)&d, 8 * sizeof(int));
     if (e != cudaSuccess) return (int)e;
     e = cudaMemset(d, 0, 8 * sizeof(int));

@@ -7,8 +7,9 @@
  *
  * It runs the same tensor-core kernels as TAPP_execute_product, but takes the
  * packed operand panels from a fixed 32 MiB device array that the library
- * owns, and never calls cudaMalloc, cudaFree or any other allocator (nor the
- * host heap). Consequences:
+ * owns; this path of the library calls neither cudaMalloc, cudaFree nor any
+ * other device or host allocator (validation included: the self-aliasing
+ * check needs no temporaries). Consequences:
  *   - all four operand pointers must be device pointers (host operands would
  *     need staging buffers);
  *   - only products that the tensor cores run qualify (BF16BF16_ACCUM_F32,
@@ -17,7 +18,10 @@
  *     TAPP_B200_ERR_SCRATCH before any launch;
  *   - the first call on a device looks the array's device address up (make
  *     it before any stream capture), and calls whose work overlaps on the GPU
- *     share the array and race on it.
+ *     share the array and race on it;
+ *   - a synchronous call reports a bounded wait that expired in its kernels
+ *     (TAPP_B200_ERR_CUDA); an asynchronous call returns before they run, so
+ *     such an expiry is reported by the next synchronous call on the device.
  */
 #include <string.h>
 

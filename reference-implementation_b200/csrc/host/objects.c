@@ -209,3 +209,8 @@ long long tapp_b200_kernel_launches(void)
 {
     return tbk_launch_count();
 }
+
+long long tapp_b200_device_allocations(void)
+{
+    return tbk_allocation_count();
+}

@@ -54,32 +54,35 @@ static int structure(const tb_tensor_view* C, const tb_tensor_view* D)
 /* Modes sorted by |stride| (ties: smaller extent first, the order the
  * reference's merge sort produces); each stride must reach past the span of
  * the previous mode. A zero stride aliases when there are two or more modes.
- * The reference sorts through int temporaries (:923-926); this keeps 64 bits. */
+ * The reference sorts through int temporaries (:923-926); this keeps 64 bits.
+ * No sorted copy is made: for every mode, its successor in that order (the
+ * smallest (|stride|, extent, position) above its own) is found by a scan,
+ * which compares the same neighbouring pairs as a sort would, in O(n^2) time
+ * and no memory (the allocation-free entry point validates through here). */
 static int aliasing(const tb_tensor_view* D)
 {
     int n = D->nmode;
     if (n <= 1) return 0;
     for (int i = 0; i < n; i++)
         if (D->strides[i] == 0) return 8;
-    int64_t s[TB_MAXMODES * 4], e[TB_MAXMODES * 4];
-    int64_t *ps = s, *pe = e;
-    if (n > TB_MAXMODES * 4) {
-        ps = malloc(sizeof(int64_t) * (size_t)n);
-        pe = malloc(sizeof(int64_t) * (size_t)n);
-        if (!ps || !pe) { free(ps); free(pe); return TAPP_B200_ERR_NOMEM; }
-    }
     for (int i = 0; i < n; i++) {
-        int64_t v = D->strides[i] < 0 ? -D->strides[i] : D->strides[i], x = D->extents[i];
-        int j = i - 1;
-        while (j >= 0 && (ps[j] > v || (ps[j] == v && pe[j] > x))) { ps[j + 1] = ps[j]; pe[j + 1] = pe[j]; j--; }
-        ps[j + 1] = v;
-        pe[j + 1] = x;
+        const int64_t vi = D->strides[i] < 0 ? -D->strides[i] : D->strides[i], xi = D->extents[i];
+        int next = -1;
+        int64_t vn = 0, xn = 0;
+        for (int j = 0; j < n; j++) {
+            if (j == i) continue;
+            const int64_t vj = D->strides[j] < 0 ? -D->strides[j] : D->strides[j], xj = D->extents[j];
+            const int above = vj > vi || (vj == vi && (xj > xi || (xj == xi && j > i)));
+            if (!above) continue;
+            if (next < 0 || vj < vn || (vj == vn && (xj < xn || (xj == xn && j < next)))) {
+                next = j;
+                vn = vj;
+                xn = xj;
+            }
+        }
+        if (next >= 0 && vn < vi * xi) return 8;
     }
-    int r = 0;
-    for (int i = 0; i + 1 < n; i++)
-        if (ps[i + 1] < ps[i] * pe[i]) { r = 8; break; }
-    if (ps != s) { free(ps); free(pe); }
-    return r;
+    return 0;
 }
 
 int tb_scalar_is_zero(const void* s, TAPP_datatype t)

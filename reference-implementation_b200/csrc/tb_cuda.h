@@ -67,6 +67,7 @@ int tbk_run_group(const tb_plan* const* plans, const tb_ptrs* ptrs, int n, void*
                   void* stream);
 
 long long tbk_launch_count(void);
+long long tbk_allocation_count(void);
 
 /* Reads (and clears) the word kernels set when one of their bounded waits
  * expired; returns 0 or a cudaError_t value. Synchronises the device. */

@@ -50,6 +50,8 @@ class B200Lib(TappLib):
         L.tapp_b200_describe_plan.argtypes = [intptr, intptr, C.c_size_t, C.c_char_p]
         L.tapp_b200_kernel_launches.restype = C.c_longlong
         L.tapp_b200_kernel_launches.argtypes = []
+        L.tapp_b200_device_allocations.restype = C.c_longlong
+        L.tapp_b200_device_allocations.argtypes = []
         L.TAPP_attr_set.restype = C.c_int
         L.TAPP_attr_set.argtypes = [intptr, C.c_int, C.c_void_p]
         L.TAPP_attr_get.restype = C.c_int
@@ -85,6 +87,9 @@ class B200Lib(TappLib):
 
     def launches(self) -> int:
         return int(self.lib.tapp_b200_kernel_launches())
+
+    def allocations(self) -> int:
+        return int(self.lib.tapp_b200_device_allocations())
 
 
 def load() -> B200Lib:

@@ -2,7 +2,9 @@
 
 Run in a container where the reference sources are present:
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference <reference checkout>
+
+(or with TAPP_REFERENCE_DIR set instead of --reference)
 
 What it does:
   1. builds the reference from its own C sources (oracle/Makefile, target
@@ -165,8 +167,11 @@ def _ref_code(ref, rec) -> int:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get("TAPP_REFERENCE_DIR", "/root/reference"))
+    ap.add_argument("--reference", default=os.environ.get("TAPP_REFERENCE_DIR"),
+                    help="checkout of the reference (default: $TAPP_REFERENCE_DIR)")
     a = ap.parse_args()
+    if not a.reference:
+        ap.error("give --reference <reference checkout> or set TAPP_REFERENCE_DIR")
     build_and_record(a.reference)
     explain_strings()
     error_cases()

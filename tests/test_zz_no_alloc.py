@@ -45,10 +45,37 @@ def _device(case, torch):
     return out
 
 
-@pytest.mark.parametrize("prec,split", [(tapp_b200.TAPP_BF16BF16_ACCUM_F32, 0), (tapp_b200.TAPP_F32F32_ACCUM_F32, 1)])
-def test_noalloc_matches_execute_product(tapp, oracle, gpu, prec, split):
+def _matmul_case(rng, m, n, k, prec):
+    """D[m,n] = 1.3 sum_k A[m,k] B[k,n] + 0.7 C, binary32 storage, ragged
+    sizes (not multiples of the 128 x 256 tiles nor of the 64-deep
+    contraction blocks)."""
+    from tapp_b200.case import Case, alloc, fill_uniform, scalar
+    from tapp_b200.workloads import colmajor
+    T = lambda ext, idx: fill_uniform(alloc(tapp_b200.TAPP_F32, ext, colmajor(ext), [ord(c) for c in idx]), rng)
+    return Case(T([m, k], "mk"), T([k, n], "kn"), T([m, n], "mn"), T([m, n], "mn"),
+                scalar(tapp_b200.TAPP_F32, 1.3), scalar(tapp_b200.TAPP_F32, 0.7), prec, False, f"matmul_{m}x{n}x{k}")
+
+
+def _cases():
+    from tapp_b200.workloads import dense_contraction_case
+    F32, BF16P, F16P = tapp_b200.TAPP_F32F32_ACCUM_F32, tapp_b200.TAPP_BF16BF16_ACCUM_F32, 5
+    return [
+        ("dense16_bf16", lambda: large_dense_case(np.random.default_rng(21), BF16P, tapp_b200.TAPP_F32, extent=16), 0),
+        ("dense16_split", lambda: large_dense_case(np.random.default_rng(21), F32, tapp_b200.TAPP_F32, extent=16), 1),
+        ("matmul_ragged_f16", lambda: _matmul_case(np.random.default_rng(24), 200, 300, 150, F16P), 0),
+        ("matmul_ragged_split", lambda: _matmul_case(np.random.default_rng(25), 333, 129, 517, F32), 1),
+        ("complex_bf16", lambda: dense_contraction_case(np.random.default_rng(26), extent=12,
+                                                        dtype=tapp_b200.TAPP_C32, prec=BF16P), 0),
+    ]
+
+
+@pytest.mark.parametrize("name,make,split", _cases(), ids=[c[0] for c in _cases()])
+def test_noalloc_matches_execute_product(tapp, oracle, gpu, name, make, split):
+    """Two calls in a row through the allocation-free entry point give the D
+    that TAPP_execute_product gives (within the bound of the GPU tests), and
+    the library asks CUDA for no memory during them."""
     import torch
-    case = large_dense_case(np.random.default_rng(21), prec, tapp_b200.TAPP_F32, extent=16)
+    case = make()
     _, D64, scale = oracle.execute_f64(case.copy())
     bound = error_bound(case, scale, D64, 2.0 ** -16 if split else 0.0)
     plan, infos = _plan(tapp, case)
@@ -61,14 +88,19 @@ def test_noalloc_matches_execute_product(tapp, oracle, gpu, prec, split):
     err = tapp.lib.TAPP_execute_product(plan, ex, C.byref(st), case.alpha.ctypes.data, dev[0][1], dev[1][1],
                                         case.beta.ctypes.data, dev[2][1], dev[3][1])
     assert err == 0
-    want = dev[3][0].cpu().numpy().view(np.float32).astype(np.complex128)
+    # D is dense in every case: its buffer holds exactly its elements
+    read_d = lambda: dev[3][0].cpu().numpy().view(case.D.buf.dtype).astype(np.complex128)
+    want = read_d()
     noalloc = _noalloc(tapp)
     for call in range(2):
         dev[3][0].copy_(D0)
+        torch.cuda.synchronize()
+        a0 = tapp.allocations()
         err = noalloc(plan, ex, case.alpha.ctypes.data, dev[0][1], dev[1][1], case.beta.ctypes.data,
                       dev[2][1], dev[3][1])
         assert err == 0, tapp.explain(err)
-        got = dev[3][0].cpu().numpy().view(np.float32).astype(np.complex128)
+        assert tapp.allocations() == a0, "the allocation-free entry point asked CUDA for memory"
+        got = read_d()
         assert (np.abs(got - want) <= bound).all(), call
         assert (np.abs(got - D64) <= bound).all(), call
     tapp.lib.TAPP_destroy_executor(ex)
