@@ -4,25 +4,28 @@
 Workload (one step = one TAPP_execute_product): the dense 4-index
 contraction D[a,b,i,j] = sum_{c,d} A[a,c,i,d] B[d,b,c,j] + 0.5 C with every
 extent 64 (M = N = K = 4096), float32 storage, inputs N(0,1) with 1% of the
-entries scaled by 1e3, synthetic and seeded. The headline precision is
-TAPP_BF16BF16_ACCUM_F32 (bfloat16 products, float32 accumulation); the line
-also reports the other precision modes of the same product, among them the
-plain CUDA-core float32 path, each with its error against a binary64
-evaluation.
+entries scaled by 1e3, synthetic and seeded. The headline is the float32
+product (TAPP_F32F32_ACCUM_F32) in the library's split-bfloat16 mode: each
+operand split into a bfloat16 high and low part, three products accumulated
+in binary32 on the tensor cores; its error against a binary64 evaluation is
+on the line. The other precision modes of the same product (bfloat16, f16,
+16-bit storage, the plain CUDA-core float32 path) are reported under
+"modes", each with its error.
 
   value      TFLOP/s with all operands resident in HBM (2*M*N*K flops per
              step, CUDA events on the launching stream, max over ranks)
   e2e        the same through the C ABI with pinned HOST buffers: each step
              copies A, B, C to the device and D back (inside the timed region)
-  roofline   the dominant kernel (the tcgen05 GEMM): algorithmic flops per
-             launch / its measured duration, against the measured bf16 peak
+  roofline   the dominant kernel (the tcgen05 GEMM): useful flops per launch
+             / its measured duration, against the measured bf16 peak; the
+             tensor pipe runs three products per useful one (pipe_frac)
   cpu_baseline  the reference's own CPU product (built from its sources into
              oracle/_ref) on this host's cores, on a bounded slab of D
 
 `--impl reference` times only the reference's CPU product (all host threads)
-on the same workload and prints its line. Multi-GPU runs (torchrun) are
-replicas: every rank runs the whole product on its own GPU, no collective on
-the data path; timing is the max over ranks.
+on the same workload, metric and precision (float32) and prints its line.
+Multi-GPU runs (torchrun) are replicas: every rank runs the whole product on
+its own GPU, no collective on the data path; timing is the max over ranks.
 """
 from __future__ import annotations
 
@@ -31,7 +34,6 @@ import ctypes as C
 import json
 import os
 import statistics
-import subprocess
 import sys
 import threading
 import time
@@ -46,13 +48,16 @@ import numpy as np  # noqa: E402
 EXTENT = 64
 FLOPS = 2.0 * (EXTENT ** 2) ** 3          # 2 * M * N * K
 WORKLOAD = "dense_4index_contraction_64^4"
+METRIC = f"TFLOP/s ({WORKLOAD}, F32)"     # the same string on both arms
+HEADLINE = "split_bf16_f32"
+STEP_DESCRIPTION = "pack A, pack B (hi/lo bfloat16 panels), tcgen05 GEMM + fused epilogue"
 MODES = {
     # name: (precision, storage of A and B, f32_mode, forced path)
+    "split_bf16_f32": (0, 0, 1, 0),
     "bf16": (6, 0, 0, 0),
     "f16": (5, 0, 0, 0),
     "bf16_storage": (6, 5, 0, 0),
     "f16_storage": (5, 4, 0, 0),
-    "split_bf16_f32": (0, 0, 1, 0),
     "plain_f32": (0, 0, 0, 3),
 }
 
@@ -93,8 +98,7 @@ def dist_env():
 def cpu_reference_run(threads: int | None = None, i_slab: int = 16):
     """Times the reference's CPU product on `threads` disjoint slabs of D
     (D[:, :, 0:i_slab, t] for thread t, views into the same tensors), in
-    TAPP_F32F32_ACCUM_F32: the reference's BF16 precision does not compile
-    and its default build leaves D untouched for it. Returns a dict."""
+    TAPP_F32F32_ACCUM_F32, the precision of the headline. Returns a dict."""
     import oracle
     from tapp_b200.workloads import large_dense_case
     from tapp_b200.case import Tensor, Case
@@ -133,18 +137,23 @@ def cpu_reference_run(threads: int | None = None, i_slab: int = 16):
     wall = time.perf_counter() - t0
     assert all(e == 0 for e in errs), errs
     flops = 2.0 * (EXTENT * EXTENT * i_slab) * EXTENT ** 2 * threads
-    return {"value": flops / wall / 1e12, "unit": "TFLOP/s", "cores": threads, "kind": kind,
+    return {"value": flops / wall / 1e12, "unit": "TFLOP/s", "cores": threads, "kind": kind, "flops": flops,
             "sample": f"{threads} threads x D[:,:,0:{i_slab},t] slab ({EXTENT * EXTENT * i_slab} outputs x "
-                      f"K={EXTENT ** 2} each), F32F32_ACCUM_F32 (the reference runs no bfloat16 product); "
-                      f"{wall:.1f} s wall",
+                      f"K={EXTENT ** 2} each), F32F32_ACCUM_F32; {wall:.2f} s wall",
             "seconds": wall}
 
 
 def run_reference(args):
+    """The reference arm: the reference's own CPU product on all host
+    threads, each step one bounded slab of the workload's D (16 threads x
+    D[:,:,0:2,t]); value = the slab's flops / its wall time, ms_per_step =
+    that wall time (a time that ran). The reference's cost is linear in the
+    number of D elements (product.c:338), so the whole step's time is the
+    slab's times the ratio of flops, reported beside it."""
     rank, _, world = dist_env()
     if rank != 0:
         return
-    vals = []
+    vals, walls = [], []
     for _ in range(min(max(args.warmup, 0), 3)):
         cpu_reference_run(i_slab=1)
     info = None
@@ -152,17 +161,22 @@ def run_reference(args):
     for _ in range(max(args.steps, 1)):
         info = cpu_reference_run(i_slab=2)
         vals.append(info["value"])
+        walls.append(info["seconds"])
         total += info["seconds"]
         if total > 90.0:  # keep the whole run within a few minutes
             break
     value = statistics.median(vals)
-    line = {"metric": f"TFLOP/s ({WORKLOAD})", "value": value, "unit": "TFLOP/s", "impl": "reference",
+    slab_ms = statistics.median(walls) * 1e3
+    slab_flops = info["flops"]
+    line = {"metric": METRIC, "value": value, "unit": "TFLOP/s", "impl": "reference",
             "n_gpus": args.gpus, "steps": len(vals), "warmup": args.warmup,
-            "ms_per_step": FLOPS / (value * 1e12) * 1e3, "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": slab_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "extents": EXTENT, "M": EXTENT ** 2, "N": EXTENT ** 2,
-                       "K": EXTENT ** 2, "precision": "F32F32_ACCUM_F32 (reference has no bf16 product)",
-                       "timed": "bounded slab of D per step, extrapolated per flop"},
+                       "K": EXTENT ** 2, "precision": "F32F32_ACCUM_F32",
+                       "step": "one bounded slab of D on all host threads (the sample below)"},
+            "extrapolation": {"slab_flops": slab_flops, "full_step_flops": FLOPS,
+                              "factor": FLOPS / slab_flops, "full_step_ms_est": slab_ms * FLOPS / slab_flops},
             "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": info["cores"], "kind": info["kind"],
                              "sample": info["sample"]},
             "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -173,63 +187,74 @@ def run_reference(args):
 # GPU
 
 class ClockSampler:
-    """nvidia-smi samples of SM clock and throttle reasons (read-only)."""
-    FIELDS = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
-              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-              "clocks_event_reasons.sw_power_cap")
+    """SM clock and clock-event (throttle) reasons of one GPU, sampled by a
+    thread through NVML every `period` seconds while the block runs (read
+    only; nothing is set). summary() keeps the samples inside the timed
+    region's wall-clock window."""
+    REASONS = (("hw_slowdown", 0x8), ("sw_thermal_slowdown", 0x20), ("hw_thermal_slowdown", 0x40),
+               ("hw_power_brake_slowdown", 0x80), ("sw_power_cap", 0x4))
 
-    def __init__(self, index: int):
-        self.index = index
-        self.proc = None
+    def __init__(self, device: int, period: float = 0.001):
+        self.device = device
+        self.period = period
+        self.rows = []
+        self._stop = threading.Event()
+        self._th = None
+
+    def _handle(self, nv):
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.device).uuid)
+            if not uuid.startswith("GPU-"):
+                uuid = "GPU-" + uuid
+            return nv.nvmlDeviceGetHandleByUUID(uuid)
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.device)
+
+    def _run(self, nv, h):
+        get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        while not self._stop.is_set():
+            try:
+                self.rows.append((time.time(), float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                                  float(self.max_mhz), int(get_reasons(h))))
+            except Exception:
+                pass
+            self._stop.wait(self.period)
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-        except OSError:
-            self.proc = None
-        time.sleep(0.3)
+            import pynvml as nv
+            nv.nvmlInit()
+            h = self._handle(nv)
+            self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            self._th = threading.Thread(target=self._run, args=(nv, h), daemon=True)
+            self._th.start()
+        except Exception:
+            self._th = None
+        time.sleep(0.05)
         return self
 
     def __exit__(self, *a):
-        self.lines = []
-        if self.proc is None:
-            return
-        time.sleep(0.25)
-        self.proc.terminate()
-        try:
-            out, _ = self.proc.communicate(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-            out, _ = self.proc.communicate()
-        self.lines = [l for l in out.splitlines() if l.strip()]
+        time.sleep(0.05)
+        self._stop.set()
+        if self._th is not None:
+            self._th.join(timeout=5)
 
     def summary(self, t0=None, t1=None):
-        """Median SM clock and the throttle reasons seen in [t0, t1] (wall
-        clock); all samples when the window holds none."""
-        from datetime import datetime
-        rows = []
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for l in getattr(self, "lines", []):
-            f = [x.strip() for x in l.split(",")]
-            if len(f) < 8:
-                continue
-            try:
-                ts = datetime.strptime(f[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
-                rows.append((ts, float(f[1]), float(f[2]), f[4:8]))
-            except ValueError:
-                continue
+        """Median SM clock and the reasons seen in [t0, t1] (wall clock); all
+        samples when the window holds none."""
+        rows = list(self.rows)
         inside = [r for r in rows if t0 is not None and t0 <= r[0] <= t1]
         use = inside or rows
         reasons = set()
         for r in use:
-            for n, v in zip(names, r[3]):
-                if v.lower().startswith("active"):
-                    reasons.add(n)
+            for name, bit in self.REASONS:
+                if r[3] & bit:
+                    reasons.add(name)
         return {"sm_mhz": statistics.median([r[1] for r in use]) if use else None,
                 "sm_max_mhz": use[-1][2] if use else None, "reasons": sorted(reasons),
-                "samples": len(use), "samples_in_timed_region": len(inside)}
+                "samples": len(use), "samples_in_timed_region": len(inside), "source": "NVML"}
 
 
 def measured_peaks():
@@ -424,6 +449,80 @@ def batched_measure(lib, torch, batches=64, n=512, steps=20):
             "batched": {"tflops": flops / (t_b * 1e-3) / 1e12, "ms": t_b, "launches": l_b},
             "one_call_per_batch": {"tflops": flops / (t_s * 1e-3) / 1e12, "ms": t_s, "launches": l_s},
             "speedup": t_s / t_b}
+
+
+def small_configs_measure(lib, torch, with_cpu=True, steps=200, e2e_calls=50):
+    """The reference's own small cases, through the C ABI:
+      c1  D[a,b,c,d] = 1.3 sum_{e,f} A[a,e,b,f] B[f,c,e,d] + 0.7 C, float32,
+          F32F32_ACCUM_F32, every extent 16, dense column-major, U[-1, 1]:
+          plain CUDA-core float32 and split bfloat16;
+      c2  D[a,h,c] = alpha sum_{k,u,v} A[a,h,k,k,u] conj(B[k,h,c,v]) + beta C,
+          complex float, DEFAULT precision (Hadamard h, diagonal k, unary u and
+          v; A a view with a negative and a zero stride; D permuted against C).
+    Per call: device time with operands in HBM (CUDA events, `steps` calls)
+    and end-to-end time from pinned host buffers (synchronous calls, wall
+    clock). With with_cpu, the reference's CPU product runs the same inputs
+    (one call, one thread, best of 3) and the GPU results are compared with
+    its D: max |D_gpu - D_ref| / max |D_ref|."""
+    from tapp_b200.workloads import dense_contraction_case, mixed_classes_case
+    ref = None
+    if with_cpu:
+        import oracle
+        ref = oracle.reference_lib()
+    stream = torch.cuda.current_stream().cuda_stream
+    cases = {"c1": (dense_contraction_case(np.random.default_rng(0x7A990001), extent=16), 2.0 * 16 ** 6,
+                    [("plain_f32", 0), ("split_bf16_f32", 1)]),
+             "c2": (mixed_classes_case(np.random.default_rng(0x7A990002)), 8.0 * 40 * 36 * 24 * 12,
+                    [("default_c32", 0)])}
+    out = {}
+    for key, (case, flops, variants) in cases.items():
+        res = {"flops": flops}
+        d_ref = None
+        if ref is not None:
+            walls = []
+            for _ in range(3):
+                rc = case.copy()
+                t0 = time.perf_counter()
+                assert rc.run(ref) == 0
+                walls.append(time.perf_counter() - t0)
+            d_ref = rc.D.buf[rc.D.base + rc.D.offsets()].astype(np.complex128)
+            res["reference_cpu"] = {"ms": min(walls) * 1e3, "cores": 1, "gflops": flops / min(walls) / 1e9,
+                                    "kind": "reference"}
+        for name, f32_mode in variants:
+            dev = [to_device(t, torch) for t in (case.A, case.B, case.C, case.D)]
+            ex = make_executor(lib, stream, f32_mode=f32_mode)
+            prod = Product(lib, case, [d[1] for d in dev], ex)
+            ms = time_device(torch, prod, steps, 10, lambda: None)
+            got = dev[3][0].cpu().numpy().view(case.D.buf.dtype)
+            prod.close()
+            lib.lib.TAPP_destroy_executor(ex)
+            # from pinned host buffers, D copied back every call
+            pinned = []
+            for t in (case.A, case.B, case.C, case.D):
+                h = torch.from_numpy(t.buf.view(np.uint8).copy()).pin_memory()
+                pinned.append((h, h.data_ptr() + t.base * t.itemsize))
+            ex_h = make_executor(lib, None, f32_mode=f32_mode, async_=False)
+            prod_h = Product(lib, case, [q[1] for q in pinned], ex_h)
+            for _ in range(3):
+                prod_h()
+            t0 = time.perf_counter()
+            for _ in range(e2e_calls):
+                prod_h()
+            e2e_us = (time.perf_counter() - t0) / e2e_calls * 1e6
+            prod_h.close()
+            lib.lib.TAPP_destroy_executor(ex_h)
+            v = {"device_us": ms * 1e3, "tflops": flops / (ms * 1e-3) / 1e12, "e2e_us": e2e_us,
+                 "h2d_bytes": sum(t.buf.nbytes for t in (case.A, case.B, case.C)), "d2h_bytes": case.D.buf.nbytes}
+            if d_ref is not None:
+                # repeated steps apply beta * C to the same C, so D is the same every step
+                g = got[case.D.base + case.D.offsets()].astype(np.complex128)
+                v["max_abs_err_vs_reference_rel_to_max"] = float(np.abs(g - d_ref).max() / np.abs(d_ref).max())
+                v["speedup_vs_reference_cpu_e2e"] = res["reference_cpu"]["ms"] * 1e3 / e2e_us
+            res[name] = v
+            del dev, pinned
+        out[key] = res
+    out["c1"]["split_vs_plain_device"] = out["c1"]["plain_f32"]["device_us"] / out["c1"]["split_bf16_f32"]["device_us"]
+    return out
 
 
 def hbm_peak():
@@ -749,10 +848,11 @@ def run_b200(args):
             print(json.dumps(double_measure(lib, torch, slices, ab=args.double_ab, ij=args.double_ij)), flush=True)
         return
 
-    # ---------------- headline: BF16BF16_ACCUM_F32, operands in HBM ----------------
-    case = mode_case("bf16")
+    # ---------------- headline: float32 in split-bfloat16 mode, operands in HBM ----------------
+    case = mode_case(HEADLINE)
+    _, _, head_f32_mode, _ = MODES[HEADLINE]
     dev = [to_device(t, torch) for t in (case.A, case.B, case.C, case.D)]
-    ex = make_executor(lib, stream)
+    ex = make_executor(lib, stream, f32_mode=head_f32_mode)
     prod = Product(lib, case, [d[1] for d in dev], ex)
     n0 = lib.launches()
     window = [None, None]
@@ -764,7 +864,7 @@ def run_b200(args):
     if args.only_headline:
         if rank == 0:
             print(json.dumps({"ms_per_step": t_ms, "tflops": FLOPS / (t_ms * 1e-3) / 1e12,
-                              "gpu_launches": gpu_launches}), flush=True)
+                              "gpu_launches": gpu_launches, "clocks": clocks}), flush=True)
         prod.close()
         lib.lib.TAPP_destroy_executor(ex)
         if dist is not None:
@@ -774,7 +874,7 @@ def run_b200(args):
     value = replica_tflops(world, FLOPS, t_max * 1e-3)
 
     # ---------------- dominant kernel: GEMM duration per launch ----------------
-    ex_s = make_executor(lib, stream, async_=False, status=True)
+    ex_s = make_executor(lib, stream, f32_mode=head_f32_mode, async_=False, status=True)
     prod_s = Product(lib, case, [d[1] for d in dev], ex_s)
     mains, devs = [], []
     for i in range(min(max(args.steps, 3), 20)):
@@ -790,21 +890,23 @@ def run_b200(args):
     traffic = profiled_traffic()
     roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_source": f"{peak_kind} bf16 dense burst",
-                "kernel": "tb::tc::k_gemm", "kernel_us": main_us, "step_device_us": dev_us,
-                "flops_per_launch": FLOPS}
+                "kernel": "tb::tc::k_gemm (split bfloat16)", "kernel_us": main_us, "step_device_us": dev_us,
+                "flops_per_launch": FLOPS, "pipe_flops_per_launch": 3 * FLOPS,
+                "pipe_frac": 3 * achieved / peak, "step_frac": FLOPS / (dev_us * 1e-6) / 1e12 / peak,
+                "note": "achieved counts useful flops (2*M*N*K); the tensor pipe runs the three bfloat16 "
+                        "products hi*hi + hi*lo + lo*hi, 3x that (pipe_frac)"}
     prod_s.close()
     lib.lib.TAPP_destroy_executor(ex_s)
 
-    # ---------------- other precision modes, with binary64 error ----------------
+    # ---------------- error of the headline and the other precision modes ----------------
     modes = {}
-    ref64 = f64_slab_reference(lib, torch, case) if not args.no_modes else None
+    ref64 = f64_slab_reference(lib, torch, case)
     D_head = dev[3][0].cpu().numpy().view(np.float32)
-    if ref64 is not None:
-        err = np.abs(slab_values(case.D, D_head) - ref64)
-        modes["bf16"] = {"tflops": value / world, "max_abs_err_rel_to_max": float(err.max() / np.abs(ref64).max())}
+    head_err = float(np.abs(slab_values(case.D, D_head) - ref64).max() / np.abs(ref64).max())
+    modes[HEADLINE] = {"tflops": value / world, "ms": t_ms, "max_abs_err_rel_to_max": head_err}
     if not args.no_modes:
         for name, (prec, storage, f32_mode, path) in MODES.items():
-            if name == "bf16":
+            if name == HEADLINE:
                 continue
             mc = mode_case(name)
             mdev = [to_device(t, torch) for t in (mc.A, mc.B, mc.C, mc.D)]
@@ -827,7 +929,7 @@ def run_b200(args):
     for t in (case.A, case.B, case.C, case.D):
         h = torch.from_numpy(t.buf.view(np.uint8)).pin_memory()
         pinned.append((h, h.data_ptr() + t.base * t.itemsize))
-    ex_h = make_executor(lib, None, async_=False)
+    ex_h = make_executor(lib, None, f32_mode=head_f32_mode, async_=False)
     prod_h = Product(lib, case, [p[1] for p in pinned], ex_h)
     e2e_steps = max(3, min(args.steps, 20))
     for _ in range(2):
@@ -848,6 +950,9 @@ def run_b200(args):
     prod_h.close()
     lib.lib.TAPP_destroy_executor(ex_h)
 
+    small = small_configs_measure(lib, torch, with_cpu=(rank == 0 and not args.no_cpu)) \
+        if world == 1 and not args.no_modes else None
+
     served = None
     if world == 1 and args.served > 0:
         served = served_measure(lib, torch, args.served)
@@ -862,20 +967,25 @@ def run_b200(args):
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_reference_run()
         cpu.pop("seconds", None)
+        cpu.pop("flops", None)
 
     if rank == 0:
-        line = {"metric": f"TFLOP/s ({WORKLOAD}, BF16BF16_ACCUM_F32)", "value": value, "unit": "TFLOP/s",
+        line = {"metric": METRIC, "value": value, "unit": "TFLOP/s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16",
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic",
                 "config": {"workload": WORKLOAD, "extents": EXTENT, "M": EXTENT ** 2, "N": EXTENT ** 2,
-                           "K": EXTENT ** 2, "storage": "f32 A,B,C,D", "precision": "BF16BF16_ACCUM_F32",
+                           "K": EXTENT ** 2, "storage": "f32 A,B,C,D", "precision": "F32F32_ACCUM_F32",
+                           "f32_mode": "split bfloat16 (TAPP_B200_ATTR_F32_MODE = 1)",
                            "parallelism": f"replicas x{world}",
                            "l2": "inputs 256 MiB > 126 MB L2 (A,B,C,D 64 MiB each)",
-                           "step": "pack A, pack B, tcgen05 GEMM + fused epilogue"},
+                           "step": STEP_DESCRIPTION},
+                "max_abs_err_rel_to_max": head_err,
+                "error_reference": "binary64 evaluation of D[:,:,:,0:2] from the same stored inputs",
                 "vs_plain_gpu": (value / world / plain) if plain else None,
-                "modes": modes, "batched": batched, "tucker_chain": chain, "tucker": tucker, "double": double, "served": served, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu,
-                "clocks": clocks, "gpu_launches": gpu_launches}
+                "modes": modes, "small_configs": small, "batched": batched, "tucker_chain": chain,
+                "tucker": tucker, "double": double, "served": served, "roofline": roofline, "e2e": e2e,
+                "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": gpu_launches}
         print(json.dumps(line), flush=True)
     prod.close()
     lib.lib.TAPP_destroy_executor(ex)
