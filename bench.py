@@ -50,7 +50,7 @@ FLOPS = 2.0 * (EXTENT ** 2) ** 3          # 2 * M * N * K
 WORKLOAD = "dense_4index_contraction_64^4"
 METRIC = f"TFLOP/s ({WORKLOAD}, F32)"     # the same string on both arms
 HEADLINE = "split_bf16_f32"
-STEP_DESCRIPTION = "pack A, pack B (hi/lo bfloat16 panels), tcgen05 GEMM + fused epilogue"
+STEP_DESCRIPTION = "one tcgen05 GEMM launch: converter warps split A and B into bfloat16 hi/lo in shared memory (read in place), fused epilogue"
 MODES = {
     # name: (precision, storage of A and B, f32_mode, forced path)
     "split_bf16_f32": (0, 0, 1, 0),

@@ -399,6 +399,27 @@ struct EpiParams {
     int64_t Lper;
 };
 
+// An operand the split-bfloat16 GEMM reads in place from binary32 storage:
+// index -> element offset maps of its row (M or N), contracted and batch
+// modes (at most 4 each, indices below 2^31), and its major side: mn = 1
+// when its contiguous mode (stride 1, extent a multiple of 8) is a row mode,
+// 0 when it is a contracted mode. Every other stride is a multiple of 4 and
+// the base is 16-byte aligned, so each run of 8 elements along the
+// contiguous mode is two 16-byte loads.
+struct CvtDim {
+    int32_t n;
+    uint32_t size;
+    FastDiv div[4];
+    int64_t st[4];
+};
+struct CvtOperand {
+    const float* base;
+    const void* const* bases;  // batched product: base of batch b = l / lper, else NULL
+    int64_t lper;              // batch modes per batch
+    int32_t mn, pad;
+    CvtDim rows, ks, ls;
+};
+
 struct GemmParams {
     int32_t tiles_m, tiles_n, num_tiles, num_kb;
     EpiParams e;
@@ -428,6 +449,8 @@ struct GemmParams {
     // logical dims present in each direct operand's map (bit j: dim j; dims
     // of extent 1 are left out, fewer dims copy faster)
     int32_t a_dims, b_dims;
+    // split-bfloat16 GEMM reading binary32 operands in place (k_gemm<.., CVT>)
+    CvtOperand ca, cb;
 };
 
 // work item it of the persistent schedule: tile, contraction-block range and
@@ -489,16 +512,34 @@ __device__ __forceinline__ unsigned long long now_ns()
     return t;
 }
 
+// try_wait with cluster-scope acquire: for a barrier that threads of the
+// other CTA of a pair arrive on (release, cluster scope) after writing
+// shared memory that this thread's MMAs then read
+__device__ __forceinline__ bool mbar_try_cluster(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
 // Waits for the phase of `parity` to complete; gives up after limit_ns (4 s
 // in the kernels; or at once when another role already gave up), raises
 // *abort_flag and returns false.
+template <bool CLUSTER = false>
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
                                           unsigned long long limit_ns = WAIT_NS)
 {
-    if (mbar_try(bar, parity)) return true;
+    auto try_ = [&] { return CLUSTER ? mbar_try_cluster(bar, parity) : mbar_try(bar, parity); };
+    if (try_()) return true;
     const unsigned long long t0 = now_ns();
     for (uint32_t i = 1;; i++) {
-        if (mbar_try(bar, parity)) return true;
+        if (try_()) return true;
         if ((i & 255) == 0) {
             if (*abort_flag) return false;
             if (now_ns() - t0 > limit_ns) {
@@ -744,7 +785,8 @@ __device__ __forceinline__ float ld_nc_f32(const float* p)
     return v;
 }
 
-__device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, %0;" ::"n"(EPI_THREADS) : "memory"); }
+template <int N>
+__device__ __forceinline__ void epi_bar_n() { asm volatile("bar.sync 1, %0;" ::"n"(N) : "memory"); }
 
 // beta * op_C(C) for one output (0 when beta == 0)
 __device__ __forceinline__ void load_beta_c(const EpiParams& e, const void* Cbase, int64_t offC, float& br, float& bi)
@@ -778,6 +820,132 @@ __device__ __forceinline__ void finish_out(const EpiParams& e, void* Dbase, int6
     store_elem<float>(Dbase, offD, e.tD, accr, acci);
 }
 
+// ---------------------------------------------------------------------------
+// In-place split-bfloat16 operands (k_gemm<.., CVT = true>): eight converter
+// warps per CTA load the binary32 tiles of A and B with 16-byte loads,
+// split every value into hi = bf16(x) and lo = bf16(x - hi), and store both
+// in the swizzled layouts the MMAs read (K-major or MN-major, 128-byte
+// swizzle). Per CTA and 64-deep contraction block a converter thread owns 4
+// units of 8 consecutive elements of each operand:
+//   K-major (contiguous along k): rows hi2 + 4 cw + 32 j (j < 4), the k run
+//     8 lo3 .. 8 lo3 + 7; the 8 lanes of a row store one whole 128-byte row
+//   MN-major (contiguous along rows): rows 64 h + 8 lo3 .. + 7 (h < 2) at
+//     k = hi2 + 4 cw + 32 jk (jk < 2); 8 lanes store one 128-byte k-line
+// (cw the converter warp, lo3 = lane % 8, hi2 = lane / 8), so every store
+// of a warp covers whole 128-byte lines (no bank conflicts) and every 8
+// lanes read 256 contiguous bytes.
+__device__ __forceinline__ int64_t cvt_decode(const CvtDim& d, uint32_t idx)
+{
+    int64_t off = 0;
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        if (j + 1 >= d.n) break;
+        const uint32_t q = fdiv(idx, d.div[j]);
+        off += (int64_t)(idx - q * d.div[j].d) * d.st[j];
+        idx = q;
+    }
+    return d.n ? off + (int64_t)idx * d.st[d.n - 1] : 0;
+}
+
+// element offsets of this thread's unit rows for one tile (-1: past the
+// end); returns the tile's operand base (its batch's, in a batched product)
+__device__ __forceinline__ const float* cvt_rows(const CvtOperand& o, int64_t row0, int64_t l, int cw, int lo3,
+                                                 int hi2, int64_t (&roff)[4])
+{
+    const float* base = o.base;
+    if (o.bases) {
+        base = (const float*)o.bases[l / o.lper];
+        l %= o.lper;
+    }
+    const int64_t loff = cvt_decode(o.ls, (uint32_t)l);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        int64_t r;
+        if (o.mn) r = j < 2 ? row0 + 64 * j + 8 * lo3 : -1;
+        else r = row0 + hi2 + 4 * cw + 32 * j;
+        roff[j] = (r >= 0 && r < (int64_t)o.rows.size) ? loff + cvt_decode(o.rows, (uint32_t)r) : -1;
+    }
+    return base;
+}
+
+__device__ __forceinline__ float4 ld_nc_v4(const float* p)
+{
+    float4 v;
+    asm volatile("ld.global.nc.L1::no_allocate.v4.f32 {%0,%1,%2,%3}, [%4];"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+                 : "l"(p));
+    return v;
+}
+
+// the 4 units of contraction block kb into x (zeros past the tensor's end)
+__device__ __forceinline__ void cvt_load(const CvtOperand& o, const float* base, const int64_t (&roff)[4], int kb,
+                                         int cw, int lo3, int hi2, float (&x)[32])
+{
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+        int64_t ro;
+        uint32_t k;
+        if (o.mn) {
+            ro = roff[u & 1];
+            k = (uint32_t)kb * 64 + hi2 + 4 * cw + 32 * (u >> 1);
+        } else {
+            ro = roff[u];
+            k = (uint32_t)kb * 64 + 8 * lo3;
+        }
+        float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
+        if (ro >= 0 && k < o.ks.size) {
+            const float* q = base + ro + cvt_decode(o.ks, k);
+            a = ld_nc_v4(q);
+            b = ld_nc_v4(q + 4);
+        }
+        x[8 * u + 0] = a.x; x[8 * u + 1] = a.y; x[8 * u + 2] = a.z; x[8 * u + 3] = a.w;
+        x[8 * u + 4] = b.x; x[8 * u + 5] = b.y; x[8 * u + 6] = b.z; x[8 * u + 7] = b.w;
+    }
+}
+
+// hi = bf16(x), lo = bf16(x - hi) of 8 values as two 16-byte vectors
+__device__ __forceinline__ void split8(const float* x, uint4& hi, uint4& lo)
+{
+    uint32_t h[4], w[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        __nv_bfloat162 q = __floats2bfloat162_rn(x[2 * i], x[2 * i + 1]);
+        h[i] = *(uint32_t*)&q;
+        const float a = __uint_as_float(h[i] << 16), b = __uint_as_float(h[i] & 0xffff0000u);
+        __nv_bfloat162 r = __floats2bfloat162_rn(x[2 * i] - a, x[2 * i + 1] - b);
+        w[i] = *(uint32_t*)&r;
+    }
+    hi = make_uint4(h[0], h[1], h[2], h[3]);
+    lo = make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+__device__ __forceinline__ void st_shared_v4(uint32_t addr, const uint4& v)
+{
+    asm volatile("st.shared.v4.b32 [%0], {%1,%2,%3,%4};" ::"r"(addr), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w)
+                 : "memory");
+}
+
+// stores the split units into the hi and lo tiles (128 x 64 each, 16 KiB)
+__device__ __forceinline__ void cvt_store(const CvtOperand& o, const float (&x)[32], uint32_t hi_tile,
+                                          uint32_t lo_tile, int cw, int lo3, int hi2)
+{
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+        uint32_t off;
+        if (o.mn) {
+            const int k = hi2 + 4 * cw + 32 * (u >> 1), h = u & 1;
+            off = h * 8192 + (k >> 3) * 1024 + (k & 7) * 128 + ((lo3 ^ (k & 7)) << 4);
+        } else {
+            const int r = hi2 + 4 * cw + 32 * u;
+            off = r * 128 + ((lo3 ^ (r & 7)) << 4);
+        }
+        uint4 hi, lo;
+        split8(&x[8 * u], hi, lo);
+        st_shared_v4(hi_tile + off, hi);
+        st_shared_v4(lo_tile + off, lo);
+    }
+}
+
 // EPI_F32: real product, C and D binary32 (the common case, specialised);
 // EPI_ANY: every storage type, complex outputs, op_C / op_D.
 // EPI_TMA: like EPI_F32, with C and D moved by TMA tensor copies through a
@@ -786,13 +954,23 @@ __device__ __forceinline__ void finish_out(const EpiParams& e, void* Dbase, int6
 // 32-bit integer accumulators added into a binary64 workspace.
 enum { EPI_ANY = 0, EPI_F32 = 1, EPI_TMA = 2, EPI_I32 = 3 };
 
-template <int EPI, bool CTA2>
-__global__ void __launch_bounds__(NTHREADS, 1)
+// CVT: the split-bfloat16 product of binary32 operands read in place by
+// eight converter warps (warps 8-15, 512 threads) instead of TMA loads of
+// packed panels; stages of 64 KiB (A hi, A lo, B hi, B lo), three MMAs per
+// 16-deep step (hi*hi, hi*lo, lo*hi), four epilogue warps (4-7).
+template <int EPI, bool CTA2, bool CVT = false>
+__global__ void __launch_bounds__(CVT ? 512 : NTHREADS, 1)
     k_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, GemmParams p,
            uint32_t idesc, const __grid_constant__ CUtensorMap tmC, const __grid_constant__ CUtensorMap tmD)
 {
     using G = Geo<CTA2>;
-    constexpr int NS = G::stages;
+    constexpr int NS = CVT ? 3 : G::stages;
+    constexpr int SB = CVT ? 4 * BM * BK * 2 : G::stage_bytes;  // bytes per stage
+    constexpr int EW = CVT ? 4 : EPI_WARPS;                      // epilogue warps
+    constexpr int ET = EW * 32;
+    constexpr int CS = EW / 4;  // a warp's chunk step: the warps of a lane quarter interleave
+    static_assert(!CVT || (CTA2 && NS * SB <= STAGES * STAGE_BYTES), "split stages fit the ring");
+    auto epi_bar = [] { epi_bar_n<ET>(); };
     constexpr int KSTEP = EPI == EPI_I32 ? 2 * BK : BK;  // elements per 128-byte stage row
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     // 1024-byte alignment by pointer arithmetic on the shared array (an
@@ -817,16 +995,17 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     const uint32_t rank = CTA2 ? cluster_rank() : 0;  // 0 = the pair's leader, which issues the MMAs
     if (threadIdx.x == 0) {
         for (int s = 0; s < NS; s++) {
-            mbar_init(&full[s], 1);
+            // CVT: one arrival per converter warp (of both CTAs of a pair)
+            mbar_init(&full[s], CVT ? (CTA2 ? 16 : 8) : 1);
             mbar_init(&empty[s], 1);
         }
         for (int a = 0; a < 2; a++) {
             mbar_init(&tfull[a], 1);
             // one CTA: every epilogue thread arrives; pair: one arrival per
             // epilogue warp of either CTA, on the leader's barrier
-            mbar_init(&tempty[a], CTA2 ? 2 * EPI_WARPS : EPI_THREADS);
+            mbar_init(&tempty[a], CTA2 ? 2 * EW : ET);
         }
-        for (int w = 0; w < EPI_WARPS; w++) mbar_init(&cbar[w], 1);
+        for (int w = 0; w < EW; w++) mbar_init(&cbar[w], 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -858,7 +1037,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     // overlap; a box that lands before the expectation only drives the
     // barrier's transaction count below zero for a moment
     const bool two_producers = p.a_direct || p.b_direct;
-    if (warp == 0 || (warp == 3 && two_producers)) {
+    if (!CVT && (warp == 0 || (warp == 3 && two_producers))) {
         // ---------------- TMA producer ----------------
         if (lane == 0) {
             const bool do_a = warp == 0, do_b = warp == 3 || !two_producers;
@@ -1005,13 +1184,23 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                     const int kr = kb - it.kb0;  // accumulate from the item's second block on
                     const int s = g % NS;
                     const uint32_t ph = (g / NS) & 1;
-                    if (!mbar_wait(&full[s], ph, abort_flag)) { ok = false; break; }
+                    if (!mbar_wait<CVT && CTA2>(&full[s], ph, abort_flag)) { ok = false; break; }
                     fence_after();
-                    const uint32_t a = smem_u32(tiles + s * G::stage_bytes);
+                    const uint32_t a = smem_u32(tiles + s * SB);
                     const uint32_t b = a + G::a_bytes;
 #pragma unroll
                     for (int k = 0; k < BK / 16; k++) {  // 32 bytes of K per instruction
-                        if (EPI != EPI_I32 && (p.a_mn | p.b_mn)) {
+                        if (CVT) {
+                            // A hi, A lo, B hi, B lo tiles of 16 KiB: hi*hi + hi*lo + lo*hi
+                            auto desc = [&](uint32_t t, int mn) {
+                                return mn ? smem_desc_mn(t + k * 2048) : smem_desc(t + k * 32);
+                            };
+                            const uint64_t ah = desc(a, p.a_mn), al = desc(a + 16384, p.a_mn);
+                            const uint64_t bh = desc(a + 32768, p.b_mn), bl = desc(a + 49152, p.b_mn);
+                            mma_f16_pair(d_tmem, ah, bh, idesc, (kr | k) != 0);
+                            mma_f16_pair(d_tmem, ah, bl, idesc, 1);
+                            mma_f16_pair(d_tmem, al, bh, idesc, 1);
+                        } else if (EPI != EPI_I32 && (p.a_mn | p.b_mn)) {
                             // an MN-major operand advances 16 k-rows (2048 bytes) per instruction
                             const uint64_t da = p.a_mn ? smem_desc_mn(a + k * 2048) : smem_desc(a + k * 32);
                             const uint64_t db = p.b_mn ? smem_desc_mn(b + k * 2048) : smem_desc(b + k * 32);
@@ -1040,7 +1229,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                 mbar_wait(&empty[last % NS], (last / NS) & 1, &never);
             }
         }
-    } else if (warp >= 4) {
+    } else if (warp >= 4 && warp < 4 + EW) {
         // ---------------- epilogue ----------------
         // Warp w drains TMEM lanes 32*(w%4)..+31 (its lane quarter); the two
         // warps of a quarter take alternate 32-column chunks. For each chunk
@@ -1049,7 +1238,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         const EpiParams& e = p.e;
         const int q = warp & 3;
         const int half = (warp - 4) >> 2;        // 0 or 1: which chunks
-        const int et = threadIdx.x - 128;        // 0 .. EPI_THREADS-1
+        const int et = threadIdx.x - 128;        // 0 .. ET-1
         const int cols_out = e.cplx ? BN / 2 : BN;
         uint32_t epi_cphase = 0;  // completed phases of this warp's C-box barrier
         // the accumulator buffer is free again once every epilogue thread has
@@ -1072,7 +1261,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             const int64_t row0 = (int64_t)tm * G::tile_m + (int64_t)rank * BM;  // this CTA's first row
             // column offsets of this tile (the TMA epilogue needs none: its
             // staging boxes share this memory)
-            for (int c = et; EPI != EPI_TMA && EPI != EPI_I32 && c < cols_out; c += EPI_THREADS) {
+            for (int c = et; EPI != EPI_TMA && EPI != EPI_I32 && c < cols_out; c += ET) {
                 const int64_t n = (int64_t)tn * cols_out + c;
                 int64_t oc = 0, od = 0;
                 if (n < e.N) decode2(e.nn, n, oc, od);
@@ -1114,8 +1303,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                 fence_after();
                 if (ok0 && first) {
 #pragma unroll 1
-                    for (int t = 0; t < BN / 64; t++) {
-                        const int ch = half + 2 * t;
+                    for (int t = 0; t < BN / 32 / CS; t++) {
+                        const int ch = half + CS * t;
                         uint32_t r[32];
                         tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + acc * BN + ch * 32, r);
 #pragma unroll
@@ -1190,18 +1379,17 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                     for (int j = 0; j < e.ll.n; j++) cc[k++] = lc[j];
                     while (k < 5) cc[k++] = 0;
                 };
-                const int nch = BN / 64;  // chunks per warp
-                int cc[BN / 64][5];       // tensor-map coordinates of this warp's chunks
-#pragma unroll
-                for (int t = 0; t < nch; t++) coords(half + 2 * t, cc[t]);
+                const int nch = BN / 32 / CS;  // chunks per warp
                 const float alpha = e.alpha_re, beta = e.beta_re;
                 const int rmode = e.round_C;
                 const bool bzero = e.beta_zero != 0;
                 bool ok = true;
                 auto issue_c = [&](int t) {
                     if (lane == 0 && !bzero) {
+                        int cc[5];
+                        coords(half + CS * t, cc);
                         mbar_expect_tx(&cbar[ew], STAGE_EPI_BYTES);
-                        tma_load_5d(box, mapC, &cbar[ew], cc[t]);
+                        tma_load_5d(box, mapC, &cbar[ew], cc);
                     }
                 };
                 issue_c(0);
@@ -1215,7 +1403,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                 fence_after();
 #pragma unroll 1
                 for (int t = 0; t < nch; t++) {
-                    const int ch = half + 2 * t;
+                    const int ch = half + CS * t;
                     uint32_t r[32];
                     if (ok) tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + acc * BN + ch * 32, r);
                     if (ok && add_part) {
@@ -1240,7 +1428,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                     }
                     __syncwarp();
                     if (lane == 0 && ok && cok) {
-                        tma_store_5d(mapD, box, cc[t]);
+                        int cc[5];
+                        coords(ch, cc);
+                        tma_store_5d(mapD, box, cc);
                         asm volatile("cp.async.bulk.commit_group;" ::: "memory");
                         // the box is reused by the next load: wait until the store has read it
                         asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
@@ -1267,8 +1457,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                     double* wrow = e.W + ((int64_t)l * e.M + m) * e.N;
                     const bool pairs = (e.N & 1) == 0;
 #pragma unroll 1
-                    for (int t = 0; t < BN / 64; t++) {
-                        const int ch = half + 2 * t;
+                    for (int t = 0; t < BN / 32 / CS; t++) {
+                        const int ch = half + CS * t;
                         uint32_t r[32];
                         __syncwarp();
                         tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + acc * BN + ch * 32, r);
@@ -1320,6 +1510,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                     }
                 };
                 fetch(half, buf[0]);
+                constexpr int NCH = BN / 32 / CS;
                 bool ok = pre_ok;
                 if (!pre) {
                     if (et == 0) *epi_ok = mbar_wait(&tfull[acc], aph, abort_flag) ? 1 : 0;
@@ -1329,9 +1520,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                 fence_after();
                 if (ok) {
 #pragma unroll
-                    for (int t = 0; t < BN / 64; t++) {
-                        const int ch = half + 2 * t;
-                        if (t + 1 < BN / 64) fetch(ch + 2, buf[(t + 1) & 1]);
+                    for (int t = 0; t < NCH; t++) {
+                        const int ch = half + CS * t;
+                        if (t + 1 < NCH) fetch(ch + CS, buf[(t + 1) & 1]);
                         uint32_t r[32];
                         tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + acc * BN + ch * 32, r);
                         if (add_part) {
@@ -1359,7 +1550,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             const bool ok = *epi_ok != 0;
             fence_after();
             if (ok) {
-                for (int ch = half; ch < BN / 32; ch += 2) {
+                for (int ch = half; ch < BN / 32; ch += CS) {
                     const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + acc * BN + ch * 32;
                     if (!e.cplx) {
                         float br[32], bi[32];
@@ -1404,6 +1595,47 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         // no early exit above: every epilogue thread takes every tile's barriers,
         // and after an expired wait the remaining waits give up at once
         if (EPI == EPI_TMA && lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+    } else if (CVT && warp >= 8) {
+        // ---------------- converters: binary32 tiles -> bfloat16 hi / lo ----------------
+        // Every wait is bounded; a converter that gives up stops converting,
+        // and the MMA issuer's next wait on the stage it would have filled
+        // gives up too.
+        const int cw = warp - 8, lo3 = lane & 7, hi2 = lane >> 3;
+        uint32_t g = 0;
+        bool ok = true;
+        for (int i = 0; i < my_tiles && ok; i++) {
+            const Item it = item_of(p, unit + i * units);
+            const int tile = it.tile;
+            const int tm = tile % p.tiles_m;
+            const int rest = tile / p.tiles_m;
+            const int tn = rest % p.tiles_n;
+            const int l = rest / p.tiles_n;
+            int64_t ra_off[4], rb_off[4];
+            const float* abase = cvt_rows(p.ca, (int64_t)tm * G::tile_m + (int64_t)rank * BM, l, cw, lo3, hi2, ra_off);
+            const float* bbase = cvt_rows(p.cb, (int64_t)tn * BN + (int64_t)rank * G::b_rows, l, cw, lo3, hi2, rb_off);
+            float xa[32], xb[32];
+            cvt_load(p.ca, abase, ra_off, it.kb0, cw, lo3, hi2, xa);
+            cvt_load(p.cb, bbase, rb_off, it.kb0, cw, lo3, hi2, xb);
+            for (int kb = it.kb0; kb < it.kb1; kb++, g++) {
+                const int s = g % NS;
+                const uint32_t ph = (g / NS) & 1;
+                if (!mbar_wait(&empty[s], ph ^ 1, abort_flag)) { ok = false; break; }
+                const uint32_t st = smem_u32(tiles + s * SB);
+                // each operand's next block is requested as soon as its
+                // registers are free, so the loads run under the other's stores
+                cvt_store(p.ca, xa, st, st + 16384, cw, lo3, hi2);
+                if (kb + 1 < it.kb1) cvt_load(p.ca, abase, ra_off, kb + 1, cw, lo3, hi2, xa);
+                cvt_store(p.cb, xb, st + 32768, st + 49152, cw, lo3, hi2);
+                if (kb + 1 < it.kb1) cvt_load(p.cb, bbase, rb_off, kb + 1, cw, lo3, hi2, xb);
+                // generic-proxy stores -> the MMAs' async-proxy reads
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                __syncwarp();
+                if (lane == 0) {
+                    if (CTA2) mbar_arrive_cluster(cluster_addr(&full[s], 0));
+                    else mbar_arrive(&full[s]);
+                }
+            }
+        }
     }
     fence_before();
     if (CTA2) cluster_sync();  // the leader's MMAs into this CTA's TMEM, and remote signals, are done
@@ -1539,28 +1771,32 @@ struct Workspace {
 
 // Launches the GEMM: 1-CTA (128x256 tiles) or CTA pairs (256x256 tiles,
 // cluster of 2, cta_group::2) when M spans at least two 128-row halves.
+// cvt: the split-bfloat16 GEMM converting binary32 operands in place (pairs only).
 static cudaError_t launch_gemm(int kind, bool cta2, int grid, const CUtensorMap& tmA, const CUtensorMap& tmB,
                                const GemmParams& gp, uint32_t idesc, const CUtensorMap& tmC, const CUtensorMap& tmD,
-                               cudaStream_t s)
+                               cudaStream_t s, bool cvt = false)
 {
     void (*kern)(CUtensorMap, CUtensorMap, GemmParams, uint32_t, CUtensorMap, CUtensorMap);
-    if (cta2)
+    if (cvt)
+        kern = kind == EPI_TMA ? k_gemm<EPI_TMA, true, true> : kind == EPI_F32 ? k_gemm<EPI_F32, true, true>
+               : k_gemm<EPI_ANY, true, true>;
+    else if (cta2)
         kern = kind == EPI_TMA ? k_gemm<EPI_TMA, true> : kind == EPI_F32 ? k_gemm<EPI_F32, true>
                : kind == EPI_I32 ? k_gemm<EPI_I32, true> : k_gemm<EPI_ANY, true>;
     else
         kern = kind == EPI_TMA ? k_gemm<EPI_TMA, false> : kind == EPI_F32 ? k_gemm<EPI_F32, false>
                : kind == EPI_I32 ? k_gemm<EPI_I32, false> : k_gemm<EPI_ANY, false>;
-    static int attr_done[64][4][2];
+    static int attr_done[64][4][2][2];
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev < 0 || dev >= 64 || !attr_done[dev][kind][cta2]) {
+    if (dev < 0 || dev >= 64 || !attr_done[dev][kind][cta2][cvt]) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
         if (e != cudaSuccess) return e;
-        if (dev >= 0 && dev < 64) attr_done[dev][kind][cta2] = 1;
+        if (dev >= 0 && dev < 64) attr_done[dev][kind][cta2][cvt] = 1;
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)grid, 1, 1);
-    cfg.blockDim = dim3(NTHREADS, 1, 1);
+    cfg.blockDim = dim3(cvt ? 512 : NTHREADS, 1, 1);
     cfg.dynamicSmemBytes = SMEM_BYTES;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
@@ -1744,8 +1980,118 @@ static int64_t group_batches(int64_t num, size_t per_batch, int64_t Lsz, int64_t
     return G < 1 ? 1 : G;
 }
 
+// Index map of a mode list for the in-place converters (at most 4 modes,
+// every index below 2^31).
+static bool make_cvt_dim(tc::CvtDim* o, const tb_modes& m, int side)
+{
+    if (m.n > 4 || m.size >= (1ll << 31)) return false;
+    memset(o, 0, sizeof(*o));
+    o->n = m.n;
+    o->size = (uint32_t)m.size;
+    for (int j = 0; j < m.n; j++) {
+        o->div[j] = make_fastdiv((uint32_t)m.ext[j]);
+        o->st[j] = side == 0 ? m.sA[j] : m.sB[j];
+    }
+    return true;
+}
+
+// Whether operand `side` (0 A, 1 B) of a split-bfloat16 product can be read
+// in place by the converter warps, and its description if so: binary32
+// storage, no unary modes, at most 4 row, contracted and batch modes, its
+// contiguous mode first in its row or contracted list with stride 1 and an
+// extent divisible by 8, every other stride divisible by 4, base 16-byte
+// aligned.
+static bool make_cvt_operand(tc::CvtOperand* o, const tb_plan* P, int side, const void* base)
+{
+    using namespace tc;
+    const tb_modes& R = side == 0 ? P->M : P->N;
+    const tb_modes& U = side == 0 ? P->UA : P->UB;
+    if ((side == 0 ? P->tA : P->tB) != T_F32 || U.n != 0 || !base || ((uintptr_t)base & 15) || R.n < 1 ||
+        P->K.n < 1)
+        return false;
+    memset(o, 0, sizeof(*o));
+    if (!make_cvt_dim(&o->rows, R, side) || !make_cvt_dim(&o->ks, P->K, side) || !make_cvt_dim(&o->ls, P->L, side))
+        return false;
+    o->mn = min_stride(R, side) < min_stride(P->K, side);
+    const CvtDim& fast = o->mn ? o->rows : o->ks;
+    if (fast.st[0] != 1 || fast.div[0].d % 8 != 0) return false;
+    const CvtDim* all[3] = {&o->rows, &o->ks, &o->ls};
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < all[i]->n; j++)
+            if (!(all[i] == &fast && j == 0) && all[i]->st[j] % 4 != 0) return false;
+    o->base = (const float*)base;
+    return true;
+}
+
+// Whether a split-bfloat16 product runs on the converter warps with A and B
+// read in place (CTA pairs: at least 256 rows of A), and their descriptions.
+static bool split_in_place(const tb_plan* P, const void* A, const void* B, tc::CvtOperand* ca, tc::CvtOperand* cb)
+{
+    return P->path == TB_PATH_TC && P->tc_mode == TB_TC_SPLIT_BF16 && P->compute == TB_R32 &&
+           P->M.size >= 2 * tc::BM && tc::num_sms() % 2 == 0 && make_cvt_operand(ca, P, 0, A) &&
+           make_cvt_operand(cb, P, 1, B);
+}
+
+// Epilogue parameters of one product (or one group of a batched product,
+// Lg = batches x batch modes) for C and D with their own strides.
+static void fill_epilogue(tc::EpiParams& ep, const tb_plan* P, const void* C, void* D, int64_t Lg)
+{
+    using namespace tc;
+    ep.C = C;
+    ep.D = D;
+    ep.tC = P->tC;
+    ep.tD = P->tD;
+    ep.cplx = P->compute == TB_C32;
+    ep.beta_zero = P->beta_zero;
+    ep.conjC = P->conjC;
+    ep.conjD = P->conjD;
+    ep.conjD_f32 = P->conjD_round_f32;
+    ep.round_C = P->round_in;
+    ep.alpha_re = (float)P->alpha_re;
+    ep.alpha_im = (float)P->alpha_im;
+    ep.beta_re = (float)P->beta_re;
+    ep.beta_im = (float)P->beta_im;
+    ep.M = P->M.size;
+    ep.N = P->N.size;
+    ep.L = Lg;
+    fill_modes(ep.mm, P->M, 2, 3);
+    fill_modes(ep.nn, P->N, 2, 3);
+    fill_modes(ep.ll, P->L, 2, 3);
+}
+
+// A last round that fills at most half the units runs its tiles as two
+// half-contraction items each (partial sums handed over in memory).
+static void plan_split_round(tc::GemmParams& gp, int kind, int units, void** split_ws, cudaStream_t s)
+{
+    using namespace tc;
+    *split_ws = nullptr;
+    if (!((kind == EPI_TMA || kind == EPI_F32) && gp.num_tiles > units && gp.num_kb >= 2)) return;
+    const int r = gp.num_tiles % units;
+    if (r == 0 || 2 * r > units) return;
+    const size_t pbytes = (size_t)r * 2 * BN * BM * sizeof(float);
+    const size_t fbytes = (size_t)r * 2 * 2 * sizeof(int);
+    if (pool_alloc(split_ws, pbytes + fbytes, s) == cudaSuccess &&
+        cudaMemsetAsync((char*)*split_ws + pbytes, 0, fbytes, s) == cudaSuccess) {
+        gp.split_tiles = r;
+        gp.partial = (float*)*split_ws;
+        gp.pcount = (int*)((char*)*split_ws + pbytes);
+        gp.pready = gp.pcount + r * 2;
+    } else if (*split_ws) {
+        cudaFreeAsync(*split_ws, s);
+        *split_ws = nullptr;
+    }
+    (void)cudaGetLastError();
+}
+
 cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t s, int* kernels, void** main_timer)
 {
+    // split-bfloat16 products whose binary32 operands the converter warps
+    // read in place (every batch's A and B 16-byte aligned): no pack
+    // launches, no panels
+    tc::CvtOperand cva, cvb;
+    bool cvt = split_in_place(P, d[0].A, d[0].B, &cva, &cvb);
+    for (int b = 1; b < num && cvt; b++)
+        if (((uintptr_t)d[b].A & 15) || ((uintptr_t)d[b].B & 15)) cvt = false;
     using namespace tc;
     *kernels = 0;
     const int cplx = P->compute == TB_C32;
@@ -1756,7 +2102,7 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
     const int64_t Kseg = round_up(Kreal, 8);
     const int64_t Kld = Kseg * split;
     const int64_t Nout = N * (cplx ? 2 : 1);
-    const size_t bytesA = (size_t)Lsz * M * Kld * 2, bytesB = (size_t)Lsz * Nout * Kld * 2;
+    const size_t bytesA = cvt ? 0 : (size_t)Lsz * M * Kld * 2, bytesB = cvt ? 0 : (size_t)Lsz * Nout * Kld * 2;
     const bool cta2 = M >= 2 * BM && num_sms() % 2 == 0;
     const int64_t tiles_per_batch = ((M + (cta2 ? 2 * BM : BM) - 1) / (cta2 ? 2 * BM : BM)) * ((Nout + BN - 1) / BN) * Lsz;
     // A batched product runs in groups of G batches: one pack launch per
@@ -1767,11 +2113,12 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
     const size_t scratch = round_up((int64_t)(bytesA * G), 256) + round_up((int64_t)(bytesB * G), 256);
 
     void* ws = nullptr;
-    cudaError_t e = pool_alloc(&ws, scratch, s);  // reused by every group: same stream, in order
+    cudaError_t e = cudaSuccess;
+    if (scratch) e = pool_alloc(&ws, scratch, s);  // reused by every group: same stream, in order
     if (e != cudaSuccess) return e;
     int* flag = device_error_word();
     if (!flag) {
-        cudaFreeAsync(ws, s);
+        if (ws) cudaFreeAsync(ws, s);
         return cudaErrorMemoryAllocation;
     }
     const void** dptr = nullptr;  // device copy of [A...][B...][C...][D...]
@@ -1782,7 +2129,7 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
         const size_t pbytes = sizeof(void*) * 4 * (size_t)num;
         const void** host = (const void**)malloc(pbytes);
         if (!host) {
-            cudaFreeAsync(ws, s);
+            if (ws) cudaFreeAsync(ws, s);
             return cudaErrorMemoryAllocation;
         }
         for (int b = 0; b < num; b++) {
@@ -1806,7 +2153,7 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
         }
         if (e != cudaSuccess) {
             if (dptr) cudaFreeAsync(dptr, s);
-            cudaFreeAsync(ws, s);
+            if (ws) cudaFreeAsync(ws, s);
             return e;
         }
     }
@@ -1821,7 +2168,8 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
         // describe one batch's tensors)
         CUtensorMap dmap[2];
         int dir[2] = {0, 0}, dmn[2] = {0, 0}, de0[2] = {0, 0}, dk0[2] = {0, 0}, dbox[2] = {0, 0}, dmask[2] = {0, 0};
-        if (G == 1 && split == 1)
+        if (cvt) dir[0] = dir[1] = 1;  // no pack; the converters read A and B
+        else if (G == 1 && split == 1)
             for (int side = 0; side < 2; side++)
                 dir[side] = direct_type_ok(P, side) &&
                             make_direct_map(&dmap[side], side == 0 ? d[b0].A : d[b0].B, P, side,
@@ -1878,9 +2226,15 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
         if (e != cudaSuccess) break;
 
         CUtensorMap tmA, tmB;
-        if (dir[0]) tmA = dmap[0];
-        if (dir[1]) tmB = dmap[1];
-        if ((!dir[0] && !make_map(&tmA, pA, fmt, Kld, M, Lg, BM)) ||
+        if (cvt) {
+            memset(&tmA, 0, sizeof(tmA));  // unused: no TMA operand loads
+            tmB = tmA;
+        } else {
+            if (dir[0]) tmA = dmap[0];
+            if (dir[1]) tmB = dmap[1];
+        }
+        if (cvt) {
+        } else if ((!dir[0] && !make_map(&tmA, pA, fmt, Kld, M, Lg, BM)) ||
             (!dir[1] && !make_map(&tmB, pB, fmt, Kld, Nout, Lg, cta2 ? Geo<true>::b_rows : BN))) {
             e = cudaErrorInvalidValue;
             break;
@@ -1890,12 +2244,27 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
         gp.tiles_m = (int)((M + (cta2 ? 2 * BM : BM) - 1) / (cta2 ? 2 * BM : BM));
         gp.tiles_n = (int)((Nout + BN - 1) / BN);
         gp.num_tiles = gp.tiles_m * gp.tiles_n * (int)Lg;
-        gp.num_kb = (int)((Kld + BK - 1) / BK);
+        gp.num_kb = (int)(((cvt ? K : Kld) + BK - 1) / BK);
         gp.error = flag;
-        gp.a_direct = dir[0];
-        gp.b_direct = dir[1];
-        gp.a_mn = dir[0] && dmn[0];
-        gp.b_mn = dir[1] && dmn[1];
+        if (cvt) {
+            gp.ca = cva;
+            gp.cb = cvb;
+            gp.ca.base = (const float*)d[b0].A;
+            gp.cb.base = (const float*)d[b0].B;
+            if (G > 1) {
+                gp.ca.bases = (const void* const*)(dptr + b0);
+                gp.cb.bases = (const void* const*)(dptr + num + b0);
+                gp.ca.lper = gp.cb.lper = Lsz;
+            }
+            gp.a_mn = cva.mn;
+            gp.b_mn = cvb.mn;
+        }
+        gp.a_direct = cvt ? 0 : dir[0];
+        gp.b_direct = cvt ? 0 : dir[1];
+        if (!cvt) {
+            gp.a_mn = dir[0] && dmn[0];
+            gp.b_mn = dir[1] && dmn[1];
+        }
         gp.a_e0 = de0[0];
         gp.a_k0 = dk0[0];
         gp.b_e0 = de0[1];
@@ -1905,31 +2274,12 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
         gp.a_dims = dmask[0];
         gp.b_dims = dmask[1];
         EpiParams& ep = gp.e;
-        ep.C = d[b0].C;
-        ep.D = d[b0].D;
+        fill_epilogue(ep, P, d[b0].C, d[b0].D, Lg);
         if (G > 1) {
             ep.Cs = dptr + 2 * num + b0;
             ep.Ds = (void* const*)(dptr + 3 * num + b0);
             ep.Lper = Lsz;
         }
-        ep.tC = P->tC;
-        ep.tD = P->tD;
-        ep.cplx = cplx;
-        ep.beta_zero = P->beta_zero;
-        ep.conjC = P->conjC;
-        ep.conjD = P->conjD;
-        ep.conjD_f32 = P->conjD_round_f32;
-        ep.round_C = P->round_in;
-        ep.alpha_re = (float)P->alpha_re;
-        ep.alpha_im = (float)P->alpha_im;
-        ep.beta_re = (float)P->beta_re;
-        ep.beta_im = (float)P->beta_im;
-        ep.M = M;
-        ep.N = N;
-        ep.L = Lg;
-        fill_modes(ep.mm, P->M, 2, 3);
-        fill_modes(ep.nn, P->N, 2, 3);
-        fill_modes(ep.ll, P->L, 2, 3);
         const uint32_t ab = fmt == 1 ? 0u : 1u;  // operand format: 0 f16, 1 bf16
         const uint32_t mma_m = cta2 ? 2 * BM : BM;
         const uint32_t idesc = (1u << 4) | (ab << 7) | (ab << 10) | ((uint32_t)gp.a_mn << 15) |
@@ -1956,31 +2306,12 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
         }
         const int kind = tma_epi ? EPI_TMA : (f32_epi ? EPI_F32 : EPI_ANY);
         const int units = cta2 ? num_sms() / 2 : num_sms();
-        // A last round that fills at most half the units runs its tiles as
-        // two half-contraction items each (partial sums handed over in memory)
         void* split_ws = nullptr;
-        if ((kind == EPI_TMA || kind == EPI_F32) && gp.num_tiles > units && gp.num_kb >= 2) {
-            const int r = gp.num_tiles % units;
-            if (r > 0 && 2 * r <= units) {
-                const size_t pbytes = (size_t)r * 2 * BN * BM * sizeof(float);
-                const size_t fbytes = (size_t)r * 2 * 2 * sizeof(int);
-                if (pool_alloc(&split_ws, pbytes + fbytes, s) == cudaSuccess &&
-                    cudaMemsetAsync((char*)split_ws + pbytes, 0, fbytes, s) == cudaSuccess) {
-                    gp.split_tiles = r;
-                    gp.partial = (float*)split_ws;
-                    gp.pcount = (int*)((char*)split_ws + pbytes);
-                    gp.pready = gp.pcount + r * 2;
-                } else if (split_ws) {
-                    cudaFreeAsync(split_ws, s);
-                    split_ws = nullptr;
-                }
-                (void)cudaGetLastError();
-            }
-        }
+        plan_split_round(gp, kind, units, &split_ws, s);
         const int items = gp.num_tiles + gp.split_tiles;
         const int grid = (items < units ? items : units) * (cta2 ? 2 : 1);
         if (main_timer && b0 == 0) tbk_timer_begin(s, main_timer);
-        e = launch_gemm(kind, cta2, grid, tmA, tmB, gp, idesc, tmC, tmD, s);
+        e = launch_gemm(kind, cta2, grid, tmA, tmB, gp, idesc, tmC, tmD, s, cvt);
         if (main_timer && b0 == 0) tbk_timer_end(s, *main_timer);
         if (split_ws) cudaFreeAsync(split_ws, s);
         count_launch();
@@ -1990,7 +2321,7 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
     if (dptr) cudaFreeAsync(dptr, s);
     if (dmaps) cudaFreeAsync(dmaps, s);
     free(maps);
-    cudaFreeAsync(ws, s);
+    if (ws) cudaFreeAsync(ws, s);
     return e;
 }
 
@@ -2239,6 +2570,19 @@ int tbk_wait_selftest(unsigned long long limit_ns, int* out)
     if (e == cudaSuccess) e = cudaMemcpy(out, d + 4, 4 * sizeof(int), cudaMemcpyDeviceToHost);
     cudaFree(d);
     return (int)e;
+}
+
+// How the tensor-core path loads a plan's operands when A and B start on
+// 16-byte boundaries: 1 split-bfloat16 read in place by the converter warps
+// (one launch), 0 otherwise. No device call (the SM count is not queried
+// either: B200 has an even number).
+int tbk_tc_split_in_place(const tb_plan* P)
+{
+    tb::tc::CvtOperand ca, cb;
+    const void* aligned = (const void*)(uintptr_t)256;
+    return P->path == TB_PATH_TC && P->tc_mode == TB_TC_SPLIT_BF16 && P->compute == TB_R32 &&
+           P->M.size >= 2 * tb::tc::BM && tb::make_cvt_operand(&ca, P, 0, aligned) &&
+           tb::make_cvt_operand(&cb, P, 1, aligned);
 }
 
 // Reads and clears the error word of the allocation-free path (synchronises).

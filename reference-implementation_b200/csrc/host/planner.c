@@ -465,6 +465,8 @@ size_t tb_describe(const tb_plan* p, size_t maxlen, char* out)
              paths[p->path], comp[p->compute], p->prec, p->round_in, p->conjA, p->conjB, p->conjC, p->conjD,
              p->beta_zero);
     if (p->path == TB_PATH_TC) at = put(out, maxlen, at, " tc_mode=%s", tcm[p->tc_mode]);
+    if (p->path == TB_PATH_TC && p->tc_mode == TB_TC_SPLIT_BF16)
+        at = put(out, maxlen, at, " operands=%s", tbk_tc_split_in_place(p) ? "in_place" : "packed");
     if (p->path == TB_PATH_SLICED) at = put(out, maxlen, at, " slices=%d", p->slices);
     if (p->path == TB_PATH_SIMT) {
         static const char* kern[] = {"tiled", "narrow", "narrow_stream", "narrow_coop", "narrow_cstream"};
