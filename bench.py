@@ -50,10 +50,12 @@ FLOPS = 2.0 * (EXTENT ** 2) ** 3          # 2 * M * N * K
 WORKLOAD = "dense_4index_contraction_64^4"
 METRIC = f"TFLOP/s ({WORKLOAD}, F32)"     # the same string on both arms
 HEADLINE = "split_bf16_f32"
-STEP_DESCRIPTION = "one tcgen05 GEMM launch: converter warps split A and B into bfloat16 hi/lo in shared memory (read in place), fused epilogue"
+STEP_DESCRIPTION = ("a pass per operand writes [hi | lo] bfloat16 panels, then one tcgen05 GEMM "
+                    "(three MMAs per 16-deep step on TMA-loaded hi/lo tiles) with the fused epilogue")
 MODES = {
     # name: (precision, storage of A and B, f32_mode, forced path)
     "split_bf16_f32": (0, 0, 1, 0),
+    "split_bf16_f32_in_place": (0, 0, 3, 0),
     "bf16": (6, 0, 0, 0),
     "f16": (5, 0, 0, 0),
     "bf16_storage": (6, 5, 0, 0),

@@ -44,7 +44,12 @@ enum {
      * TAPP_DEFAULT_PREC on binary32 data):
      *   0 plain binary32 on CUDA cores (default),
      *   1 split-bfloat16 on tensor cores: each operand is split into a
-     *     bfloat16 high and low part, three products accumulate in binary32. */
+     *     bfloat16 high and low part, three products accumulate in binary32;
+     *   2 the same with the operands always split into packed hi/lo panels
+     *     first (one pass over each, then the GEMM);
+     *   3 the same with the operands always read in place where their
+     *     layout allows (binary32 storage; the GEMM splits them itself).
+     * Mode 1 picks the faster of 2 and 3 for the product. */
     TAPP_B200_ATTR_F32_MODE = 0x1002,
     /* value: int*. Force an execution path: 0 automatic (default),
      * 1 CUDA-core element kernel, 2 CUDA-core reduction, 3 tiled CUDA-core
@@ -72,6 +77,11 @@ enum {
      *     element of each row. Inputs must be finite (a row or column with
      *     a non-finite value gives NaN). Environment: TAPP_B200_F64_MODE. */
     TAPP_B200_ATTR_F64_MODE = 0x1007,
+    /* value: int*. Tile shape of grouped tensor-core products
+     * (tapp_b200_execute_group, servers): 0 per shape class from the tuned
+     * table (tapp_b200_load_tile_table), else by size (default), 1 256 x 256
+     * tiles on SM pairs, 2 128 x 128 tiles. */
+    TAPP_B200_ATTR_TILE = 0x1008,
 };
 
 /* ---- keys readable from a status object with TAPP_attr_get ---- */
@@ -180,6 +190,36 @@ TAPP_EXPORT TAPP_error tapp_b200_execute_chain(int n, const TAPP_tensor_product*
                                                const void* const* alphas, const void* const* betas,
                                                const void* const* A, const void* const* B,
                                                const void* const* C, void* const* D);
+
+/*
+ * Products of different plans in one call (the reference's batched product,
+ * api/include/tapp/product.h:66-75, covers many products of one plan; this
+ * entry point has no counterpart there). Product i is plans[i] with
+ * alphas[i], betas[i], A[i], B[i], C ? C[i] : NULL and D[i] as
+ * TAPP_execute_product takes them. Products that run on the tensor cores
+ * from binary32 storage (BF16BF16_ACCUM_F32, F16F16_ACCUM_F32, or F32 in
+ * split mode) without unary modes and with all operands on the device run
+ * together in one persistent launch per tile shape (TAPP_B200_ATTR_TILE),
+ * their operands read in place; every other product runs as
+ * TAPP_execute_product runs it. All products are validated first, with the
+ * codes of TAPP_execute_product; nothing runs if one fails. The products must
+ * be independent (no D overlapping another product's operands). Synchronous
+ * unless the executor is asynchronous; TAPP_B200_ERR_INVALID for missing
+ * pointers or an executor attached to a server.
+ */
+TAPP_EXPORT TAPP_error tapp_b200_execute_group(int n, const TAPP_tensor_product* plans, TAPP_executor exec,
+                                               const void* const* alphas, const void* const* betas,
+                                               const void* const* A, const void* const* B,
+                                               const void* const* C, void* const* D);
+
+/*
+ * Loads the table of tile shapes per shape class written by the tuner
+ * (tapp_b200/tuner.py) for grouped tensor-core products with
+ * TAPP_B200_ATTR_TILE = 0; NULL drops the table (sizes decide). The
+ * environment variable TAPP_B200_TILE_TABLE names a table loaded at first
+ * use. Returns 0, or TAPP_B200_ERR_INVALID when the file cannot be read.
+ */
+TAPP_EXPORT TAPP_error tapp_b200_load_tile_table(const char* path);
 
 /*
  * Serving: a request loop that runs products as they arrive on one GPU.

@@ -130,6 +130,9 @@ cudaError_t launch_sliced(const tb_plan* P, const tb_ptrs* d, cudaStream_t s, in
 size_t reduce_scratch_bytes(const tb_plan* P, size_t real_bytes);
 cudaError_t launch_generic_group(const tb_plan* const* P, const tb_ptrs* d, int n, void* host, void* dev,
                                  cudaStream_t s);
+size_t group_tc_bytes(int n);
+cudaError_t launch_group_tc(const tb_plan* const* P, const tb_ptrs* d, int n, void* host, void* dev, int tile,
+                            cudaStream_t s, int64_t* tiles_out);
 
 static void CUDART_CB free_host_buffer(void* p) { free(p); }
 
@@ -353,6 +356,38 @@ size_t tbk_scratch_bytes(const tb_plan* plan)
         return tb::reduce_scratch_bytes(plan, plan->compute == TB_R32 || plan->compute == TB_C32 ? 4 : 8);
     default: return 0;
     }
+}
+
+size_t tbk_group_tc_bytes(int n) { return tb::group_tc_bytes(n); }
+
+int tbk_run_group_tc(const tb_plan* const* plans, const tb_ptrs* ptrs, int n, void* host_desc, void* dev_desc, int tile,
+                     void* stream, int64_t* tiles)
+{
+    return (int)tb::launch_group_tc(plans, ptrs, n, host_desc, dev_desc, tile, (cudaStream_t)stream, tiles);
+}
+
+// One grouped tensor-core launch with descriptor buffers of its own: a host
+// buffer freed by a stream callback once its copy has run, device memory
+// from the pool.
+int tbk_run_group_tc_owned(const tb_plan* const* plans, const tb_ptrs* ptrs, int n, int tile, void* stream,
+                           int64_t* tiles)
+{
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t bytes = tb::group_tc_bytes(n);
+    void* host = malloc(bytes);
+    if (!host) return (int)cudaErrorMemoryAllocation;
+    void* dev = nullptr;
+    cudaError_t e = tb::pool_alloc(&dev, bytes, s);
+    if (e == cudaSuccess) {
+        e = tb::launch_group_tc(plans, ptrs, n, host, dev, tile, s, tiles);
+        cudaFreeAsync(dev, s);
+    }
+    if (e == cudaSuccess) e = cudaLaunchHostFunc(s, tb::free_host_buffer, host);
+    else {
+        cudaStreamSynchronize(s);
+        free(host);
+    }
+    return (int)e;
 }
 
 int tbk_run_group(const tb_plan* const* plans, const tb_ptrs* ptrs, int n, void* host_desc, void* dev_desc,

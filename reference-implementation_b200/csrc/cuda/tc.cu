@@ -26,6 +26,7 @@
 
 #include "../tb_cuda.h"
 #include "tb_common.cuh"
+#include "tc_device.cuh"
 
 namespace tb {
 cudaError_t launch_generic(const tb_plan* P, const tb_ptrs* d, cudaStream_t s);
@@ -34,56 +35,6 @@ cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t s);
 cudaError_t stage_copy(void* dev_dst, const void* src, size_t bytes, cudaStream_t s);
 
 namespace tc {
-
-constexpr int BM = 128, BN = 256, BK = 64, STAGES = 4;
-constexpr int A_BYTES = BM * BK * 2;
-constexpr int B_BYTES = BN * BK * 2;
-constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
-
-// Stage geometry per CTA. One CTA: A 128x64 and B 256x64 per stage, 4
-// stages. CTA pair (cta_group::2, 256x256 tiles): each CTA holds its 128
-// rows of A and 128 of the 256 columns of B, 6 stages. Same 192 KiB.
-template <bool CTA2>
-struct Geo {
-    static constexpr int stages = CTA2 ? 6 : 4;
-    static constexpr int b_rows = CTA2 ? 128 : 256;   // rows of B per CTA per stage
-    static constexpr int a_bytes = BM * BK * 2;
-    static constexpr int b_bytes = b_rows * BK * 2;
-    static constexpr int stage_bytes = a_bytes + b_bytes;
-    static constexpr int tile_m = CTA2 ? 2 * BM : BM;  // output rows per tile
-};
-static_assert(Geo<true>::stages * Geo<true>::stage_bytes == STAGES * STAGE_BYTES, "same ring size");
-constexpr int TMEM_COLS = 512;
-constexpr int EPI_WARPS = 8;                    // two warps per TMEM lane quarter
-constexpr int EPI_THREADS = EPI_WARPS * 32;
-constexpr int NTHREADS = 128 + EPI_THREADS;
-constexpr int STAGE_EPI_BYTES = 32 * 32 * 4;  // one 32x32 fp32 box per epilogue warp
-// tiles | barriers | epilogue staging (the per-thread epilogue keeps its
-// column-offset tables in the staging area instead)
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/ + 8 * STAGE_EPI_BYTES;
-static_assert(2 * BN * 8 <= 8 * STAGE_EPI_BYTES, "column tables fit in the staging area");
-static_assert(SMEM_BYTES <= 232448, "dynamic shared memory limit of sm_100");
-constexpr unsigned long long WAIT_NS = 4000000000ull;  // 4 s per wait
-
-struct ModeList {
-    int32_t n;
-    int32_t pad;
-    int64_t ext[TB_MAXMODES];
-    int64_t s0[TB_MAXMODES];  // stride in the first tensor (C, or the packed source)
-    int64_t s1[TB_MAXMODES];  // stride in the second tensor (D)
-};
-
-__host__ __device__ inline void decode2(const ModeList& m, int64_t idx, int64_t& o0, int64_t& o1)
-{
-    o0 = 0;
-    o1 = 0;
-    for (int j = 0; j < m.n; j++) {
-        int64_t c = idx % m.ext[j];
-        idx /= m.ext[j];
-        o0 += c * m.s0[j];
-        o1 += c * m.s1[j];
-    }
-}
 
 // ---------------------------------------------------------------------------
 // pack
@@ -315,10 +266,11 @@ __global__ void __launch_bounds__(256, 4) k_pack_real(PackParams p)
 #pragma unroll
         for (int h = 0; h < 4; h++) {
             float a = v[r][g * 8 + 2 * h], b = v[r][g * 8 + 2 * h + 1];
-            if (SPLIT == 3) {
+            if (SPLIT >= 2) {
                 const float ah = __bfloat162float(__float2bfloat16_rn(a));
                 const float bh = __bfloat162float(__float2bfloat16_rn(b));
-                const bool use_lo = p.is_B ? (seg == 1) : (seg == 2);  // A: hi, hi, lo   B: hi, lo, hi
+                // three segments: A hi, hi, lo and B hi, lo, hi; two: [hi | lo] for both
+                const bool use_lo = SPLIT == 2 ? seg == 1 : p.is_B ? (seg == 1) : (seg == 2);
                 if (use_lo) { a -= ah; b -= bh; } else { a = ah; b = bh; }
             }
             if (FMT == 1) {
@@ -338,6 +290,7 @@ template <typename T, bool RF, int VEC>
 static void launch_pack_real3(const PackParams& pp, int split, int fmt, dim3 grid, cudaStream_t s)
 {
     if (split == 3) k_pack_real<T, 3, 0, RF, VEC><<<grid, 256, 0, s>>>(pp);
+    else if (split == 2) k_pack_real<T, 2, 0, RF, VEC><<<grid, 256, 0, s>>>(pp);
     else if (fmt == 1) k_pack_real<T, 1, 1, RF, VEC><<<grid, 256, 0, s>>>(pp);
     else k_pack_real<T, 1, 0, RF, VEC><<<grid, 256, 0, s>>>(pp);
 }
@@ -376,200 +329,6 @@ static void launch_pack_real(const PackParams& pp, int split, int fmt, int64_t l
     }
 }
 
-// ---------------------------------------------------------------------------
-// GEMM
-struct EpiParams {
-    const void* C;
-    void* D;
-    int32_t tC, tD, cplx, beta_zero, conjC, conjD, conjD_f32, round_C;
-    float alpha_re, alpha_im, beta_re, beta_im;
-    int64_t M, N, L;   // output sizes (N counts complex elements when cplx)
-    ModeList mm, nn, ll;  // s0 = stride in C, s1 = stride in D
-    // EPI_I32 (integer slice products): W[l][m][n] = (first ? 0 : W) + level_scale * acc,
-    // W dense binary64 with N columns
-    double* W;
-    double level_scale;
-    int32_t w_first, w_pad;
-    // batched product: C and D of batch b = l / Lper (device arrays), else NULL;
-    // with the TMA epilogue, also their tensor maps (tmCs NULL when beta = 0)
-    const void* const* Cs;
-    void* const* Ds;
-    const CUtensorMap* tmCs;
-    const CUtensorMap* tmDs;
-    int64_t Lper;
-};
-
-// An operand the split-bfloat16 GEMM reads in place from binary32 storage:
-// index -> element offset maps of its row (M or N), contracted and batch
-// modes (at most 4 each, indices below 2^31), and its major side: mn = 1
-// when its contiguous mode (stride 1, extent a multiple of 8) is a row mode,
-// 0 when it is a contracted mode. Every other stride is a multiple of 4 and
-// the base is 16-byte aligned, so each run of 8 elements along the
-// contiguous mode is two 16-byte loads.
-struct CvtDim {
-    int32_t n;
-    uint32_t size;
-    FastDiv div[4];
-    int64_t st[4];
-};
-struct CvtOperand {
-    const float* base;
-    const void* const* bases;  // batched product: base of batch b = l / lper, else NULL
-    int64_t lper;              // batch modes per batch
-    int32_t mn, pad;
-    CvtDim rows, ks, ls;
-};
-
-struct GemmParams {
-    int32_t tiles_m, tiles_n, num_tiles, num_kb;
-    EpiParams e;
-    int* error;       // set to 1 when a wait times out
-    // The last split_tiles tiles (the last, partial round of the persistent
-    // schedule) run as two work items each, the two halves of the
-    // contraction. Whichever half finishes first (pcount, per tile and CTA
-    // rank) writes its raw sums to partial ([col][row]) and raises pready; the
-    // other adds them and runs the epilogue. The first is running when the
-    // second waits for it, so the wait cannot depend on scheduling. pcount and
-    // pready start at zero.
-    int32_t split_tiles, pad_s;
-    float* partial;
-    int* pcount;
-    int* pready;
-    // Operands read in place (16-bit storage, no pack): the tensor map has
-    // the dims (row mode 0, k mode 0, row mode 1, k mode 1, batch) in the
-    // MN-major case and (k mode 0, row mode 0, k mode 1, row mode 1, batch)
-    // in the K-major case; every stage loads 64-row x 64-k boxes. e0/k0 are
-    // the extents of row mode 0 and k mode 0 (multiples of 64).
-    int32_t a_direct, b_direct, a_mn, b_mn;
-    int32_t a_e0, a_k0, b_e0, b_k0;
-    // box shape of each direct operand: 0 one 64-row box per 64 rows, 1 all
-    // rows in one box along row mode 1 (row mode 0 has extent 64), 2 all rows
-    // in one box along row mode 0 (K-major, extent a multiple of the rows)
-    int32_t a_box, b_box;
-    // logical dims present in each direct operand's map (bit j: dim j; dims
-    // of extent 1 are left out, fewer dims copy faster)
-    int32_t a_dims, b_dims;
-    // split-bfloat16 GEMM reading binary32 operands in place (k_gemm<.., CVT>)
-    CvtOperand ca, cb;
-};
-
-// work item it of the persistent schedule: tile, contraction-block range and
-// role (0 whole tile, 1 and 2 the two halves of a split tile)
-struct Item {
-    int tile, kb0, kb1, role;
-};
-
-__device__ __forceinline__ Item item_of(const GemmParams& p, int it)
-{
-    const int nfull = p.num_tiles - p.split_tiles;
-    if (it < nfull) return Item{it, 0, p.num_kb, 0};
-    const int j = it - nfull, kh = p.num_kb / 2;
-    return (j & 1) ? Item{nfull + j / 2, kh, p.num_kb, 2} : Item{nfull + j / 2, 0, kh, 1};
-}
-
-// TMA epilogue: C and D as (up to) 5-d tensor maps whose dims are
-// [first M mode, first N mode, further M modes, further N modes, L modes];
-// every warp moves 32 x 32 boxes (32 consecutive rows of the first M mode,
-// 32 consecutive columns of the first N mode).
-struct TmaEpi {
-    int32_t rank;
-}; 
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
-{
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity)
-{
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-__device__ __forceinline__ unsigned long long now_ns()
-{
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-// try_wait with cluster-scope acquire: for a barrier that threads of the
-// other CTA of a pair arrive on (release, cluster scope) after writing
-// shared memory that this thread's MMAs then read
-__device__ __forceinline__ bool mbar_try_cluster(uint64_t* bar, uint32_t parity)
-{
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// Waits for the phase of `parity` to complete; gives up after limit_ns (4 s
-// in the kernels; or at once when another role already gave up), raises
-// *abort_flag and returns false.
-template <bool CLUSTER = false>
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
-                                          unsigned long long limit_ns = WAIT_NS)
-{
-    auto try_ = [&] { return CLUSTER ? mbar_try_cluster(bar, parity) : mbar_try(bar, parity); };
-    if (try_()) return true;
-    const unsigned long long t0 = now_ns();
-    for (uint32_t i = 1;; i++) {
-        if (try_()) return true;
-        if ((i & 255) == 0) {
-            if (*abort_flag) return false;
-            if (now_ns() - t0 > limit_ns) {
-                *abort_flag = 1;
-                return false;
-            }
-        }
-    }
-}
-
-// Waits until another CTA raised *flag (acquire, GPU scope); gives up like
-// mbar_wait.
-__device__ __forceinline__ bool flag_wait(const int* flag, volatile int* abort_flag,
-                                          unsigned long long limit_ns = WAIT_NS)
-{
-    const unsigned long long t0 = now_ns();
-    for (uint32_t i = 0;; i++) {
-        int v;
-        asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(flag) : "memory");
-        if (v) return true;
-        if ((i & 63) == 63) {
-            if (*abort_flag) return false;
-            if (now_ns() - t0 > limit_ns) {
-                *abort_flag = 1;
-                return false;
-            }
-        }
-    }
-}
-
 // Self-test of the bounded waits: one thread waits, with the kernels' own
 // flag_wait and mbar_wait, on a flag that nothing raises and on the first
 // phase of an mbarrier that nothing completes, limit_ns each. Both must give
@@ -590,386 +349,28 @@ __global__ void k_wait_selftest(const int* flag, int* out, unsigned long long li
     out[3] = abort_word;
 }
 
-__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* tm, uint64_t* bar, int c0, int c1, int c2)
-{
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
-        ::"r"(smem_u32(dst)), "l"(tm), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
-        : "memory");
-}
-
-__device__ __forceinline__ void tma_load_5d(void* dst, const CUtensorMap* tm, uint64_t* bar, const int (&c)[5])
-{
-    asm volatile(
-        "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6, %7}], [%2];"
-        ::"r"(smem_u32(dst)), "l"(tm), "r"(smem_u32(bar)), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(c[4])
-        : "memory");
-}
-
-__device__ __forceinline__ void tma_store_5d(const CUtensorMap* tm, const void* src, const int (&c)[5])
-{
-    asm volatile("cp.async.bulk.tensor.5d.global.shared::cta.bulk_group [%0, {%2, %3, %4, %5, %6}], [%1];"
-                 ::"l"(tm), "r"(smem_u32(src)), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(c[4])
-                 : "memory");
-}
-
-__device__ __forceinline__ void tma_load_3d_pair(void* dst, const CUtensorMap* tm, uint32_t bar_cluster, int c0, int c1,
-                                                 int c2)
-{
-    asm volatile(
-        "cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
-        ::"r"(smem_u32(dst)), "l"(tm), "r"(bar_cluster), "r"(c0), "r"(c1), "r"(c2)
-        : "memory");
-}
-
-__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* tm, uint64_t* bar, const int (&c)[5])
-{
-    asm volatile(
-        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6}], [%2];"
-        ::"r"(smem_u32(dst)), "l"(tm), "r"(smem_u32(bar)), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3])
-        : "memory");
-}
-
-__device__ __forceinline__ void tma_load_4d_pair(void* dst, const CUtensorMap* tm, uint32_t bar_cluster, const int (&c)[5])
-{
-    asm volatile(
-        "cp.async.bulk.tensor.4d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6}], [%2];"
-        ::"r"(smem_u32(dst)), "l"(tm), "r"(bar_cluster), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3])
-        : "memory");
-}
-
-__device__ __forceinline__ void tma_load_3d_c(void* dst, const CUtensorMap* tm, uint64_t* bar, const int (&c)[5])
-{
-    tma_load_3d(dst, tm, bar, c[0], c[1], c[2]);
-}
-
-__device__ __forceinline__ void tma_load_5d_pair(void* dst, const CUtensorMap* tm, uint32_t bar_cluster, const int (&c)[5])
-{
-    asm volatile(
-        "cp.async.bulk.tensor.5d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6, %7}], [%2];"
-        ::"r"(smem_u32(dst)), "l"(tm), "r"(bar_cluster), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(c[4])
-        : "memory");
-}
-
-// address of the same shared-memory location in CTA `rank` of the cluster
-__device__ __forceinline__ uint32_t cluster_addr(const void* p, uint32_t rank)
-{
-    uint32_t r;
-    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(p)), "r"(rank));
-    return r;
-}
-
-__device__ __forceinline__ uint32_t cluster_rank()
-{
-    uint32_t r;
-    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
-    return r;
-}
-
-__device__ __forceinline__ void cluster_sync()
-{
-    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive_cluster(uint32_t bar_cluster)
-{
-    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(bar_cluster) : "memory");
-}
-
-__device__ __forceinline__ void mma_f16_pair(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t accumulate)
-{
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-        ::"r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accumulate)
-        : "memory");
-}
-
-// commit to the barrier at this offset in both CTAs of the pair
-__device__ __forceinline__ void mma_commit_pair(uint64_t* bar)
-{
-    const uint16_t mask = 3;
-    asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;"
-                 ::"r"(smem_u32(bar)), "h"(mask)
-                 : "memory");
-}
-
-__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-
-// K-major operand tile with 128-byte swizzle: rows of 64 16-bit elements,
-// 8-row groups 1024 bytes apart.
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr)
-{
-    uint64_t d = 0;
-    d |= (uint64_t)((addr & 0x3FFFF) >> 4);
-    d |= (uint64_t)1 << 16;             // leading byte offset 16 B (unused with 128B swizzle)
-    d |= (uint64_t)(1024 >> 4) << 32;   // stride byte offset between 8-row groups
-    d |= (uint64_t)1 << 46;             // descriptor version (sm100)
-    d |= (uint64_t)2 << 61;             // SWIZZLE_128B
-    return d;
-}
-
-// signed 8-bit operands, 32-bit integer accumulators (exact)
-__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t accumulate)
-{
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}"
-        ::"r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accumulate)
-        : "memory");
-}
-
-__device__ __forceinline__ void mma_i8_pair(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t accumulate)
-{
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n\t}"
-        ::"r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accumulate)
-        : "memory");
-}
-
-// MN-major operand tile with 128-byte swizzle: 64-element (128-byte) rows
-// along M/N holding one k each, 8 k-rows per 1024-byte group (SBO), the
-// second 64-row half of the tile 8 KiB further (LBO)
-__device__ __forceinline__ uint64_t smem_desc_mn(uint32_t addr)
-{
-    uint64_t d = 0;
-    d |= (uint64_t)((addr & 0x3FFFF) >> 4);
-    d |= (uint64_t)(8192 >> 4) << 16;   // leading byte offset: between 64-row halves
-    d |= (uint64_t)(1024 >> 4) << 32;   // stride byte offset: between 8-k groups
-    d |= (uint64_t)1 << 46;
-    d |= (uint64_t)2 << 61;             // SWIZZLE_128B
-    return d;
-}
-
-__device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t accumulate)
-{
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-        ::"r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accumulate)
-        : "memory");
-}
-
-__device__ __forceinline__ void mma_commit(uint64_t* bar)
-{
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-                 : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32])
-{
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
-
-// read-only global load kept as its own instruction, so a run of them stays
-// in flight together before any result is used
-__device__ __forceinline__ float ld_nc_f32(const float* p)
-{
-    float v;
-    asm volatile("ld.global.nc.f32 %0, [%1];" : "=f"(v) : "l"(p));
-    return v;
-}
-
-template <int N>
-__device__ __forceinline__ void epi_bar_n() { asm volatile("bar.sync 1, %0;" ::"n"(N) : "memory"); }
-
-// beta * op_C(C) for one output (0 when beta == 0)
-__device__ __forceinline__ void load_beta_c(const EpiParams& e, const void* Cbase, int64_t offC, float& br, float& bi)
-{
-    br = 0.f;
-    bi = 0.f;
-    if (e.beta_zero) return;
-    float cr, ci;
-    load_rounded<float>(Cbase, offC, e.tC, e.round_C, cr, ci);
-    if (e.conjC) ci = -ci;
-    if (e.cplx) {
-        br = e.beta_re * cr - e.beta_im * ci;
-        bi = e.beta_re * ci + e.beta_im * cr;
-    } else {
-        br = e.beta_re * cr;
-    }
-}
-
-__device__ __forceinline__ void finish_out(const EpiParams& e, void* Dbase, int64_t offD, float ar, float ai, float br,
-                                           float bi)
-{
-    float accr, acci;
-    if (e.cplx) {
-        accr = e.alpha_re * ar - e.alpha_im * ai + br;
-        acci = e.alpha_re * ai + e.alpha_im * ar + bi;
-    } else {
-        accr = e.alpha_re * ar + br;
-        acci = 0.f;
-    }
-    if (e.conjD) acci = -acci;
-    store_elem<float>(Dbase, offD, e.tD, accr, acci);
-}
-
-// ---------------------------------------------------------------------------
-// In-place split-bfloat16 operands (k_gemm<.., CVT = true>): eight converter
-// warps per CTA load the binary32 tiles of A and B with 16-byte loads,
-// split every value into hi = bf16(x) and lo = bf16(x - hi), and store both
-// in the swizzled layouts the MMAs read (K-major or MN-major, 128-byte
-// swizzle). Per CTA and 64-deep contraction block a converter thread owns 4
-// units of 8 consecutive elements of each operand:
-//   K-major (contiguous along k): rows hi2 + 4 cw + 32 j (j < 4), the k run
-//     8 lo3 .. 8 lo3 + 7; the 8 lanes of a row store one whole 128-byte row
-//   MN-major (contiguous along rows): rows 64 h + 8 lo3 .. + 7 (h < 2) at
-//     k = hi2 + 4 cw + 32 jk (jk < 2); 8 lanes store one 128-byte k-line
-// (cw the converter warp, lo3 = lane % 8, hi2 = lane / 8), so every store
-// of a warp covers whole 128-byte lines (no bank conflicts) and every 8
-// lanes read 256 contiguous bytes.
-__device__ __forceinline__ int64_t cvt_decode(const CvtDim& d, uint32_t idx)
-{
-    int64_t off = 0;
-#pragma unroll
-    for (int j = 0; j < 3; j++) {
-        if (j + 1 >= d.n) break;
-        const uint32_t q = fdiv(idx, d.div[j]);
-        off += (int64_t)(idx - q * d.div[j].d) * d.st[j];
-        idx = q;
-    }
-    return d.n ? off + (int64_t)idx * d.st[d.n - 1] : 0;
-}
-
-// element offsets of this thread's unit rows for one tile (-1: past the
-// end); returns the tile's operand base (its batch's, in a batched product)
-__device__ __forceinline__ const float* cvt_rows(const CvtOperand& o, int64_t row0, int64_t l, int cw, int lo3,
-                                                 int hi2, int64_t (&roff)[4])
-{
-    const float* base = o.base;
-    if (o.bases) {
-        base = (const float*)o.bases[l / o.lper];
-        l %= o.lper;
-    }
-    const int64_t loff = cvt_decode(o.ls, (uint32_t)l);
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-        int64_t r;
-        if (o.mn) r = j < 2 ? row0 + 64 * j + 8 * lo3 : -1;
-        else r = row0 + hi2 + 4 * cw + 32 * j;
-        roff[j] = (r >= 0 && r < (int64_t)o.rows.size) ? loff + cvt_decode(o.rows, (uint32_t)r) : -1;
-    }
-    return base;
-}
-
-__device__ __forceinline__ float4 ld_nc_v4(const float* p)
-{
-    float4 v;
-    asm volatile("ld.global.nc.L1::no_allocate.v4.f32 {%0,%1,%2,%3}, [%4];"
-                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
-                 : "l"(p));
-    return v;
-}
-
-// the 4 units of contraction block kb into x (zeros past the tensor's end)
-__device__ __forceinline__ void cvt_load(const CvtOperand& o, const float* base, const int64_t (&roff)[4], int kb,
-                                         int cw, int lo3, int hi2, float (&x)[32])
-{
-#pragma unroll
-    for (int u = 0; u < 4; u++) {
-        int64_t ro;
-        uint32_t k;
-        if (o.mn) {
-            ro = roff[u & 1];
-            k = (uint32_t)kb * 64 + hi2 + 4 * cw + 32 * (u >> 1);
-        } else {
-            ro = roff[u];
-            k = (uint32_t)kb * 64 + 8 * lo3;
-        }
-        float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
-        if (ro >= 0 && k < o.ks.size) {
-            const float* q = base + ro + cvt_decode(o.ks, k);
-            a = ld_nc_v4(q);
-            b = ld_nc_v4(q + 4);
-        }
-        x[8 * u + 0] = a.x; x[8 * u + 1] = a.y; x[8 * u + 2] = a.z; x[8 * u + 3] = a.w;
-        x[8 * u + 4] = b.x; x[8 * u + 5] = b.y; x[8 * u + 6] = b.z; x[8 * u + 7] = b.w;
-    }
-}
-
-// hi = bf16(x), lo = bf16(x - hi) of 8 values as two 16-byte vectors
-__device__ __forceinline__ void split8(const float* x, uint4& hi, uint4& lo)
-{
-    uint32_t h[4], w[4];
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-        __nv_bfloat162 q = __floats2bfloat162_rn(x[2 * i], x[2 * i + 1]);
-        h[i] = *(uint32_t*)&q;
-        const float a = __uint_as_float(h[i] << 16), b = __uint_as_float(h[i] & 0xffff0000u);
-        __nv_bfloat162 r = __floats2bfloat162_rn(x[2 * i] - a, x[2 * i + 1] - b);
-        w[i] = *(uint32_t*)&r;
-    }
-    hi = make_uint4(h[0], h[1], h[2], h[3]);
-    lo = make_uint4(w[0], w[1], w[2], w[3]);
-}
-
-__device__ __forceinline__ void st_shared_v4(uint32_t addr, const uint4& v)
-{
-    asm volatile("st.shared.v4.b32 [%0], {%1,%2,%3,%4};" ::"r"(addr), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w)
-                 : "memory");
-}
-
-// stores the split units into the hi and lo tiles (128 x 64 each, 16 KiB)
-__device__ __forceinline__ void cvt_store(const CvtOperand& o, const float (&x)[32], uint32_t hi_tile,
-                                          uint32_t lo_tile, int cw, int lo3, int hi2)
-{
-#pragma unroll
-    for (int u = 0; u < 4; u++) {
-        uint32_t off;
-        if (o.mn) {
-            const int k = hi2 + 4 * cw + 32 * (u >> 1), h = u & 1;
-            off = h * 8192 + (k >> 3) * 1024 + (k & 7) * 128 + ((lo3 ^ (k & 7)) << 4);
-        } else {
-            const int r = hi2 + 4 * cw + 32 * u;
-            off = r * 128 + ((lo3 ^ (r & 7)) << 4);
-        }
-        uint4 hi, lo;
-        split8(&x[8 * u], hi, lo);
-        st_shared_v4(hi_tile + off, hi);
-        st_shared_v4(lo_tile + off, lo);
-    }
-}
-
-// EPI_F32: real product, C and D binary32 (the common case, specialised);
-// EPI_ANY: every storage type, complex outputs, op_C / op_D.
-// EPI_TMA: like EPI_F32, with C and D moved by TMA tensor copies through a
-// per-warp shared-memory box (C and D expressible as tensor maps).
-// EPI_I32: signed 8-bit operands (kind::i8, rows of 128 elements per stage),
-// 32-bit integer accumulators added into a binary64 workspace.
-enum { EPI_ANY = 0, EPI_F32 = 1, EPI_TMA = 2, EPI_I32 = 3 };
-
 // CVT: the split-bfloat16 product of binary32 operands read in place by
 // eight converter warps (warps 8-15, 512 threads) instead of TMA loads of
 // packed panels; stages of 64 KiB (A hi, A lo, B hi, B lo), three MMAs per
 // 16-deep step (hi*hi, hi*lo, lo*hi), four epilogue warps (4-7).
-template <int EPI, bool CTA2, bool CVT = false>
-__global__ void __launch_bounds__(CVT ? 512 : NTHREADS, 1)
+// LOAD = 2: the split-bfloat16 product from packed panels that hold each
+// operand's hi and lo parts side by side ([hi | lo] along k): TMA brings A hi,
+// A lo, B hi, B lo of one 64-deep block into a 64 KiB stage and the same
+// three MMAs run on it (4 bytes of panel per element instead of the 6 of
+// three-segment panels).
+template <int EPI, bool CTA2, int LOAD = 0>
+__global__ void __launch_bounds__(LOAD == 1 ? 512 : NTHREADS, 1)
     k_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, GemmParams p,
            uint32_t idesc, const __grid_constant__ CUtensorMap tmC, const __grid_constant__ CUtensorMap tmD)
 {
     using G = Geo<CTA2>;
-    constexpr int NS = CVT ? 3 : G::stages;
-    constexpr int SB = CVT ? 4 * BM * BK * 2 : G::stage_bytes;  // bytes per stage
+    constexpr bool CVT = LOAD == 1, SPL = LOAD == 2, TRI = LOAD != 0;  // TRI: three MMAs per step
+    constexpr int NS = TRI ? 3 : G::stages;
+    constexpr int SB = TRI ? 4 * BM * BK * 2 : G::stage_bytes;  // bytes per stage
     constexpr int EW = CVT ? 4 : EPI_WARPS;                      // epilogue warps
     constexpr int ET = EW * 32;
     constexpr int CS = EW / 4;  // a warp's chunk step: the warps of a lane quarter interleave
-    static_assert(!CVT || (CTA2 && NS * SB <= STAGES * STAGE_BYTES), "split stages fit the ring");
+    static_assert(!TRI || (CTA2 && NS * SB <= STAGES * STAGE_BYTES), "split stages fit the ring");
     auto epi_bar = [] { epi_bar_n<ET>(); };
     constexpr int KSTEP = EPI == EPI_I32 ? 2 * BK : BK;  // elements per 128-byte stage row
     extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -1080,7 +481,7 @@ __global__ void __launch_bounds__(CVT ? 512 : NTHREADS, 1)
                     const int s = g % NS;
                     const uint32_t ph = (g / NS) & 1;
                     if (!mbar_wait(&empty[s], ph ^ 1, abort_flag)) { ok = false; break; }
-                    uint8_t* a = tiles + s * G::stage_bytes;
+                    uint8_t* a = tiles + s * SB;
                     // one chunk of an in-place operand: logical coordinates
                     // (row0, k0, row1, k1, batch) or (k0, row0, k1, row1,
                     // batch), then those of the dims the map keeps
@@ -1113,11 +514,17 @@ __global__ void __launch_bounds__(CVT ? 512 : NTHREADS, 1)
                     if (!do_a) {
                     } else if (CTA2) {
                         // both halves land on the leader's barrier, which expects the pair's bytes
-                        if (rank == 0) mbar_expect_tx(&full[s], 2 * G::stage_bytes);
+                        if (rank == 0) mbar_expect_tx(&full[s], 2 * SB);
                     } else {
                         mbar_expect_tx(&full[s], G::stage_bytes);
                     }
-                    if (!do_a) {
+                    if (SPL) {
+                        // A hi, A lo, B hi, B lo of block kb (lo at k offset lo_off)
+                        tma_load_3d_pair(a, &tmA, fb, kb * BK, arow, l);
+                        tma_load_3d_pair(a + 16384, &tmA, fb, p.lo_off + kb * BK, arow, l);
+                        tma_load_3d_pair(a + 32768, &tmB, fb, kb * BK, brow, l);
+                        tma_load_3d_pair(a + 49152, &tmB, fb, p.lo_off + kb * BK, brow, l);
+                    } else if (!do_a) {
                     } else if (p.a_direct) {
                         const int nc = p.a_box ? 1 : BM / 64;
 #pragma unroll
@@ -1129,7 +536,7 @@ __global__ void __launch_bounds__(CVT ? 512 : NTHREADS, 1)
                     } else {
                         tma_load_3d(a, &tmA, &full[s], kb * KSTEP, tm * BM, l);
                     }
-                    if (!do_b) {
+                    if (SPL || !do_b) {
                     } else if (p.b_direct) {
                         const int nc = p.b_box ? 1 : G::b_rows / 64;
 #pragma unroll
@@ -1190,7 +597,7 @@ __global__ void __launch_bounds__(CVT ? 512 : NTHREADS, 1)
                     const uint32_t b = a + G::a_bytes;
 #pragma unroll
                     for (int k = 0; k < BK / 16; k++) {  // 32 bytes of K per instruction
-                        if (CVT) {
+                        if (TRI) {
                             // A hi, A lo, B hi, B lo tiles of 16 KiB: hi*hi + hi*lo + lo*hi
                             auto desc = [&](uint32_t t, int mn) {
                                 return mn ? smem_desc_mn(t + k * 2048) : smem_desc(t + k * 32);
@@ -1771,32 +1178,36 @@ struct Workspace {
 
 // Launches the GEMM: 1-CTA (128x256 tiles) or CTA pairs (256x256 tiles,
 // cluster of 2, cta_group::2) when M spans at least two 128-row halves.
-// cvt: the split-bfloat16 GEMM converting binary32 operands in place (pairs only).
+// load 1: the split-bfloat16 GEMM converting binary32 operands in place;
+// load 2: the split-bfloat16 GEMM from [hi | lo] panels (both pairs only).
 static cudaError_t launch_gemm(int kind, bool cta2, int grid, const CUtensorMap& tmA, const CUtensorMap& tmB,
                                const GemmParams& gp, uint32_t idesc, const CUtensorMap& tmC, const CUtensorMap& tmD,
-                               cudaStream_t s, bool cvt = false)
+                               cudaStream_t s, int load = 0)
 {
     void (*kern)(CUtensorMap, CUtensorMap, GemmParams, uint32_t, CUtensorMap, CUtensorMap);
-    if (cvt)
-        kern = kind == EPI_TMA ? k_gemm<EPI_TMA, true, true> : kind == EPI_F32 ? k_gemm<EPI_F32, true, true>
-               : k_gemm<EPI_ANY, true, true>;
+    if (load == 1)
+        kern = kind == EPI_TMA ? k_gemm<EPI_TMA, true, 1> : kind == EPI_F32 ? k_gemm<EPI_F32, true, 1>
+               : k_gemm<EPI_ANY, true, 1>;
+    else if (load == 2)
+        kern = kind == EPI_TMA ? k_gemm<EPI_TMA, true, 2> : kind == EPI_F32 ? k_gemm<EPI_F32, true, 2>
+               : k_gemm<EPI_ANY, true, 2>;
     else if (cta2)
         kern = kind == EPI_TMA ? k_gemm<EPI_TMA, true> : kind == EPI_F32 ? k_gemm<EPI_F32, true>
                : kind == EPI_I32 ? k_gemm<EPI_I32, true> : k_gemm<EPI_ANY, true>;
     else
         kern = kind == EPI_TMA ? k_gemm<EPI_TMA, false> : kind == EPI_F32 ? k_gemm<EPI_F32, false>
                : kind == EPI_I32 ? k_gemm<EPI_I32, false> : k_gemm<EPI_ANY, false>;
-    static int attr_done[64][4][2][2];
+    static int attr_done[64][4][2][3];
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev < 0 || dev >= 64 || !attr_done[dev][kind][cta2][cvt]) {
+    if (dev < 0 || dev >= 64 || !attr_done[dev][kind][cta2][load]) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
         if (e != cudaSuccess) return e;
-        if (dev >= 0 && dev < 64) attr_done[dev][kind][cta2][cvt] = 1;
+        if (dev >= 0 && dev < 64) attr_done[dev][kind][cta2][load] = 1;
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)grid, 1, 1);
-    cfg.blockDim = dim3(cvt ? 512 : NTHREADS, 1, 1);
+    cfg.blockDim = dim3(load == 1 ? 512 : NTHREADS, 1, 1);
     cfg.dynamicSmemBytes = SMEM_BYTES;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
@@ -1995,41 +1406,67 @@ static bool make_cvt_dim(tc::CvtDim* o, const tb_modes& m, int side)
     return true;
 }
 
-// Whether operand `side` (0 A, 1 B) of a split-bfloat16 product can be read
-// in place by the converter warps, and its description if so: binary32
-// storage, no unary modes, at most 4 row, contracted and batch modes, its
-// contiguous mode first in its row or contracted list with stride 1 and an
-// extent divisible by 8, every other stride divisible by 4, base 16-byte
-// aligned.
-static bool make_cvt_operand(tc::CvtOperand* o, const tb_plan* P, int side, const void* base)
+// Whether operand `side` (0 A, 1 B) of a tensor-core product can be read in
+// place by converter warps, and its description if so: binary32 storage, no
+// unary modes, at most 4 row, contracted and batch modes. vec = 1 (two
+// 16-byte loads per run of 8 elements) when its contiguous mode comes first
+// in its row or contracted list with stride 1 and an extent divisible by 8,
+// every other stride is divisible by 4 and the base is 16-byte aligned;
+// otherwise, with `scalar_ok` (the grouped kernel), vec = 0: element-wise
+// loads through offset tables, any strides.
+static bool make_cvt_operand(tc::CvtOperand* o, const tb_plan* P, int side, const void* base, bool scalar_ok = false)
 {
     using namespace tc;
     const tb_modes& R = side == 0 ? P->M : P->N;
     const tb_modes& U = side == 0 ? P->UA : P->UB;
-    if ((side == 0 ? P->tA : P->tB) != T_F32 || U.n != 0 || !base || ((uintptr_t)base & 15) || R.n < 1 ||
+    if ((side == 0 ? P->tA : P->tB) != T_F32 || U.n != 0 || !base || ((uintptr_t)base & 3) || R.n < 1 ||
         P->K.n < 1)
         return false;
     memset(o, 0, sizeof(*o));
     if (!make_cvt_dim(&o->rows, R, side) || !make_cvt_dim(&o->ks, P->K, side) || !make_cvt_dim(&o->ls, P->L, side))
         return false;
+    o->base = (const float*)base;
     o->mn = min_stride(R, side) < min_stride(P->K, side);
     const CvtDim& fast = o->mn ? o->rows : o->ks;
-    if (fast.st[0] != 1 || fast.div[0].d % 8 != 0) return false;
+    bool vec = ((uintptr_t)base & 15) == 0 && fast.st[0] == 1 && fast.div[0].d % 8 == 0;
     const CvtDim* all[3] = {&o->rows, &o->ks, &o->ls};
-    for (int i = 0; i < 3; i++)
+    for (int i = 0; i < 3 && vec; i++)
         for (int j = 0; j < all[i]->n; j++)
-            if (!(all[i] == &fast && j == 0) && all[i]->st[j] % 4 != 0) return false;
-    o->base = (const float*)base;
-    return true;
+            if (!(all[i] == &fast && j == 0) && all[i]->st[j] % 4 != 0) vec = false;
+    o->vec = vec;
+    return vec || scalar_ok;
 }
 
-// Whether a split-bfloat16 product runs on the converter warps with A and B
-// read in place (CTA pairs: at least 256 rows of A), and their descriptions.
+// Whether a split-bfloat16 product can run on the converter warps with A
+// and B read in place (CTA pairs: at least 256 rows of A), and their
+// descriptions.
 static bool split_in_place(const tb_plan* P, const void* A, const void* B, tc::CvtOperand* ca, tc::CvtOperand* cb)
 {
     return P->path == TB_PATH_TC && P->tc_mode == TB_TC_SPLIT_BF16 && P->compute == TB_R32 &&
            P->M.size >= 2 * tc::BM && tc::num_sms() % 2 == 0 && make_cvt_operand(ca, P, 0, A) &&
            make_cvt_operand(cb, P, 1, B);
+}
+
+// Whether a split-bfloat16 product can run from [hi | lo] panels: a real
+// product on CTA pairs whose operands both go through the real pack (no
+// unary modes, real storage).
+static bool split_panels_ok(const tb_plan* P)
+{
+    auto real = [](int t) { return t == T_F32 || t == T_F64 || t == T_F16 || t == T_BF16; };
+    return P->path == TB_PATH_TC && P->tc_mode == TB_TC_SPLIT_BF16 && P->compute == TB_R32 &&
+           P->M.size >= 2 * tc::BM && tc::num_sms() % 2 == 0 && P->UA.n == 0 && P->UB.n == 0 && real(P->tA) &&
+           real(P->tB);
+}
+
+// Route of a split-bfloat16 product's operands: 1 read in place by the
+// converter warps, 2 [hi | lo] panels, 0 three-segment panels. The
+// automatic choice (split_route 1) prefers the panels where both are
+// possible: the converters are slower on the measured workloads.
+static int split_route(const tb_plan* P, bool in_place_ok)
+{
+    const bool panels = split_panels_ok(P);
+    if (in_place_ok && (P->split_route == 3 || !panels)) return 1;
+    return panels ? 2 : 0;
 }
 
 // Epilogue parameters of one product (or one group of a batched product,
@@ -2058,6 +1495,35 @@ static void fill_epilogue(tc::EpiParams& ep, const tb_plan* P, const void* C, vo
     fill_modes(ep.nn, P->N, 2, 3);
     fill_modes(ep.ll, P->L, 2, 3);
 }
+
+// Descriptor of one product for the grouped kernel (group.cu): a real
+// binary32 product of the tensor-core path (16-bit precisions or split
+// bfloat16) whose operands the converter warps read in place. cta2: 256 x
+// 256 tiles on CTA pairs, else 128 x 128. False when it does not qualify.
+bool group_item(const tb_plan* P, const tb_ptrs* d, bool cta2, tc::GroupItem* g)
+{
+    using namespace tc;
+    if (P->path != TB_PATH_TC || P->compute != TB_R32 ||
+        (P->tc_mode != TB_TC_BF16 && P->tc_mode != TB_TC_F16 && P->tc_mode != TB_TC_SPLIT_BF16))
+        return false;
+    memset(g, 0, sizeof(*g));
+    if (!make_cvt_operand(&g->a, P, 0, d->A, true) || !make_cvt_operand(&g->b, P, 1, d->B, true)) return false;
+    fill_epilogue(g->e, P, d->C, d->D, P->L.size);
+    const int64_t tm = cta2 ? 2 * BM : BM, tn = cta2 ? BN : 128;
+    const int64_t tiles_m = (P->M.size + tm - 1) / tm, tiles_n = (P->N.size + tn - 1) / tn;
+    if (tiles_m * tiles_n * P->L.size >= (1ll << 30)) return false;
+    g->tiles_m = (int32_t)tiles_m;
+    g->tiles_n = (int32_t)tiles_n;
+    g->num_kb = (int32_t)((P->K.size + BK - 1) / BK);
+    g->mode = P->tc_mode;
+    const uint32_t ab = P->tc_mode == TB_TC_F16 ? 0u : 1u;  // operand format: 0 f16, 1 bf16
+    g->idesc = (1u << 4) | (ab << 7) | (ab << 10) | ((uint32_t)g->a.mn << 15) | ((uint32_t)g->b.mn << 16) |
+               ((uint32_t)(tn >> 3) << 17) | ((uint32_t)(tm >> 4) << 24);
+    g->f32_epi = P->tD == T_F32 && (P->beta_zero || P->tC == T_F32) && !P->conjD;
+    return true;
+}
+
+int tc_sm_count() { return tc::num_sms(); }
 
 // A last round that fills at most half the units runs its tiles as two
 // half-contraction items each (partial sums handed over in memory).
@@ -2089,17 +1555,20 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
     // read in place (every batch's A and B 16-byte aligned): no pack
     // launches, no panels
     tc::CvtOperand cva, cvb;
-    bool cvt = split_in_place(P, d[0].A, d[0].B, &cva, &cvb);
-    for (int b = 1; b < num && cvt; b++)
-        if (((uintptr_t)d[b].A & 15) || ((uintptr_t)d[b].B & 15)) cvt = false;
+    bool in_place = split_in_place(P, d[0].A, d[0].B, &cva, &cvb);
+    for (int b = 1; b < num && in_place; b++)
+        if (((uintptr_t)d[b].A & 15) || ((uintptr_t)d[b].B & 15)) in_place = false;
+    const int route = P->tc_mode == TB_TC_SPLIT_BF16 ? split_route(P, in_place) : 0;
+    const bool cvt = route == 1, spl = route == 2;
     using namespace tc;
     *kernels = 0;
     const int cplx = P->compute == TB_C32;
-    const int split = P->tc_mode == TB_TC_SPLIT_BF16 ? 3 : 1;
+    const int split = P->tc_mode == TB_TC_SPLIT_BF16 ? (spl ? 2 : 3) : 1;
     const int fmt = P->tc_mode == TB_TC_F16 ? 1 : 0;
     const int64_t M = P->M.size, N = P->N.size, Lsz = P->L.size, K = P->K.size;
     const int64_t Kreal = K * (cplx ? 2 : 1);
-    const int64_t Kseg = round_up(Kreal, 8);
+    // [hi | lo] panels: each part a whole number of 64-deep blocks (zeros past K)
+    const int64_t Kseg = round_up(Kreal, spl ? 64 : 8);
     const int64_t Kld = Kseg * split;
     const int64_t Nout = N * (cplx ? 2 : 1);
     const size_t bytesA = cvt ? 0 : (size_t)Lsz * M * Kld * 2, bytesB = cvt ? 0 : (size_t)Lsz * Nout * Kld * 2;
@@ -2244,7 +1713,8 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
         gp.tiles_m = (int)((M + (cta2 ? 2 * BM : BM) - 1) / (cta2 ? 2 * BM : BM));
         gp.tiles_n = (int)((Nout + BN - 1) / BN);
         gp.num_tiles = gp.tiles_m * gp.tiles_n * (int)Lg;
-        gp.num_kb = (int)(((cvt ? K : Kld) + BK - 1) / BK);
+        gp.num_kb = (int)(((cvt ? K : spl ? Kseg : Kld) + BK - 1) / BK);
+        gp.lo_off = spl ? (int32_t)Kseg : 0;
         gp.error = flag;
         if (cvt) {
             gp.ca = cva;
@@ -2311,7 +1781,7 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
         const int items = gp.num_tiles + gp.split_tiles;
         const int grid = (items < units ? items : units) * (cta2 ? 2 : 1);
         if (main_timer && b0 == 0) tbk_timer_begin(s, main_timer);
-        e = launch_gemm(kind, cta2, grid, tmA, tmB, gp, idesc, tmC, tmD, s, cvt);
+        e = launch_gemm(kind, cta2, grid, tmA, tmB, gp, idesc, tmC, tmD, s, cvt ? 1 : spl ? 2 : 0);
         if (main_timer && b0 == 0) tbk_timer_end(s, *main_timer);
         if (split_ws) cudaFreeAsync(split_ws, s);
         count_launch();
@@ -2574,15 +2044,22 @@ int tbk_wait_selftest(unsigned long long limit_ns, int* out)
 
 // How the tensor-core path loads a plan's operands when A and B start on
 // 16-byte boundaries: 1 split-bfloat16 read in place by the converter warps
-// (one launch), 0 otherwise. No device call (the SM count is not queried
-// either: B200 has an even number).
+// (one launch), 0 otherwise (packed panels). No kernel launch or copy.
 int tbk_tc_split_in_place(const tb_plan* P)
 {
     tb::tc::CvtOperand ca, cb;
     const void* aligned = (const void*)(uintptr_t)256;
-    return P->path == TB_PATH_TC && P->tc_mode == TB_TC_SPLIT_BF16 && P->compute == TB_R32 &&
-           P->M.size >= 2 * tb::tc::BM && tb::make_cvt_operand(&ca, P, 0, aligned) &&
-           tb::make_cvt_operand(&cb, P, 1, aligned);
+    if (P->path != TB_PATH_TC || P->tc_mode != TB_TC_SPLIT_BF16) return 0;
+    return tb::split_route(P, tb::split_in_place(P, aligned, aligned, &ca, &cb)) == 1;
+}
+
+// Whether a plan can join a grouped tensor-core launch with operands A and B
+// (group.cu). No device call.
+int tbk_tc_groupable(const tb_plan* P, const void* A, const void* B)
+{
+    tb::tc::GroupItem g;
+    tb_ptrs d = {A, B, nullptr, nullptr};
+    return tb::group_item(P, &d, true, &g) ? 1 : 0;
 }
 
 // Reads and clears the error word of the allocation-free path (synchronises).

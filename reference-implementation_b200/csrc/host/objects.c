@@ -147,6 +147,12 @@ TAPP_error TAPP_attr_set(TAPP_attr attr, TAPP_key key, void* value)
         e->f64_mode = v;
         return 0;
     }
+    case TAPP_B200_ATTR_TILE: {
+        const int v = value ? *(int*)value : 0;
+        if (v < 0 || v > 2) return TAPP_B200_ERR_INVALID;
+        e->tile = v;
+        return 0;
+    }
     case TAPP_B200_ATTR_SERVER:
         if (value && !tb_server_is_live((const struct tb_server*)value)) return TAPP_B200_ERR_INVALID;
         e->server = (struct tb_server*)value;
@@ -171,6 +177,7 @@ TAPP_error TAPP_attr_get(TAPP_attr attr, TAPP_key key, void** value)
         case TAPP_B200_ATTR_WANT_STATUS: *(int*)*value = e->want_status; return 0;
         case TAPP_B200_ATTR_SERVER: *value = e->server; return 0;
         case TAPP_B200_ATTR_F64_MODE: *(int*)*value = e->f64_mode; return 0;
+        case TAPP_B200_ATTR_TILE: *(int*)*value = e->tile; return 0;
         default: return TAPP_B200_ERR_INVALID;
         }
     }
@@ -201,6 +208,7 @@ TAPP_error TAPP_attr_clear(TAPP_attr attr, TAPP_key key)
     case TAPP_B200_ATTR_WANT_STATUS: e->want_status = 0; return 0;
     case TAPP_B200_ATTR_SERVER: e->server = NULL; return 0;
     case TAPP_B200_ATTR_F64_MODE: e->f64_mode = 0; return 0;
+    case TAPP_B200_ATTR_TILE: e->tile = 0; return 0;
     default: return TAPP_B200_ERR_INVALID;
     }
 }

@@ -382,7 +382,11 @@ int tb_build_plan(const tb_tensor_view* A, const tb_tensor_view* B,
     if ((P->compute == TB_R32 || P->compute == TB_C32) && ksz > 0) {
         if (prec == TAPP_BF16BF16_ACCUM_F32) { tc_ok = 1; P->tc_mode = TB_TC_BF16; }
         else if (prec == TAPP_F16F16_ACCUM_F32 || prec == TAPP_F16F16_ACCUM_F16) { tc_ok = 1; P->tc_mode = TB_TC_F16; }
-        else if (opt && opt->f32_mode == 1) { tc_ok = 1; P->tc_mode = TB_TC_SPLIT_BF16; }
+        else if (opt && opt->f32_mode >= 1 && opt->f32_mode <= 3) {
+            tc_ok = 1;
+            P->tc_mode = TB_TC_SPLIT_BF16;
+            P->split_route = opt->f32_mode;
+        }
     }
     /* launch limits of the pack grid (z = batch, y = contraction tiles) and the tile count */
     const int64_t kcols = ksz * (P->compute == TB_C32 ? 2 : 1);

@@ -78,6 +78,7 @@ static int resolve_executor(TAPP_executor exec, tb_exec_settings* s)
         s->want_status = e->want_status;
         s->server = e->server;
         s->f64_mode = e->f64_mode;
+        s->tile = e->tile;
         return 0;
     }
     int id = *(const int*)exec;
@@ -533,5 +534,87 @@ TAPP_error tapp_b200_execute_chain(int n, const TAPP_tensor_product* plans, TAPP
     }
     free(inter);
     free(dout);
+    return err;
+}
+
+/* Products of different plans in one call. Products whose plans run on the
+ * tensor cores from binary32 storage, with all operands on the device and
+ * operands the converter warps read in place, run in grouped launches (one
+ * per tile shape, tiles.c); every other product runs as TAPP_execute_product
+ * runs it, on the same stream. Every product is validated before anything
+ * runs (the first failing product's code is returned). The products must be
+ * independent: no D may overlap another product's operands. */
+TAPP_error tapp_b200_execute_group(int n, const TAPP_tensor_product* plans, TAPP_executor exec,
+                                   const void* const* alphas, const void* const* betas, const void* const* A,
+                                   const void* const* B, const void* const* C, void* const* D)
+{
+    if (n < 0 || (n > 0 && (!plans || !alphas || !betas || !A || !B || !D))) return TAPP_B200_ERR_INVALID;
+    if (n == 0) return 0;
+    tb_exec_settings s;
+    int err = resolve_executor(exec, &s);
+    if (err) return err;
+    if (s.server) return TAPP_B200_ERR_INVALID;
+    tb_plan* P = malloc(sizeof(tb_plan) * (size_t)n);
+    int* tile = malloc(sizeof(int) * (size_t)n);
+    const tb_plan** gp = malloc(sizeof(tb_plan*) * (size_t)n);
+    tb_ptrs* gd = malloc(sizeof(tb_ptrs) * (size_t)n);
+    int any_tc = 0;
+    if (!P || !tile || !gp || !gd) {
+        err = TAPP_B200_ERR_NOMEM;
+        goto done;
+    }
+    for (int i = 0; i < n && !err; i++) {
+        struct tb_product* p = (struct tb_product*)plans[i];
+        tile[i] = 0;
+        if (!p || p->magic != TB_MAGIC_PRODUCT || !A[i] || !B[i] || !D[i] || !alphas[i] || !betas[i]) {
+            err = TAPP_B200_ERR_INVALID;
+            break;
+        }
+        tb_tensor_view v[4];
+        err = tb_product_views(p, v);
+        if (!err) err = tb_validate(&v[0], &v[1], &v[2], &v[3], betas[i], C && C[i] != NULL);
+        if (!err) err = tb_product_plan(p, v, alphas[i], betas[i], &s, &P[i]);
+        if (err || P[i].path != TB_PATH_TC || !tbk_tc_groupable(&P[i], A[i], B[i])) continue;
+        const void* q[4] = {A[i], B[i], C ? C[i] : NULL, D[i]};
+        int on_device = 1;
+        for (int k = 0; k < 4 && on_device; k++) {
+            if (!q[k] || (k == 2 && P[i].beta_zero)) continue;
+            int kind = 0, dev = -1;
+            on_device = !tbk_pointer_kind(q[k], &kind, &dev) && (kind == TBK_PTR_DEVICE || kind == TBK_PTR_MANAGED);
+        }
+        if (on_device) tile[i] = s.tile ? s.tile : tb_tile_choice(&P[i]);
+    }
+    if (err) goto done;
+    for (int t = 1; t <= 2 && !err; t++) {
+        int m = 0;
+        for (int i = 0; i < n; i++)
+            if (tile[i] == t) {
+                gp[m] = &P[i];
+                gd[m].A = A[i];
+                gd[m].B = B[i];
+                gd[m].C = P[i].beta_zero ? NULL : (C ? C[i] : NULL);
+                gd[m].D = D[i];
+                m++;
+            }
+        if (!m) continue;
+        any_tc = 1;
+        int64_t tiles = 0;
+        const int e = tbk_run_group_tc_owned(gp, gd, m, t, s.stream, &tiles);
+        if (e) err = cuda_err(e);
+    }
+    for (int i = 0; i < n && !err; i++)
+        if (!tile[i])
+            err = run((struct tb_product*)plans[i], exec, NULL, alphas[i], A[i], B[i], betas[i], C ? C[i] : NULL,
+                      D[i]);
+    if (!err && !s.async) {
+        int e = tbk_stream_sync(s.stream);
+        if (e) err = cuda_err(e);
+        if (!err && any_tc && (e = tbk_check_device_error())) err = cuda_err(e);
+    }
+done:
+    free(P);
+    free(tile);
+    free(gp);
+    free(gd);
     return err;
 }

@@ -38,6 +38,7 @@ struct tb_executor {
     int want_status;
     struct tb_server* server;   /* TAPP_B200_ATTR_SERVER */
     int f64_mode;               /* TAPP_B200_ATTR_F64_MODE */
+    int tile;                   /* TAPP_B200_ATTR_TILE */
 };
 
 struct tb_handle {
@@ -124,7 +125,12 @@ typedef struct tb_exec_settings {
     int async, f32_mode, force_path, want_status;
     struct tb_server* server;
     int f64_mode;
+    int tile;     /* grouped tensor-core tile shape: 0 table / rule, 1 256x256, 2 128x128 */
 } tb_exec_settings;
+
+/* tiles.c: tile shape of a grouped tensor-core product (1: 256 x 256 on CTA
+ * pairs, 2: 128 x 128) from the tuned table, else from the size rule */
+int tb_tile_choice(const tb_plan* P);
 
 int tb_product_views(struct tb_product* p, tb_tensor_view v[4]);
 int tb_product_plan(struct tb_product* p, const tb_tensor_view v[4], const void* alpha, const void* beta,

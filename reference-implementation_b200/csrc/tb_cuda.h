@@ -67,6 +67,21 @@ size_t tbk_scratch_bytes(const tb_plan* plan);
 int tbk_run_group(const tb_plan* const* plans, const tb_ptrs* ptrs, int n, void* host_desc, void* dev_desc,
                   void* stream);
 
+/* Grouped tensor-core products (group.cu): n products of different plans,
+ * each a real binary32 product of the tensor-core path (16-bit precisions or
+ * split bfloat16) whose A and B the converter warps read in place
+ * (tbk_tc_groupable), run in one launch with tile shape `tile` (1: 256 x 256
+ * on CTA pairs, 2: 128 x 128). host_desc is host memory of
+ * tbk_group_tc_bytes(n) that must stay untouched until the stream has run the
+ * copy; dev_desc device memory of the same size. *tiles receives the number
+ * of tiles launched. The _owned form allocates and frees both itself. */
+size_t tbk_group_tc_bytes(int n);
+int tbk_tc_groupable(const tb_plan* plan, const void* A, const void* B);
+int tbk_run_group_tc(const tb_plan* const* plans, const tb_ptrs* ptrs, int n, void* host_desc, void* dev_desc, int tile,
+                     void* stream, int64_t* tiles);
+int tbk_run_group_tc_owned(const tb_plan* const* plans, const tb_ptrs* ptrs, int n, int tile, void* stream,
+                           int64_t* tiles);
+
 long long tbk_launch_count(void);
 long long tbk_allocation_count(void);
 

@@ -26,6 +26,7 @@ INCLUDE_DIR = os.path.join(REPO_DIR, "include")
 # implementation-defined keys and codes (include/tapp_b200.h)
 ERR_CUDA, ERR_LIMIT, ERR_UNSUPPORTED, ERR_NOMEM, ERR_INVALID, ERR_LABELS = 0x1001, 0x1002, 0x1003, 0x1004, 0x1005, 0x1006
 ATTR_STREAM, ATTR_ASYNC, ATTR_F32_MODE, ATTR_PATH, ATTR_WANT_STATUS = 0x1000, 0x1001, 0x1002, 0x1004, 0x1005
+ATTR_F64_MODE, ATTR_TILE = 0x1007, 0x1008
 STATUS_PATH, STATUS_KERNELS, STATUS_FLOPS, STATUS_DEVICE_US, STATUS_TC_MODE, STATUS_MAIN_US = (
     0x1100, 0x1101, 0x1102, 0x1103, 0x1104, 0x1105)
 STATUS_ERR_BOUND = 0x1106
@@ -52,6 +53,10 @@ class B200Lib(TappLib):
         L.tapp_b200_kernel_launches.argtypes = []
         L.tapp_b200_device_allocations.restype = C.c_longlong
         L.tapp_b200_device_allocations.argtypes = []
+        L.tapp_b200_execute_group.restype = C.c_int
+        L.tapp_b200_execute_group.argtypes = [C.c_int, C.POINTER(intptr), intptr] + [C.POINTER(C.c_void_p)] * 6
+        L.tapp_b200_load_tile_table.restype = C.c_int
+        L.tapp_b200_load_tile_table.argtypes = [C.c_char_p]
         L.TAPP_attr_set.restype = C.c_int
         L.TAPP_attr_set.argtypes = [intptr, C.c_int, C.c_void_p]
         L.TAPP_attr_get.restype = C.c_int
@@ -90,6 +95,16 @@ class B200Lib(TappLib):
 
     def allocations(self) -> int:
         return int(self.lib.tapp_b200_device_allocations())
+
+    def execute_group(self, plans, executor, alphas, betas, A, B, Cs, D) -> int:
+        """tapp_b200_execute_group over lists (pointers as ints, Cs may hold None)."""
+        n = len(plans)
+        arr = lambda v: (C.c_void_p * n)(*v)
+        return int(self.lib.tapp_b200_execute_group(n, (intptr * n)(*plans), executor, arr(alphas), arr(betas),
+                                                    arr(A), arr(B), arr(Cs), arr(D)))
+
+    def load_tile_table(self, path: str | None) -> int:
+        return int(self.lib.tapp_b200_load_tile_table(None if path is None else path.encode()))
 
 
 def load() -> B200Lib:

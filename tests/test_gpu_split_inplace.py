@@ -1,15 +1,20 @@
-"""GPU parity of the split-bfloat16 product with binary32 operands read in
-place: the GEMM's converter warps load A and B from their own strided
-layouts, split each value into a bfloat16 high and low part in shared memory
-and run hi*hi + hi*lo + lo*hi on the tensor cores, with no pack launch and no
-operand panels (one kernel per product).
+"""GPU parity of the two operand routes of the split-bfloat16 product
+(float32 products on the tensor cores: hi*hi + hi*lo + lo*hi of bfloat16
+parts, accumulated in binary32):
 
-Operands qualify when their contiguous mode (stride 1, extent divisible by
-8) is a row or a contracted mode, every other stride is divisible by 4 and
-the base is 16-byte aligned; A has at least 256 rows. Each case checks the
-route (the plan description and the kernel count) and the result against the
-oracle's binary64 evaluation with the split-bfloat16 bound (tests/helpers:
-error_bound with 2^-16 relative to |alpha| sum |a||b|).
+  in place (TAPP_B200_ATTR_F32_MODE = 3): the GEMM's converter warps load A
+    and B from their own strided layouts and split each value in shared
+    memory; no pack launch, no operand panels (one kernel per product).
+    Operands qualify when their contiguous mode (stride 1, extent divisible
+    by 8) is a row or a contracted mode, every other stride is divisible by
+    4 and the base is 16-byte aligned; A has at least 256 rows.
+  panels (TAPP_B200_ATTR_F32_MODE = 2, and the automatic mode 1): one pass
+    per operand writes [hi | lo] bfloat16 panels, the GEMM's TMA loads bring
+    both parts of a 64-deep block into one stage (three launches).
+
+Each case checks the route (the plan description and the kernel count) and
+the result against the oracle's binary64 evaluation with the split-bfloat16
+bound (tests/helpers: error_bound with 2^-16 relative to |alpha| sum |a||b|).
 """
 import ctypes as C
 import zlib
@@ -70,10 +75,10 @@ CASES = {
 }
 
 
-def _executor(tapp):
+def _executor(tapp, mode=3):
     ex = tapp.create_executor()
     tapp.set_int(ex, tapp_b200.ATTR_PATH, tapp_b200.PATH_TC)
-    tapp.set_int(ex, tapp_b200.ATTR_F32_MODE, 1)
+    tapp.set_int(ex, tapp_b200.ATTR_F32_MODE, mode)
     tapp.set_int(ex, tapp_b200.ATTR_WANT_STATUS, 1)
     return ex
 
@@ -89,12 +94,14 @@ def _describe(tapp, case, ex):
     return d
 
 
+@pytest.mark.parametrize("mode", [3, 2, 1], ids=["in_place", "panels", "automatic"])
 @pytest.mark.parametrize("name", list(CASES))
-def test_split_in_place(tapp, oracle, gpu, name):
+def test_split_routes(tapp, oracle, gpu, name, mode):
     import torch
     case = CASES[name](np.random.default_rng(zlib.crc32(name.encode())))
-    ex = _executor(tapp)
-    assert "operands=in_place" in _describe(tapp, case, ex)
+    ex = _executor(tapp, mode)
+    in_place = mode == 3
+    assert ("operands=in_place" if in_place else "operands=packed") in _describe(tapp, case, ex)
     run = case.copy()
     dev, ptrs = [], []
     for t in (run.A, run.B, run.C, run.D):
@@ -109,7 +116,8 @@ def test_split_in_place(tapp, oracle, gpu, name):
                                         run.beta.ctypes.data, None if run.C_is_null else ptrs[2], ptrs[3])
     torch.cuda.synchronize()
     assert err == 0, tapp.explain(err)
-    assert tapp.status_value(st.value, tapp_b200.STATUS_KERNELS) == 1  # the GEMM alone
+    # in place: the GEMM alone; panels: a pack per operand and the GEMM
+    assert tapp.status_value(st.value, tapp_b200.STATUS_KERNELS) == (1 if in_place else 3)
     tapp.lib.TAPP_destroy_status(st.value)
     tapp.lib.TAPP_destroy_tensor_product(plan)
     for h in infos:
@@ -139,11 +147,12 @@ def test_split_packed_when_layout_does_not_qualify(tapp, oracle, gpu):
     assert (np.abs(d_values(run.D) - D64) <= bound).all()
 
 
-def test_split_in_place_repeatable(tapp, gpu):
-    """The converters' summation order is fixed: two runs of the same product
-    give the same bits."""
+@pytest.mark.parametrize("mode", [3, 2])
+def test_split_repeatable(tapp, gpu, mode):
+    """The summation order is fixed: two runs of the same product give the
+    same bits (either route)."""
     case = _matmul(np.random.default_rng(5), 512, 256, 512)
-    ex = _executor(tapp)
+    ex = _executor(tapp, mode)
     outs = []
     for _ in range(2):
         run = case.copy()

@@ -230,15 +230,25 @@ def _batched_against_single(tapp, cases, ex, shared=(), misalign=0):
 @pytest.mark.parametrize("prec,split,misalign", [(6, False, 0), (6, False, 1), (5, False, 0), (0, True, 0)])
 def test_batched_product_one_gemm(tapp, gpu, prec, split, misalign):
     """Seven batches of the 4-index contraction (extent 16) run as one pack
-    launch per operand and one GEMM launch (split bfloat16 on 16-byte aligned
-    operands: the GEMM alone, its converter warps reading every batch in
-    place); every batch equals its solo run. misalign = 1 moves every base
-    off 16-byte alignment (scalar pack loads)."""
+    launch per operand and one GEMM launch; every batch equals its solo run.
+    misalign = 1 moves every base off 16-byte alignment (scalar pack loads)."""
     rng = np.random.default_rng(60 + prec)
     cases = [large_dense_case(rng, prec, 0, extent=16) for _ in range(7)]
     ex = tc_executor(tapp, split=split)
     kernels = _batched_against_single(tapp, cases, ex, misalign=misalign)
-    assert kernels == (1 if split and not misalign else 3)
+    assert kernels == 3
+    tapp.lib.TAPP_destroy_executor(ex)
+
+
+def test_batched_split_in_place_one_launch(tapp, gpu):
+    """Split bfloat16 with the operands read in place (TAPP_B200_ATTR_F32_MODE
+    = 3): seven batches in one GEMM launch (no pack), each equal to its solo
+    run."""
+    rng = np.random.default_rng(66)
+    cases = [large_dense_case(rng, 0, 0, extent=16) for _ in range(7)]
+    ex = tc_executor(tapp)
+    tapp.set_int(ex, tapp_b200.ATTR_F32_MODE, 3)
+    assert _batched_against_single(tapp, cases, ex) == 1
     tapp.lib.TAPP_destroy_executor(ex)
 
 
