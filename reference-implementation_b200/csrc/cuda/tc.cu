@@ -2062,6 +2062,23 @@ int tbk_tc_groupable(const tb_plan* P, const void* A, const void* B)
     return tb::group_item(P, &d, true, &g) ? 1 : 0;
 }
 
+// Whether the grouped kernel computes the same bits for a plan as the
+// single-product path (TAPP_execute_product) does: the same operand values,
+// the same order of MMAs along the contraction and the same epilogue. That
+// holds unless the single product would run its split bfloat16 from
+// three-segment panels (fewer than 256 rows) or hand a last round of tiles
+// over as half contractions (more tiles than SM units). No device call.
+int tbk_tc_group_same_as_solo(const tb_plan* P)
+{
+    using namespace tb;
+    using namespace tb::tc;
+    if (P->tc_mode == TB_TC_SPLIT_BF16 && !split_panels_ok(P)) return 0;
+    const bool cta2 = P->M.size >= 2 * BM && num_sms() % 2 == 0;
+    const int64_t tiles = ((P->M.size + (cta2 ? 2 * BM : BM) - 1) / (cta2 ? 2 * BM : BM)) *
+                          ((P->N.size + BN - 1) / BN) * P->L.size;
+    return tiles <= (cta2 ? num_sms() / 2 : num_sms());
+}
+
 // Reads and clears the error word of the allocation-free path (synchronises).
 int tbk_noalloc_check_error(void)
 {

@@ -538,7 +538,7 @@ __device__ __forceinline__ const float* cvt_rows(const CvtOperand& o, int64_t ro
 __device__ __forceinline__ float4 ld_nc_v4(const float* p)
 {
     float4 v;
-    asm volatile("ld.global.nc.L1::no_allocate.v4.f32 {%0,%1,%2,%3}, [%4];"
+    asm volatile("ld.global.nc.v4.f32 {%0,%1,%2,%3}, [%4];"
                  : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
                  : "l"(p));
     return v;

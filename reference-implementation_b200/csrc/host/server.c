@@ -16,7 +16,11 @@
  *              fewer than max_in_flight are running;
  *   issue      admitted products of the CUDA-core element path with modest
  *              work are packed into one grouped launch per compute domain
- *              (tbk_run_group); every other product is a unit of its own.
+ *              (tbk_run_group); admitted tensor-core products of binary32
+ *              storage into one grouped tensor-core launch per tile shape
+ *              (tbk_run_group_tc, operands read in place), where that
+ *              launch gives the same bits as the product alone; every other
+ *              product is a unit of its own.
  *              Units are spread round-robin over the server's streams, each
  *              as: staging copies in, kernel(s), copy of D out, frees, and a
  *              stream callback;
@@ -97,6 +101,7 @@ struct tb_server {
 typedef struct srv_unit {
     struct tb_server* srv;
     int n, slab, err;
+    int tc_tile;     /* grouped tensor-core unit: its tile shape (1, 2); 0 otherwise */
     srv_req* req[SRV_GROUP_MAX];
 } srv_unit;
 
@@ -252,9 +257,12 @@ static void issue(struct tb_server* s, srv_unit* u)
             for (int i = 0; i < u->n; i++) plans[i] = &u->req[i]->P;
             u->slab = take_slab(s);
             void* ddesc = NULL;
-            e = tbk_malloc(&ddesc, tbk_group_bytes(u->n), stream);
+            const size_t bytes = u->tc_tile ? tbk_group_tc_bytes(u->n) : tbk_group_bytes(u->n);
+            e = tbk_malloc(&ddesc, bytes, stream);
             if (!e) {
-                e = tbk_run_group(plans, dp, u->n, s->slab[u->slab], ddesc, stream);
+                int64_t tiles = 0;
+                e = u->tc_tile ? tbk_run_group_tc(plans, dp, u->n, s->slab[u->slab], ddesc, u->tc_tile, stream, &tiles)
+                               : tbk_run_group(plans, dp, u->n, s->slab[u->slab], ddesc, stream);
                 tbk_free(ddesc, stream);
             }
         }
@@ -275,6 +283,16 @@ static void issue(struct tb_server* s, srv_unit* u)
         if (!u->err) u->err = TAPP_B200_ERR_CUDA;
         unit_done(u);
     }
+}
+
+/* a tensor-core product that a grouped launch runs with the same result as
+ * alone: its tile shape (1, 2), else 0 */
+static int tc_groupable(const struct tb_server* s, const srv_req* r)
+{
+    const tb_plan* P = &r->P;
+    if (P->path != TB_PATH_TC || !tbk_tc_groupable(P, r->ptr[0], r->ptr[1]) || !tbk_tc_group_same_as_solo(P))
+        return 0;
+    return s->settings.tile ? s->settings.tile : tb_tile_choice(P);
 }
 
 static int groupable(const tb_plan* P)
@@ -317,10 +335,25 @@ static void fail_now(struct tb_server* s, srv_req* r, int err)
 static void dispatch(struct tb_server* s, srv_req* batch)
 {
     srv_unit* group[4] = {NULL, NULL, NULL, NULL};
+    srv_unit* tcg[3] = {NULL, NULL, NULL};  /* grouped tensor-core units by tile shape */
     while (batch) {
         srv_req* r = batch;
         batch = r->next;
         r->next = NULL;
+        const int tile = tc_groupable(s, r);
+        if (tile) {
+            if (!tcg[tile] && !(tcg[tile] = new_unit(s))) {
+                fail_now(s, r, TAPP_B200_ERR_NOMEM);
+                continue;
+            }
+            tcg[tile]->tc_tile = tile;
+            tcg[tile]->req[tcg[tile]->n++] = r;
+            if (tcg[tile]->n == SRV_GROUP_MAX) {
+                issue(s, tcg[tile]);
+                tcg[tile] = NULL;
+            }
+            continue;
+        }
         if (groupable(&r->P)) {
             const int c = r->P.compute & 3;
             if (!group[c] && !(group[c] = new_unit(s))) {
@@ -344,6 +377,8 @@ static void dispatch(struct tb_server* s, srv_req* batch)
     }
     for (int c = 0; c < 4; c++)
         if (group[c]) issue(s, group[c]);
+    for (int t = 1; t <= 2; t++)
+        if (tcg[t]) issue(s, tcg[t]);
 }
 
 static int admissible(const struct tb_server* s)
@@ -507,6 +542,7 @@ TAPP_error tapp_b200_server_create(TAPP_b200_server* server, TAPP_executor exec,
         const struct tb_executor* x = (const struct tb_executor*)exec;
         s->settings.f32_mode = x->f32_mode;
         s->settings.force_path = x->force_path;
+        s->settings.tile = x->tile;
     }
     pthread_mutex_init(&s->lock, NULL);
     pthread_cond_init(&s->cv_sched, NULL);
@@ -515,6 +551,7 @@ TAPP_error tapp_b200_server_create(TAPP_b200_server* server, TAPP_executor exec,
     for (int i = 0; i < n_streams && !err; i++)
         if ((e = tbk_stream_create(&s->streams[i]))) err = cuda_code(e);
     s->slab_bytes = tbk_group_bytes(SRV_GROUP_MAX);
+    if (tbk_group_tc_bytes(SRV_GROUP_MAX) > s->slab_bytes) s->slab_bytes = tbk_group_tc_bytes(SRV_GROUP_MAX);
     s->n_slabs = n_streams * SRV_SLABS_PER_STREAM;
     for (int i = 0; i < s->n_slabs && !err; i++) {
         if ((e = tbk_host_alloc(&s->slab[i], s->slab_bytes))) err = cuda_code(e);

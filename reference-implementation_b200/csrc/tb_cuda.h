@@ -77,6 +77,7 @@ int tbk_run_group(const tb_plan* const* plans, const tb_ptrs* ptrs, int n, void*
  * of tiles launched. The _owned form allocates and frees both itself. */
 size_t tbk_group_tc_bytes(int n);
 int tbk_tc_groupable(const tb_plan* plan, const void* A, const void* B);
+int tbk_tc_group_same_as_solo(const tb_plan* plan);
 int tbk_run_group_tc(const tb_plan* const* plans, const tb_ptrs* ptrs, int n, void* host_desc, void* dev_desc, int tile,
                      void* stream, int64_t* tiles);
 int tbk_run_group_tc_owned(const tb_plan* const* plans, const tb_ptrs* ptrs, int n, int tile, void* stream,
