@@ -80,6 +80,7 @@ def parse():
     ap.add_argument("--only-batched", action="store_true", help="print only the batched-product measurement")
     ap.add_argument("--only-chain", action="store_true", help="print only the Tucker-chain measurement")
     ap.add_argument("--only-tucker", action="store_true", help="print only the Tucker mode-n measurement")
+    ap.add_argument("--only-tiny", action="store_true", help="print only the small-product latency measurement")
     ap.add_argument("--slices", type=str, default="7,8", help="digit slices of the sliced binary64 runs")
     ap.add_argument("--double-ab", type=int, default=160, help="extent of a, b, e, f in the binary64 workload")
     ap.add_argument("--double-ij", type=int, default=40, help="extent of i, j in the binary64 workload")
@@ -527,6 +528,93 @@ def small_configs_measure(lib, torch, with_cpu=True, steps=200, e2e_calls=50):
     return out
 
 
+def tiny_latency_measure(lib, torch, n=2000):
+    """Latency of small products (the element path: the mixed-class
+    configuration, complex float with Hadamard, diagonal and unary modes, and
+    4-index contractions with extents 4, binary32 and binary64), operands in
+    HBM, one product at a time (submit, then wait for it):
+      plain   synchronous TAPP_execute_product (a launch and a stream wait)
+      server  tapp_b200_server_submit + wait (host scheduler thread, streams,
+              stream callbacks)
+      loop    tapp_b200_loop_submit + wait (the device-resident loop: no
+              launch per product)
+    and the throughput of `n` products submitted back to back then waited."""
+    from tapp_b200.workloads import dense_contraction_case, mixed_classes_case
+    from tapp_b200.server import Server
+    rng = np.random.default_rng(17)
+    cases = [mixed_classes_case(np.random.default_rng(0x7A990002)),
+             dense_contraction_case(rng, extent=4), dense_contraction_case(rng, extent=4, dtype=1, prec=1)]
+    devs = []
+    for c in cases:
+        ts = (c.A, c.B, c.C, c.D)
+        bufs = [to_device(t, torch) for t in ts]
+        infos = [lib.tensor_info(t.dtype, t.extents, t.strides)[1] for t in ts]
+        err, plan = lib.create_product(0, [t.op for t in ts], infos, [t.idx for t in ts], c.prec)
+        assert err == 0
+        devs.append((c, bufs, infos, plan))
+    args = lambda d: (d[0].alpha.ctypes.data, d[1][0][1], d[1][1][1], d[0].beta.ctypes.data, d[1][2][1], d[1][3][1])
+    order = [devs[i % len(devs)] for i in range(n)]
+    out = {"workload": "small element-path products (mixed-class complex float; 4-index contractions, extents 4, "
+                       "f32 and f64), operands in HBM", "products": n}
+    # plain
+    ex = lib.create_executor()
+    lat = []
+    for d in order[:200]:
+        a = args(d)
+        st = C.c_ssize_t(0)
+        lib.lib.TAPP_execute_product(d[3], ex, C.byref(st), *a)
+    for d in order:
+        a = args(d)
+        st = C.c_ssize_t(0)
+        t0 = time.perf_counter()
+        lib.lib.TAPP_execute_product(d[3], ex, C.byref(st), *a)
+        lat.append(time.perf_counter() - t0)
+    lib.lib.TAPP_destroy_executor(ex)
+    lat = np.array(lat) * 1e6
+    out["plain"] = {"p50_us": float(np.percentile(lat, 50)), "p99_us": float(np.percentile(lat, 99))}
+    # server, one at a time, then all at once
+    with Server(lib, 8 << 30, n_streams=4, max_in_flight=64) as srv:
+        for d in order[:200]:
+            srv.wait(srv.submit(d[3], *args(d))[1])
+        srv.reset_stats()
+        for d in order:
+            err, t = srv.submit(d[3], *args(d))
+            srv.wait(t)
+        one = srv.stats()
+        srv.reset_stats()
+        t0 = time.perf_counter()
+        for d in order:
+            srv.submit(d[3], *args(d))
+        srv.drain()
+        burst_s = time.perf_counter() - t0
+    out["server"] = {"p50_us": one["p50_us"], "p99_us": one["p99_us"], "burst_products_per_s": n / burst_s}
+    # device loop
+    err, loop = lib.loop_create(0, blocks=8, slots=256, idle_ms=100.0)
+    assert err == 0
+    for d in order[:200]:
+        lib.lib.tapp_b200_loop_wait(loop, lib.loop_submit(loop, d[3], *args(d))[1])
+    lib.lib.tapp_b200_loop_reset_stats(loop)
+    for d in order:
+        err, t = lib.loop_submit(loop, d[3], *args(d))
+        lib.lib.tapp_b200_loop_wait(loop, t)
+    one = lib.loop_stats(loop)
+    lib.lib.tapp_b200_loop_reset_stats(loop)
+    t0 = time.perf_counter()
+    tickets = [lib.loop_submit(loop, d[3], *args(d))[1] for d in order]
+    for t in tickets:
+        lib.lib.tapp_b200_loop_wait(loop, t)
+    burst_s = time.perf_counter() - t0
+    out["loop"] = {"p50_us": one["p50_us"], "p99_us": one["p99_us"], "burst_products_per_s": n / burst_s,
+                   "launches": one["launches"]}
+    lib.lib.tapp_b200_loop_destroy(loop)
+    out["loop_vs_server_p50"] = out["server"]["p50_us"] / out["loop"]["p50_us"]
+    for c, bufs, infos, plan in devs:
+        lib.lib.TAPP_destroy_tensor_product(plan)
+        for h in infos:
+            lib.lib.TAPP_destroy_tensor_info(h)
+    return out
+
+
 def hbm_peak():
     try:
         with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
@@ -841,6 +929,10 @@ def run_b200(args):
         if rank == 0:
             print(json.dumps(tucker_measure(lib, torch)), flush=True)
         return
+    if args.only_tiny:
+        if rank == 0:
+            print(json.dumps(tiny_latency_measure(lib, torch)), flush=True)
+        return
     if args.only_batched:
         if rank == 0:
             print(json.dumps(batched_measure(lib, torch)), flush=True)
@@ -961,6 +1053,7 @@ def run_b200(args):
     batched = batched_measure(lib, torch) if world == 1 and not args.no_modes else None
     chain = chain_measure(lib, torch) if world == 1 and not args.no_modes else None
     tucker = tucker_measure(lib, torch) if world == 1 and not args.no_modes else None
+    tiny = tiny_latency_measure(lib, torch) if world == 1 and not args.no_modes else None
     double = None
     if world == 1 and not args.no_double:
         double = double_measure(lib, torch, slices)
@@ -986,7 +1079,7 @@ def run_b200(args):
                 "error_reference": "binary64 evaluation of D[:,:,:,0:2] from the same stored inputs",
                 "vs_plain_gpu": (value / world / plain) if plain else None,
                 "modes": modes, "small_configs": small, "batched": batched, "tucker_chain": chain,
-                "tucker": tucker, "double": double, "served": served, "roofline": roofline, "e2e": e2e,
+                "tucker": tucker, "tiny_latency": tiny, "double": double, "served": served, "roofline": roofline, "e2e": e2e,
                 "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": gpu_launches}
         print(json.dumps(line), flush=True)
     prod.close()

@@ -222,6 +222,40 @@ TAPP_EXPORT TAPP_error tapp_b200_execute_group(int n, const TAPP_tensor_product*
 TAPP_EXPORT TAPP_error tapp_b200_load_tile_table(const char* path);
 
 /*
+ * A device-resident request loop for small products (no counterpart in the
+ * reference, whose handle and executor are placeholders): a persistent
+ * kernel of `blocks` blocks stays on the GPU and computes products as they
+ * are submitted, with no kernel launch per product. Submission writes the
+ * product's descriptor into a ring of `slots` entries in page-locked host
+ * memory mapped into the device; the loop polls it, computes D, and marks
+ * the entry done. After idle_ms without products the kernel returns (it
+ * never spins without a bound); the next submission or wait launches it
+ * again. Products must plan to the element path (small products) and have
+ * device operands: TAPP_B200_ERR_UNSUPPORTED / TAPP_B200_ERR_INVALID
+ * otherwise. Results equal TAPP_execute_product's bit for bit. Calls that
+ * synchronise the whole device (cudaDeviceSynchronize) wait for the loop's
+ * idle return. Destroy waits for the loop to return, then frees it.
+ */
+typedef intptr_t TAPP_b200_loop;
+
+typedef struct tapp_b200_loop_counters {
+    int64_t submitted, completed, launches;  /* launches: kernel starts (the first and every restart after idle) */
+    int32_t running, pad;                    /* 1 while a launch is on the GPU */
+    double p50_us, p99_us, mean_us, max_us;  /* submission to the wait that saw the product done */
+} tapp_b200_loop_counters;
+
+TAPP_EXPORT TAPP_error tapp_b200_loop_create(TAPP_b200_loop* loop, TAPP_executor exec, int blocks, int slots,
+                                             double idle_ms);
+TAPP_EXPORT TAPP_error tapp_b200_loop_submit(TAPP_b200_loop loop, TAPP_tensor_product plan, const void* alpha,
+                                             const void* A, const void* B, const void* beta, const void* C, void* D,
+                                             int64_t* ticket);
+/* Returns once the product of `ticket` is done (30 s at most: TAPP_B200_ERR_CUDA). */
+TAPP_EXPORT TAPP_error tapp_b200_loop_wait(TAPP_b200_loop loop, int64_t ticket);
+TAPP_EXPORT TAPP_error tapp_b200_loop_stats(TAPP_b200_loop loop, tapp_b200_loop_counters* out);
+TAPP_EXPORT TAPP_error tapp_b200_loop_reset_stats(TAPP_b200_loop loop);
+TAPP_EXPORT TAPP_error tapp_b200_loop_destroy(TAPP_b200_loop loop);
+
+/*
  * Serving: a request loop that runs products as they arrive on one GPU.
  * There is no counterpart in the reference (its handle and executor are
  * placeholders).

@@ -422,3 +422,147 @@ cudaError_t launch_generic(const tb_plan* P, const tb_ptrs* d, cudaStream_t s)
 }
 
 }  // namespace tb
+
+// ---------------------------------------------------------------------------
+// Device-resident request loop (host side: host/loop.c). A persistent kernel
+// of G blocks serves small products as they arrive, without a launch per
+// product: the host writes product t's descriptor into slot t % R of a ring
+// in page-locked host memory mapped into the device, then the slot's
+// sequence word (t + 1) last. Block t % G polls that word (system-scope
+// acquire loads, with a short sleep between polls), copies the descriptor
+// into shared memory, computes every element of D with the element kernel's
+// own per-output function (so the bits equal TAPP_execute_product's on the
+// element path), and publishes t + 1 in the slot's completion word
+// (system-scope release after a system fence). A block that finds no posted
+// product for idle_ns stores the ticket it waits for in device memory and
+// returns, so the loop never spins without a bound; the host relaunches it
+// when products arrive again and the last launch has ended.
+namespace tb {
+
+struct LoopSlot {
+    GenParams p;
+    tb_ptrs q;
+    int32_t compute;
+    int32_t pad;
+    int64_t seq;     // t + 1 once the descriptor of ticket t is complete (written last)
+    int64_t done;    // t + 1 once ticket t's D is written
+    int64_t pad2[6];
+};
+
+struct LoopParams {
+    LoopSlot* slots;      // device pointer of the mapped ring
+    int64_t* next;        // device memory: per block, the ticket it serves next
+    int32_t nslots;
+    int32_t pad;
+    unsigned long long idle_ns;
+};
+
+__device__ __forceinline__ unsigned long long loop_now_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ int64_t ld_acquire_sys(const int64_t* p)
+{
+    int64_t v;
+    asm volatile("ld.acquire.sys.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release_sys(int64_t* p, int64_t v)
+{
+    asm volatile("st.release.sys.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+template <typename R, bool CPLX>
+__device__ __forceinline__ void loop_product(const GenParams& p, const tb_ptrs& q)
+{
+    for (int64_t i = threadIdx.x; i < p.sizeF; i += blockDim.x) element<R, CPLX>(p, q.A, q.B, q.C, q.D, i);
+}
+
+__global__ void __launch_bounds__(256) k_request_loop(LoopParams lp)
+{
+    __shared__ GenParams sp;
+    __shared__ tb_ptrs sq;
+    __shared__ int scomp, go;
+    const int b = blockIdx.x;
+    int64_t t = lp.next[b];
+    unsigned long long last = loop_now_ns();
+    for (;;) {
+        LoopSlot* sl = &lp.slots[t % lp.nslots];
+        if (threadIdx.x == 0) {
+            int posted = 0;
+            for (;;) {
+                if (ld_acquire_sys(&sl->seq) == t + 1) {
+                    posted = 1;
+                    break;
+                }
+                if (loop_now_ns() - last > lp.idle_ns) break;
+                __nanosleep(256);
+            }
+            go = posted;
+        }
+        __syncthreads();
+        if (!go) break;
+        // the descriptor, 8 bytes per thread and step, from host memory
+        {
+            const volatile int64_t* src = (const volatile int64_t*)&sl->p;
+            int64_t* dst = (int64_t*)&sp;
+            for (int w = threadIdx.x; w < (int)(sizeof(GenParams) / 8); w += blockDim.x) dst[w] = src[w];
+            if (threadIdx.x == 0) {
+                const volatile tb_ptrs* vq = &sl->q;
+                sq.A = vq->A;
+                sq.B = vq->B;
+                sq.C = vq->C;
+                sq.D = vq->D;
+                scomp = *(const volatile int32_t*)&sl->compute;
+            }
+        }
+        __syncthreads();
+        switch (scomp) {
+        case TB_R32: loop_product<float, false>(sp, sq); break;
+        case TB_R64: loop_product<double, false>(sp, sq); break;
+        case TB_C32: loop_product<float, true>(sp, sq); break;
+        default: loop_product<double, true>(sp, sq); break;
+        }
+        __syncthreads();  // every output of the product written
+        if (threadIdx.x == 0) {
+            __threadfence_system();
+            st_release_sys(&sl->done, t + 1);
+        }
+        t += gridDim.x;
+        last = loop_now_ns();
+    }
+    if (threadIdx.x == 0) lp.next[b] = t;
+}
+
+size_t loop_slot_bytes() { return sizeof(LoopSlot); }
+
+// Fills ring slot `slot` (host memory) with a product's descriptor, all
+// but the sequence word.
+void loop_fill(void* slot, const tb_plan* P, const tb_ptrs* d)
+{
+    LoopSlot* s = (LoopSlot*)slot;
+    fill_params(P, s->p);
+    if (P->path == TB_PATH_NOOP) s->p.sizeF = 0;  // nothing to write (empty D, or a precision left as is)
+    s->q = *d;
+    s->compute = P->compute;
+}
+
+cudaError_t loop_launch(void* slots_dev, int64_t* next, int nslots, int blocks, unsigned long long idle_ns,
+                        cudaStream_t s)
+{
+    LoopParams lp;
+    lp.slots = (LoopSlot*)slots_dev;
+    lp.next = next;
+    lp.nslots = nslots;
+    lp.pad = 0;
+    lp.idle_ns = idle_ns;
+    k_request_loop<<<blocks, 256, 0, s>>>(lp);
+    count_launch();
+    return cudaGetLastError();
+}
+
+}  // namespace tb

@@ -5,6 +5,8 @@
 
 #include <atomic>
 #include <cstdio>
+#include <cstdlib>
+#include <cstring>
 #include <mutex>
 
 #include "../tb_cuda.h"
@@ -131,6 +133,10 @@ size_t reduce_scratch_bytes(const tb_plan* P, size_t real_bytes);
 cudaError_t launch_generic_group(const tb_plan* const* P, const tb_ptrs* d, int n, void* host, void* dev,
                                  cudaStream_t s);
 size_t group_tc_bytes(int n);
+size_t loop_slot_bytes();
+void loop_fill(void* slot, const tb_plan* P, const tb_ptrs* d);
+cudaError_t loop_launch(void* slots_dev, int64_t* next, int nslots, int blocks, unsigned long long idle_ns,
+                        cudaStream_t s);
 cudaError_t launch_group_tc(const tb_plan* const* P, const tb_ptrs* d, int n, void* host, void* dev, int tile,
                             cudaStream_t s, int64_t* tiles_out);
 
@@ -398,6 +404,67 @@ int tbk_run_group(const tb_plan* const* plans, const tb_ptrs* ptrs, int n, void*
             return (int)cudaErrorInvalidValue;
     return (int)tb::launch_generic_group(plans, ptrs, n, host_desc, dev_desc, (cudaStream_t)stream);
 }
+
+// ---- device-resident request loop (host/loop.c) ----
+size_t tbk_loop_slot_bytes(void) { return tb::loop_slot_bytes(); }
+void tbk_loop_fill(void* slot, const tb_plan* P, const tb_ptrs* d) { tb::loop_fill(slot, P, d); }
+
+// page-locked host memory mapped into the device's address space
+int tbk_host_alloc_mapped(void** host, void** dev, size_t bytes)
+{
+    tb::count_allocation();
+    cudaError_t e = cudaHostAlloc(host, bytes, cudaHostAllocMapped);
+    if (e != cudaSuccess) return (int)e;
+    memset(*host, 0, bytes);
+    e = cudaHostGetDevicePointer(dev, *host, 0);
+    if (e != cudaSuccess) {
+        cudaFreeHost(*host);
+        *host = nullptr;
+    }
+    return (int)e;
+}
+
+// the per-block ticket counters of a loop of `blocks` blocks, block b starting at ticket b
+int tbk_loop_counters(int64_t** next, int blocks)
+{
+    tb::count_allocation();
+    cudaError_t e = cudaMalloc((void**)next, sizeof(int64_t) * (size_t)blocks);
+    if (e != cudaSuccess) return (int)e;
+    int64_t init[256];
+    for (int b = 0; b < blocks && b < 256; b++) init[b] = b;
+    return (int)cudaMemcpy(*next, init, sizeof(int64_t) * (size_t)blocks, cudaMemcpyHostToDevice);
+}
+
+// launches the loop on `stream` and records `*event` (created on first use) after it
+int tbk_loop_launch(void* slots_dev, int64_t* next, int nslots, int blocks, unsigned long long idle_ns, void* stream,
+                    void** event)
+{
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = cudaSuccess;
+    if (!*event) e = cudaEventCreateWithFlags((cudaEvent_t*)event, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = tb::loop_launch(slots_dev, next, nslots, blocks, idle_ns, s);
+    if (e == cudaSuccess) e = cudaEventRecord((cudaEvent_t)*event, s);
+    return (int)e;
+}
+
+// 1 when the work before the event has run, 0 while it runs, a negative code on error
+int tbk_event_done(void* event)
+{
+    cudaError_t e = cudaEventQuery((cudaEvent_t)event);
+    if (e == cudaSuccess) return 1;
+    if (e == cudaErrorNotReady) {
+        (void)cudaGetLastError();
+        return 0;
+    }
+    return -(int)e;
+}
+
+void tbk_event_destroy(void* event)
+{
+    if (event) cudaEventDestroy((cudaEvent_t)event);
+}
+
+int tbk_dev_free(void* p) { return (int)cudaFree(p); }
 
 long long tbk_launch_count(void) { return tb::g_launches.load(); }
 long long tbk_allocation_count(void) { return tb::g_allocations.load(); }

@@ -41,6 +41,13 @@ def build(jobs: int = 8) -> str:
     return LIB_PATH
 
 
+class LoopCounters(C.Structure):
+    """tapp_b200_loop_counters (include/tapp_b200.h)."""
+    _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("launches", C.c_int64),
+                ("running", C.c_int32), ("pad", C.c_int32), ("p50_us", C.c_double), ("p99_us", C.c_double),
+                ("mean_us", C.c_double), ("max_us", C.c_double)]
+
+
 class B200Lib(TappLib):
     """TappLib plus the implementation-defined entry points."""
 
@@ -57,6 +64,15 @@ class B200Lib(TappLib):
         L.tapp_b200_execute_group.argtypes = [C.c_int, C.POINTER(intptr), intptr] + [C.POINTER(C.c_void_p)] * 6
         L.tapp_b200_load_tile_table.restype = C.c_int
         L.tapp_b200_load_tile_table.argtypes = [C.c_char_p]
+        for name, args in (("tapp_b200_loop_create", [C.POINTER(intptr), intptr, C.c_int, C.c_int, C.c_double]),
+                           ("tapp_b200_loop_submit", [intptr, intptr] + [C.c_void_p] * 6 + [C.POINTER(C.c_int64)]),
+                           ("tapp_b200_loop_wait", [intptr, C.c_int64]),
+                           ("tapp_b200_loop_stats", [intptr, C.POINTER(LoopCounters)]),
+                           ("tapp_b200_loop_reset_stats", [intptr]),
+                           ("tapp_b200_loop_destroy", [intptr])):
+            f = getattr(L, name)
+            f.restype = C.c_int
+            f.argtypes = args
         L.TAPP_attr_set.restype = C.c_int
         L.TAPP_attr_set.argtypes = [intptr, C.c_int, C.c_void_p]
         L.TAPP_attr_get.restype = C.c_int
@@ -102,6 +118,21 @@ class B200Lib(TappLib):
         arr = lambda v: (C.c_void_p * n)(*v)
         return int(self.lib.tapp_b200_execute_group(n, (intptr * n)(*plans), executor, arr(alphas), arr(betas),
                                                     arr(A), arr(B), arr(Cs), arr(D)))
+
+    def loop_create(self, executor=0, blocks=4, slots=256, idle_ms=100.0) -> tuple[int, int]:
+        h = intptr(0)
+        err = self.lib.tapp_b200_loop_create(C.byref(h), executor, blocks, slots, idle_ms)
+        return err, h.value
+
+    def loop_submit(self, loop, plan, alpha_ptr, A, B, beta_ptr, Cp, D) -> tuple[int, int]:
+        t = C.c_int64(-1)
+        err = self.lib.tapp_b200_loop_submit(loop, plan, alpha_ptr, A, B, beta_ptr, Cp, D, C.byref(t))
+        return err, t.value
+
+    def loop_stats(self, loop) -> dict:
+        c = LoopCounters()
+        assert self.lib.tapp_b200_loop_stats(loop, C.byref(c)) == 0
+        return {f: getattr(c, f) for f, _ in LoopCounters._fields_ if f != "pad"}
 
     def load_tile_table(self, path: str | None) -> int:
         return int(self.lib.tapp_b200_load_tile_table(None if path is None else path.encode()))
