@@ -426,17 +426,20 @@ cudaError_t launch_generic(const tb_plan* P, const tb_ptrs* d, cudaStream_t s)
 // ---------------------------------------------------------------------------
 // Device-resident request loop (host side: host/loop.c). A persistent kernel
 // of G blocks serves small products as they arrive, without a launch per
-// product: the host writes product t's descriptor into slot t % R of a ring
+// product. The host writes product t's descriptor into slot t % R of a ring
 // in page-locked host memory mapped into the device, then the slot's
-// sequence word (t + 1) last. Block t % G polls that word (system-scope
-// acquire loads, with a short sleep between polls), copies the descriptor
-// into shared memory, computes every element of D with the element kernel's
-// own per-output function (so the bits equal TAPP_execute_product's on the
-// element path), and publishes t + 1 in the slot's completion word
-// (system-scope release after a system fence). A block that finds no posted
-// product for idle_ns stores the ticket it waits for in device memory and
-// returns, so the loop never spins without a bound; the host relaunches it
-// when products arrive again and the last launch has ended.
+// sequence word (t + 1) last. Block 0 polls that word (system-scope acquire
+// loads, a short sleep between polls), copies the descriptor into the same
+// slot of a ring in device memory and raises its device sequence word; the
+// other blocks poll the device word (an L2 read instead of a PCIe read).
+// Every block then computes its share of D's elements (element i on block
+// i / 256 mod G) with the element kernel's own per-output function, so the
+// bits equal TAPP_execute_product's on the element path; the last block to
+// finish (an arrival counter per slot) publishes t + 1 in the host slot's
+// completion word after a system fence. A block that sees no new product for
+// idle_ns stores the ticket it waits for in device memory and returns, so
+// the loop never spins without a bound; the host relaunches it when
+// products arrive again and the last launch has ended.
 namespace tb {
 
 struct LoopSlot {
@@ -451,6 +454,9 @@ struct LoopSlot {
 
 struct LoopParams {
     LoopSlot* slots;      // device pointer of the mapped ring
+    LoopSlot* dslots;     // ring in device memory: block 0's copies
+    int64_t* dseq;        // device memory: t + 1 once dslots[t % R] holds ticket t
+    int* arrive;          // device memory: blocks done with the slot's current ticket
     int64_t* next;        // device memory: per block, the ticket it serves next
     int32_t nslots;
     int32_t pad;
@@ -471,15 +477,29 @@ __device__ __forceinline__ int64_t ld_acquire_sys(const int64_t* p)
     return v;
 }
 
+__device__ __forceinline__ int64_t ld_acquire_gpu(const int64_t* p)
+{
+    int64_t v;
+    asm volatile("ld.acquire.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
 __device__ __forceinline__ void st_release_sys(int64_t* p, int64_t v)
 {
     asm volatile("st.release.sys.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
+__device__ __forceinline__ void st_release_gpu(int64_t* p, int64_t v)
+{
+    asm volatile("st.release.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
 template <typename R, bool CPLX>
 __device__ __forceinline__ void loop_product(const GenParams& p, const tb_ptrs& q)
 {
-    for (int64_t i = threadIdx.x; i < p.sizeF; i += blockDim.x) element<R, CPLX>(p, q.A, q.B, q.C, q.D, i);
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < p.sizeF; i += stride)
+        element<R, CPLX>(p, q.A, q.B, q.C, q.D, i);
 }
 
 __global__ void __launch_bounds__(256) k_request_loop(LoopParams lp)
@@ -491,48 +511,71 @@ __global__ void __launch_bounds__(256) k_request_loop(LoopParams lp)
     int64_t t = lp.next[b];
     unsigned long long last = loop_now_ns();
     for (;;) {
-        LoopSlot* sl = &lp.slots[t % lp.nslots];
+        const int64_t s = t % lp.nslots;
+        LoopSlot* hs = &lp.slots[s];
+        LoopSlot* ds = &lp.dslots[s];
         if (threadIdx.x == 0) {
+            // block 0 watches the host ring, the others the device copy
+            const int64_t* word = b == 0 ? &hs->seq : &lp.dseq[s];
             int posted = 0;
             for (;;) {
-                if (ld_acquire_sys(&sl->seq) == t + 1) {
+                if ((b == 0 ? ld_acquire_sys(word) : ld_acquire_gpu(word)) == t + 1) {
                     posted = 1;
                     break;
                 }
                 if (loop_now_ns() - last > lp.idle_ns) break;
-                __nanosleep(256);
+                __nanosleep(b == 0 ? 256 : 128);
             }
             go = posted;
         }
         __syncthreads();
         if (!go) break;
-        // the descriptor, 8 bytes per thread and step, from host memory
         {
-            const volatile int64_t* src = (const volatile int64_t*)&sl->p;
+            // the descriptor into shared memory: from host memory on block 0
+            // (which also fills the device copy), from the device copy elsewhere
+            const volatile int64_t* src = (const volatile int64_t*)(b == 0 ? &hs->p : &ds->p);
             int64_t* dst = (int64_t*)&sp;
-            for (int w = threadIdx.x; w < (int)(sizeof(GenParams) / 8); w += blockDim.x) dst[w] = src[w];
+            int64_t* dcopy = (int64_t*)&ds->p;
+            for (int w = threadIdx.x; w < (int)(sizeof(GenParams) / 8); w += blockDim.x) {
+                const int64_t v = src[w];
+                dst[w] = v;
+                if (b == 0) dcopy[w] = v;
+            }
             if (threadIdx.x == 0) {
-                const volatile tb_ptrs* vq = &sl->q;
+                const volatile tb_ptrs* vq = b == 0 ? &hs->q : &ds->q;
                 sq.A = vq->A;
                 sq.B = vq->B;
                 sq.C = vq->C;
                 sq.D = vq->D;
-                scomp = *(const volatile int32_t*)&sl->compute;
+                scomp = *(const volatile int32_t*)(b == 0 ? &hs->compute : &ds->compute);
+                if (b == 0) {
+                    ds->q = sq;
+                    ds->compute = scomp;
+                }
             }
         }
         __syncthreads();
+        if (b == 0 && threadIdx.x == 0) {
+            __threadfence();
+            st_release_gpu(&lp.dseq[s], t + 1);  // the device copy is complete
+        }
         switch (scomp) {
         case TB_R32: loop_product<float, false>(sp, sq); break;
         case TB_R64: loop_product<double, false>(sp, sq); break;
         case TB_C32: loop_product<float, true>(sp, sq); break;
         default: loop_product<double, true>(sp, sq); break;
         }
-        __syncthreads();  // every output of the product written
+        __syncthreads();  // this block's outputs of the product written
         if (threadIdx.x == 0) {
-            __threadfence_system();
-            st_release_sys(&sl->done, t + 1);
+            __threadfence();
+            if (atomicAdd(&lp.arrive[s], 1) == (int)gridDim.x - 1) {
+                // the last block: every output is written
+                lp.arrive[s] = 0;
+                __threadfence_system();
+                st_release_sys(&hs->done, t + 1);
+            }
         }
-        t += gridDim.x;
+        t++;
         last = loop_now_ns();
     }
     if (threadIdx.x == 0) lp.next[b] = t;
@@ -551,12 +594,23 @@ void loop_fill(void* slot, const tb_plan* P, const tb_ptrs* d)
     s->compute = P->compute;
 }
 
-cudaError_t loop_launch(void* slots_dev, int64_t* next, int nslots, int blocks, unsigned long long idle_ns,
+// device state of a loop: the ring copy, its sequence words, the arrival
+// counters and the per-block tickets (zeroed; every block starts at ticket 0)
+size_t loop_state_bytes(int nslots, int blocks)
+{
+    return (size_t)nslots * (sizeof(LoopSlot) + sizeof(int64_t) + sizeof(int)) + (size_t)blocks * sizeof(int64_t) + 64;
+}
+
+cudaError_t loop_launch(void* slots_dev, void* state, int nslots, int blocks, unsigned long long idle_ns,
                         cudaStream_t s)
 {
     LoopParams lp;
+    char* st = (char*)state;
     lp.slots = (LoopSlot*)slots_dev;
-    lp.next = next;
+    lp.dslots = (LoopSlot*)st;
+    lp.dseq = (int64_t*)(st + (size_t)nslots * sizeof(LoopSlot));
+    lp.next = lp.dseq + nslots;
+    lp.arrive = (int*)(lp.next + blocks);
     lp.nslots = nslots;
     lp.pad = 0;
     lp.idle_ns = idle_ns;

@@ -135,7 +135,8 @@ cudaError_t launch_generic_group(const tb_plan* const* P, const tb_ptrs* d, int 
 size_t group_tc_bytes(int n);
 size_t loop_slot_bytes();
 void loop_fill(void* slot, const tb_plan* P, const tb_ptrs* d);
-cudaError_t loop_launch(void* slots_dev, int64_t* next, int nslots, int blocks, unsigned long long idle_ns,
+size_t loop_state_bytes(int nslots, int blocks);
+cudaError_t loop_launch(void* slots_dev, void* state, int nslots, int blocks, unsigned long long idle_ns,
                         cudaStream_t s);
 cudaError_t launch_group_tc(const tb_plan* const* P, const tb_ptrs* d, int n, void* host, void* dev, int tile,
                             cudaStream_t s, int64_t* tiles_out);
@@ -424,25 +425,24 @@ int tbk_host_alloc_mapped(void** host, void** dev, size_t bytes)
     return (int)e;
 }
 
-// the per-block ticket counters of a loop of `blocks` blocks, block b starting at ticket b
-int tbk_loop_counters(int64_t** next, int blocks)
+// the device state of a loop (tb::loop_state_bytes), zeroed
+int tbk_loop_state(void** state, int nslots, int blocks)
 {
     tb::count_allocation();
-    cudaError_t e = cudaMalloc((void**)next, sizeof(int64_t) * (size_t)blocks);
+    const size_t bytes = tb::loop_state_bytes(nslots, blocks);
+    cudaError_t e = cudaMalloc(state, bytes);
     if (e != cudaSuccess) return (int)e;
-    int64_t init[256];
-    for (int b = 0; b < blocks && b < 256; b++) init[b] = b;
-    return (int)cudaMemcpy(*next, init, sizeof(int64_t) * (size_t)blocks, cudaMemcpyHostToDevice);
+    return (int)cudaMemset(*state, 0, bytes);
 }
 
 // launches the loop on `stream` and records `*event` (created on first use) after it
-int tbk_loop_launch(void* slots_dev, int64_t* next, int nslots, int blocks, unsigned long long idle_ns, void* stream,
+int tbk_loop_launch(void* slots_dev, void* state, int nslots, int blocks, unsigned long long idle_ns, void* stream,
                     void** event)
 {
     cudaStream_t s = (cudaStream_t)stream;
     cudaError_t e = cudaSuccess;
     if (!*event) e = cudaEventCreateWithFlags((cudaEvent_t*)event, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = tb::loop_launch(slots_dev, next, nslots, blocks, idle_ns, s);
+    if (e == cudaSuccess) e = tb::loop_launch(slots_dev, state, nslots, blocks, idle_ns, s);
     if (e == cudaSuccess) e = cudaEventRecord((cudaEvent_t)*event, s);
     return (int)e;
 }

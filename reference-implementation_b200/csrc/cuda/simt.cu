@@ -361,17 +361,24 @@ k_simt(Params p)
 #pragma unroll
                     for (int c = 0; c < NP; c++) b[j][c] = Bs[buf][c][kk][col_of(j)];
             }
+            // pairs of fused multiply-adds per instruction (fma2), each
+            // accumulator updated in the same order as one fma at a time
 #pragma unroll
-            for (int i = 0; i < TM; i++)
+            for (int i = 0; i < TM; i++) {
+                if (CPLX) {
 #pragma unroll
-                for (int j = 0; j < TN; j++) {
-                    acc[i][j][0] = fma(a[i][0], b[j][0], acc[i][j][0]);
-                    if (CPLX) {
-                        acc[i][j][0] = fma(-a[i][NP - 1], b[j][NP - 1], acc[i][j][0]);
-                        acc[i][j][NP - 1] = fma(a[i][0], b[j][NP - 1], acc[i][j][NP - 1]);
-                        acc[i][j][NP - 1] = fma(a[i][NP - 1], b[j][0], acc[i][j][NP - 1]);
+                    for (int j = 0; j < TN; j++) {
+                        // re += ar br, im += ar bi; then re += -ai bi, im += ai br
+                        fma2(acc[i][j][0], acc[i][j][NP - 1], a[i][0], a[i][0], b[j][0], b[j][NP - 1]);
+                        fma2(acc[i][j][0], acc[i][j][NP - 1], -a[i][NP - 1], a[i][NP - 1], b[j][NP - 1], b[j][0]);
                     }
+                } else {
+                    static_assert(CPLX || TN % 2 == 0, "register tiles of an even width");
+#pragma unroll
+                    for (int j = 0; j < TN; j += 2)
+                        fma2(acc[i][j][0], acc[i][j + 1][0], a[i][0], a[i][0], b[j][0], b[j + 1][0]);
                 }
+            }
         }
         if (s + 1 < nslices) {
             store_slice(buf ^ 1);
@@ -571,7 +578,7 @@ __global__ void __launch_bounds__(256) k_narrow(NarrowParams np)
                 if (k0 + u < p.K) {
                     const T* b = Bs + (k0 + u) * NB;
 #pragma unroll
-                    for (int n = 0; n < NB; n++) acc[n] = fma(cur[u], b[n], acc[n]);
+                    for (int n = 0; n < NB; n += 2) fma2(acc[n], acc[n + 1], cur[u], cur[u], b[n], b[n + 1]);
                 }
             }
 #pragma unroll
@@ -769,17 +776,14 @@ __global__ void __launch_bounds__(256) k_narrow_stream(NarrowParams np)
 #pragma unroll
                     for (int n = 0; n < NB; n += 4) {
                         const float4 q = *(const float4*)((const float*)b + n);
-                        acc[n] = fma(x, (T)q.x, acc[n]);
-                        acc[n + 1] = fma(x, (T)q.y, acc[n + 1]);
-                        acc[n + 2] = fma(x, (T)q.z, acc[n + 2]);
-                        acc[n + 3] = fma(x, (T)q.w, acc[n + 3]);
+                        fma2(acc[n], acc[n + 1], x, x, (T)q.x, (T)q.y);
+                        fma2(acc[n + 2], acc[n + 3], x, x, (T)q.z, (T)q.w);
                     }
                 } else {
 #pragma unroll
                     for (int n = 0; n < NB; n += 2) {
                         const double2 q = *(const double2*)((const double*)b + n);
-                        acc[n] = fma(x, (T)q.x, acc[n]);
-                        acc[n + 1] = fma(x, (T)q.y, acc[n + 1]);
+                        fma2(acc[n], acc[n + 1], x, x, (T)q.x, (T)q.y);
                     }
                 }
             }
@@ -984,17 +988,14 @@ __global__ void __launch_bounds__(256) k_narrow_coop(NarrowParams np)
 #pragma unroll
                     for (int n = 0; n < NB; n += 4) {
                         const float4 q = *(const float4*)((const float*)b + n);
-                        acc[n] = fma(x, (T)q.x, acc[n]);
-                        acc[n + 1] = fma(x, (T)q.y, acc[n + 1]);
-                        acc[n + 2] = fma(x, (T)q.z, acc[n + 2]);
-                        acc[n + 3] = fma(x, (T)q.w, acc[n + 3]);
+                        fma2(acc[n], acc[n + 1], x, x, (T)q.x, (T)q.y);
+                        fma2(acc[n + 2], acc[n + 3], x, x, (T)q.z, (T)q.w);
                     }
                 } else {
 #pragma unroll
                     for (int n = 0; n < NB; n += 2) {
                         const double2 q = *(const double2*)((const double*)b + n);
-                        acc[n] = fma(x, (T)q.x, acc[n]);
-                        acc[n + 1] = fma(x, (T)q.y, acc[n + 1]);
+                        fma2(acc[n], acc[n + 1], x, x, (T)q.x, (T)q.y);
                     }
                 }
             }

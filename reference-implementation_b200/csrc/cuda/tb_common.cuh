@@ -48,6 +48,28 @@ __device__ __forceinline__ uint32_t fdiv(uint32_t n, const FastDiv& f)
 }
 
 // ---------------------------------------------------------------------------
+// Two fused multiply-adds d_i = a_i * b_i + d_i in one instruction for
+// binary32 (fma.rn.f32x2 of sm_100: the same two round-to-nearest results as
+// two fmaf calls, half the issue slots); binary64 runs two fma calls.
+__device__ __forceinline__ void fma2(float& d0, float& d1, float a0, float a1, float b0, float b1)
+{
+    asm("{\n\t.reg .b64 ra, rb, rc;\n\t"
+        "mov.b64 ra, {%2, %3};\n\t"
+        "mov.b64 rb, {%4, %5};\n\t"
+        "mov.b64 rc, {%0, %1};\n\t"
+        "fma.rn.f32x2 rc, ra, rb, rc;\n\t"
+        "mov.b64 {%0, %1}, rc;\n\t}"
+        : "+f"(d0), "+f"(d1)
+        : "f"(a0), "f"(a1), "f"(b0), "f"(b1));
+}
+
+__device__ __forceinline__ void fma2(double& d0, double& d1, double a0, double a1, double b0, double b1)
+{
+    d0 = fma(a0, b0, d0);
+    d1 = fma(a1, b1, d1);
+}
+
+// ---------------------------------------------------------------------------
 // rounding of operands to the precision's input format
 template <typename R>
 __device__ __forceinline__ R round_in(R x, int mode)

@@ -13,9 +13,10 @@
  *            page-locked memory and then the slot's sequence word; launches
  *            the loop if it is not running (it returns after idle_ms without
  *            products, so it never spins without a bound);
- *   device   block t % blocks polls the sequence word, computes D with the
- *            element kernel's per-output function and writes the slot's
- *            completion word;
+ *   device   block 0 polls the sequence word and relays the descriptor
+ *            through device memory; every block computes its share of D
+ *            with the element kernel's per-output function; the last one to
+ *            finish writes the slot's completion word;
  *   wait     polls the completion word; if the loop has returned meanwhile
  *            (it went idle just before the product was posted), relaunches
  *            it. A wait gives up after 30 s with TAPP_B200_ERR_CUDA.
@@ -49,7 +50,7 @@ struct tb_loop {
     char* ring;        /* host view of the slots */
     void* ring_dev;    /* device view */
     size_t slot_bytes;
-    int64_t* next;     /* device: per block, the ticket it serves next */
+    void* state;       /* device: ring copy, sequence words, arrival counters, per-block tickets */
     int64_t next_ticket;
     double* t_submit;  /* per slot: submission time of its ticket */
     int64_t submitted, completed, launches;
@@ -89,7 +90,7 @@ static int ensure_running(struct tb_loop* l)
         if (d == 0) return 0;
     }
     if (tbk_set_device(l->device) ||
-        tbk_loop_launch(l->ring_dev, l->next, l->nslots, l->blocks, l->idle_ns, l->stream, &l->event))
+        tbk_loop_launch(l->ring_dev, l->state, l->nslots, l->blocks, l->idle_ns, l->stream, &l->event))
         return TAPP_B200_ERR_CUDA;
     l->launched = 1;
     l->launches++;
@@ -119,7 +120,7 @@ TAPP_error tapp_b200_loop_create(TAPP_b200_loop* loop, TAPP_executor exec, int b
     if (!err && tbk_stream_create(&l->stream)) err = TAPP_B200_ERR_CUDA;
     if (!err && tbk_host_alloc_mapped((void**)&l->ring, &l->ring_dev, l->slot_bytes * (size_t)slots))
         err = TAPP_B200_ERR_NOMEM;
-    if (!err && tbk_loop_counters(&l->next, blocks)) err = TAPP_B200_ERR_NOMEM;
+    if (!err && tbk_loop_state(&l->state, slots, blocks)) err = TAPP_B200_ERR_NOMEM;
     if (!err && !(l->t_submit = calloc((size_t)slots, sizeof(double)))) err = TAPP_B200_ERR_NOMEM;
     if (err) {
         tapp_b200_loop_destroy((TAPP_b200_loop)l);
@@ -265,7 +266,7 @@ TAPP_error tapp_b200_loop_destroy(TAPP_b200_loop loop)
     }
     if (err) return err;   /* the kernel may still read the ring: keep it */
     tbk_event_destroy(l->event);
-    if (l->next) tbk_dev_free(l->next);
+    if (l->state) tbk_dev_free(l->state);
     if (l->ring) tbk_host_free(l->ring);
     if (l->stream) tbk_stream_destroy(l->stream);
     free(l->t_submit);

@@ -84,13 +84,14 @@ int tbk_run_group_tc_owned(const tb_plan* const* plans, const tb_ptrs* ptrs, int
                            int64_t* tiles);
 
 /* Device-resident request loop (generic.cu: k_request_loop; host/loop.c):
- * slots of tbk_loop_slot_bytes() in mapped host memory, per-block ticket
- * counters in device memory, launch + completion event. */
+ * slots of tbk_loop_slot_bytes() in mapped host memory, the loop's state in
+ * device memory (ring copy, sequence words, arrival counters, per-block
+ * tickets), launch + completion event. */
 size_t tbk_loop_slot_bytes(void);
 void tbk_loop_fill(void* slot, const tb_plan* plan, const tb_ptrs* ptrs);
 int tbk_host_alloc_mapped(void** host, void** dev, size_t bytes);
-int tbk_loop_counters(int64_t** next, int blocks);
-int tbk_loop_launch(void* slots_dev, int64_t* next, int nslots, int blocks, unsigned long long idle_ns, void* stream,
+int tbk_loop_state(void** state, int nslots, int blocks);
+int tbk_loop_launch(void* slots_dev, void* state, int nslots, int blocks, unsigned long long idle_ns, void* stream,
                     void** event);
 int tbk_event_done(void* event);
 void tbk_event_destroy(void* event);
