@@ -115,12 +115,11 @@ __device__ __forceinline__ void finish(const GenParams& p, R sr, R si, const voi
     store_elem<R>(D, oD, p.tD, accr, acci);
 }
 
-// one element of D: the reference's loop nest for output index i
-template <typename R, bool CPLX>
-__device__ __forceinline__ void element(const GenParams& p, const void* A, const void* B, const void* C, void* D,
-                                        int64_t i)
+// offsets in A, B, C and D of the free coordinates of output index i
+__device__ __forceinline__ void free_offsets(const GenParams& p, int64_t i, int64_t& oA, int64_t& oB, int64_t& oC,
+                                             int64_t& oD)
 {
-    int64_t oA = 0, oB = 0, oC = 0, oD = 0;
+    oA = oB = oC = oD = 0;
     if (p.small_F) {
         uint32_t r = (uint32_t)i;
         for (int j = 0; j < p.nF; j++) {
@@ -143,6 +142,15 @@ __device__ __forceinline__ void element(const GenParams& p, const void* A, const
             oD += c * p.F_sD[j];
         }
     }
+}
+
+// one element of D: the reference's loop nest for output index i
+template <typename R, bool CPLX>
+__device__ __forceinline__ void element(const GenParams& p, const void* A, const void* B, const void* C, void* D,
+                                        int64_t i)
+{
+    int64_t oA, oB, oC, oD;
+    free_offsets(p, i, oA, oB, oC, oD);
     R sr = 0, si = 0;
     int64_t kc[TB_MAXMODES];
     for (int j = 0; j < p.nK; j++) kc[j] = 0;
@@ -170,6 +178,46 @@ __global__ void __launch_bounds__(256) k_elementwise(GenParams p, const void* A,
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < p.sizeF; i += stride)
         element<R, CPLX>(p, A, B, C, D, i);
+}
+
+// One warp per element of D for products whose contraction runs along an
+// operand's contiguous mode while consecutive outputs do not (batched
+// matrix-vector and Hadamard products with A stored contraction-fastest):
+// the lanes take every 32nd term (lane j the terms j, j + 32, ...), so each
+// load of the warp reads 32 neighbouring elements instead of 32 elements a
+// whole row apart, and a shuffle tree adds the 32 partial sums (a fixed
+// order: the same bits in every run).
+template <typename R, bool CPLX>
+__global__ void __launch_bounds__(256) k_warpdot(GenParams p, const void* A, const void* B, const void* C, void* D)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t i = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < p.sizeF; i += warps) {
+        int64_t oA, oB, oC, oD;
+        free_offsets(p, i, oA, oB, oC, oD);
+        R sr = 0, si = 0;
+        for (int64_t k = lane; k < p.sizeK; k += 32) {
+            int64_t kA = oA, kB = oB;
+            uint32_t r = (uint32_t)k;
+            for (int j = 0; j < p.nK; j++) {
+                const uint32_t q = j + 1 < p.nK ? fdiv(r, p.fK[j]) : 0;
+                const int64_t c = j + 1 < p.nK ? (int64_t)(r - q * p.fK[j].d) : (int64_t)r;
+                r = q;
+                kA += c * p.K_sA[j];
+                kB += c * p.K_sB[j];
+            }
+            R ar, ai, br, bi;
+            unary_sum<R, CPLX>(A, kA, p.tA, p.conjA, p.round_in, p.nUA, p.sizeUA, p.UA_ext, p.UA_s, ar, ai);
+            unary_sum<R, CPLX>(B, kB, p.tB, p.conjB, p.round_in, p.nUB, p.sizeUB, p.UB_ext, p.UB_s, br, bi);
+            cmac<R, CPLX>(sr, si, ar, ai, br, bi);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            sr += __shfl_xor_sync(0xffffffffu, sr, o);
+            if (CPLX) si += __shfl_xor_sync(0xffffffffu, si, o);
+        }
+        if (lane == 0) finish<R, CPLX>(p, sr, si, C, oC, D, oD);
+    }
 }
 
 // Many independent products of the same compute domain in one launch:
@@ -324,6 +372,19 @@ static void fill_params(const tb_plan* P, GenParams& g)
     for (int j = 0; j < P->UB.n; j++) { g.UB_ext[j] = P->UB.ext[j]; g.UB_s[j] = P->UB.sB[j]; }
 }
 
+// Element path kernel: the warp per output (k_warpdot) when an operand is
+// contiguous along the contraction while consecutive outputs step it by a
+// stride other than 0 or 1 (one thread per output would read it a row apart
+// from lane to lane), for contractions of at least 64 terms.
+static bool warpdot_ok(const GenParams& g)
+{
+    if (g.sizeK < 64 || g.sizeK >= (1ll << 31) || g.nK < 1 || g.nF < 1) return false;
+    auto a = [](int64_t x) { return x < 0 ? -x : x; };
+    const bool by_A = a(g.K_sA[0]) == 1 && a(g.F_sA[0]) > 1;
+    const bool by_B = a(g.K_sB[0]) == 1 && a(g.F_sB[0]) > 1;
+    return by_A || by_B;
+}
+
 template <typename R, bool CPLX>
 static cudaError_t launch_typed(const GenParams& g, int path, const tb_ptrs* d, cudaStream_t s)
 {
@@ -353,6 +414,11 @@ static cudaError_t launch_typed(const GenParams& g, int path, const tb_ptrs* d, 
         count_launch(2);
         cudaFreeAsync(ws, s);
         return e;
+    } else if (warpdot_ok(g)) {
+        int64_t blocks = (g.sizeF + 7) / 8;  // 8 warps, one output each
+        if (blocks > 148 * 32) blocks = 148 * 32;
+        if (blocks < 1) blocks = 1;
+        k_warpdot<R, CPLX><<<(unsigned)blocks, 256, 0, s>>>(g, d->A, d->B, d->C, d->D);
     } else {
         int64_t blocks = (g.sizeF + 255) / 256;
         if (blocks > 148 * 64) blocks = 148 * 64;
@@ -620,3 +686,12 @@ cudaError_t loop_launch(void* slots_dev, void* state, int nslots, int blocks, un
 }
 
 }  // namespace tb
+
+// Kernel of the element path for a plan: 0 one thread per output, 1 one warp
+// per output (k_warpdot). No device call.
+extern "C" int tbk_generic_kernel(const tb_plan* P)
+{
+    tb::GenParams g;
+    tb::fill_params(P, g);
+    return tb::warpdot_ok(g) ? 1 : 0;
+}

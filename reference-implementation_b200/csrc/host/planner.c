@@ -472,6 +472,7 @@ size_t tb_describe(const tb_plan* p, size_t maxlen, char* out)
     if (p->path == TB_PATH_TC && p->tc_mode == TB_TC_SPLIT_BF16)
         at = put(out, maxlen, at, " operands=%s", tbk_tc_split_in_place(p) ? "in_place" : "packed");
     if (p->path == TB_PATH_SLICED) at = put(out, maxlen, at, " slices=%d", p->slices);
+    if (p->path == TB_PATH_GENERIC) at = put(out, maxlen, at, " kernel=%s", tbk_generic_kernel(p) ? "warpdot" : "element");
     if (p->path == TB_PATH_SIMT) {
         static const char* kern[] = {"tiled", "narrow", "narrow_stream", "narrow_coop", "narrow_cstream"};
         const int k = tbk_simt_kernel(p);

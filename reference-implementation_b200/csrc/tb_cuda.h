@@ -22,6 +22,7 @@ enum { TBK_ERR_NOMEM = 2 };  /* cudaErrorMemoryAllocation */
 int tbk_device_count(int* count);
 int tbk_wait_selftest(unsigned long long limit_ns, int* out);
 int tbk_simt_kernel(const tb_plan* P);
+int tbk_generic_kernel(const tb_plan* P);
 int tbk_tc_split_in_place(const tb_plan* P);
 int tbk_pointer_kind(const void* p, int* kind, int* device);
 /* as tbk_pointer_kind; for device and managed memory also the allocation

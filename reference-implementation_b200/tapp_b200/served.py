@@ -127,6 +127,33 @@ class StreamRunner:
                 raise RuntimeError(f"request {i}: {err:#x} {self.tapp.explain(err)}")
         return times
 
+    def run_plain_arrivals(self, executor, arrivals):
+        """The plain path under arrivals: one caller runs the requests
+        synchronously in arrival order, each started no earlier than its
+        arrival time (a FIFO queue fed at `arrivals` seconds). Returns the
+        measured latency of every request (completion minus arrival, seconds)
+        and the span from the first arrival to the last completion."""
+        L = self.tapp.lib
+        st = intptr(0)
+        n = len(self.specs)
+        done = np.zeros(n)
+        t_start = time.perf_counter()
+        for i in range(n):
+            target = t_start + arrivals[i]
+            wait = target - time.perf_counter()
+            if wait > 2e-4:
+                time.sleep(wait - 1e-4)
+            while time.perf_counter() < target:
+                pass
+            a, b = self.scalars[i]
+            A, B, Cp, D = self.ptrs[i]
+            err = L.TAPP_execute_product(self.plans[i], executor, C.byref(st), a.ctypes.data, A, B,
+                                         b.ctypes.data, Cp, D)
+            done[i] = time.perf_counter() - t_start
+            if err:
+                raise RuntimeError(f"request {i}: {err:#x} {self.tapp.explain(err)}")
+        return done - np.asarray(arrivals), float(done[-1] - arrivals[0])
+
     def run_served(self, server: Server, arrivals=None):
         """Submits every request (at arrivals[i] seconds after the start,
         or all at once) and waits for all; returns the server's counters."""

@@ -1,0 +1,79 @@
+"""GPU parity of the element path's warp-per-output kernel (k_warpdot):
+products whose contraction runs along an operand's contiguous mode while
+consecutive outputs step that operand by a whole row (batched
+matrix-vector and Hadamard products with A stored contraction-fastest).
+Each case checks the kernel choice in the plan description, the result
+against the oracle's binary64 bound, and that two runs give the same bits.
+"""
+import numpy as np
+import pytest
+
+import tapp_b200
+from tapp_b200.case import Case, alloc, fill_uniform, scalar
+from helpers import run_on_device, error_bound, d_values
+
+pytestmark = pytest.mark.gpu
+
+
+def _t(rng, dtype, ext, idx, order):
+    strides = [0] * len(ext)
+    acc = 1
+    for i in order:
+        strides[i] = acc
+        acc *= ext[i]
+    return fill_uniform(alloc(dtype, ext, strides, [ord(c) for c in idx]), rng)
+
+
+def _matvec(rng, dtype, prec, k=300, m=70, h=9, unary=0, conj=False):
+    """D[m,h] = alpha sum_k (sum_u A[k,m,h,u]) B[k,h] + beta C, A contiguous along k."""
+    if unary:
+        A = _t(rng, dtype, [k, m, h, unary], "kmhu", [0, 1, 2, 3])
+    else:
+        A = _t(rng, dtype, [k, m, h], "kmh", [0, 1, 2])
+    B = _t(rng, dtype, [k, h], "kh", [0, 1])
+    if conj:
+        B.op = tapp_b200.TAPP_CONJUGATE
+    Cc = _t(rng, dtype, [m, h], "mh", [0, 1])
+    D = _t(rng, dtype, [m, h], "mh", [0, 1])
+    cplx = dtype in (tapp_b200.TAPP_C32, tapp_b200.TAPP_C64)
+    al = complex(0.8, -0.3) if cplx else 0.8
+    be = complex(-0.4, 0.2) if cplx else -0.4
+    return Case(A, B, Cc, D, scalar(dtype, al), scalar(dtype, be), prec, False, "matvec")
+
+
+CASES = [
+    ("f32", tapp_b200.TAPP_F32, 0, {}),
+    ("f64", tapp_b200.TAPP_F64, 1, {}),
+    ("c32_conj", tapp_b200.TAPP_C32, -1, {"conj": True}),
+    ("f32_unary", tapp_b200.TAPP_F32, -1, {"unary": 3}),
+    ("bf16_prec", tapp_b200.TAPP_F32, tapp_b200.TAPP_BF16BF16_ACCUM_F32, {"k": 97}),
+]
+
+
+def _describe(tapp, case):
+    infos = [tapp.tensor_info(t.dtype, t.extents, t.strides)[1] for t in (case.A, case.B, case.C, case.D)]
+    _, plan = tapp.create_product(0, [t.op for t in (case.A, case.B, case.C, case.D)], infos,
+                                  [case.A.idx, case.B.idx, case.C.idx, case.D.idx], case.prec)
+    d = tapp.describe(plan)
+    tapp.lib.TAPP_destroy_tensor_product(plan)
+    for h in infos:
+        tapp.lib.TAPP_destroy_tensor_info(h)
+    return d
+
+
+@pytest.mark.parametrize("name,dtype,prec,kw", CASES, ids=[c[0] for c in CASES])
+def test_warpdot(tapp, oracle, gpu, name, dtype, prec, kw):
+    case = _matvec(np.random.default_rng(len(name) * 7 + dtype), dtype, prec, **kw)
+    d = _describe(tapp, case)
+    assert "path=generic" in d and "kernel=warpdot" in d, d
+    runs = []
+    for _ in range(2):
+        run = case.copy()
+        assert run_on_device(tapp, run) == 0
+        runs.append(run)
+    assert np.array_equal(runs[0].D.buf.view(np.uint8), runs[1].D.buf.view(np.uint8))
+    e64, D64, scale = oracle.execute_f64(case.copy())
+    assert e64 == 0
+    bound = error_bound(case, scale, D64)
+    bad = np.abs(d_values(runs[0].D) - D64) > bound
+    assert not bad.any(), (name, int(bad.sum()))
