@@ -188,11 +188,10 @@ __global__ void __launch_bounds__(256) k_elementwise(GenParams p, const void* A,
 // whole row apart, and a shuffle tree adds the 32 partial sums (a fixed
 // order: the same bits in every run).
 template <typename R, bool CPLX>
-__global__ void __launch_bounds__(256) k_warpdot(GenParams p, const void* A, const void* B, const void* C, void* D)
+__device__ __forceinline__ void warp_element(const GenParams& p, const void* A, const void* B, const void* C, void* D,
+                                             int64_t i, int lane)
 {
-    const int lane = threadIdx.x & 31;
-    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-    for (int64_t i = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < p.sizeF; i += warps) {
+    {
         int64_t oA, oB, oC, oD;
         free_offsets(p, i, oA, oB, oC, oD);
         R sr = 0, si = 0;
@@ -218,6 +217,14 @@ __global__ void __launch_bounds__(256) k_warpdot(GenParams p, const void* A, con
         }
         if (lane == 0) finish<R, CPLX>(p, sr, si, C, oC, D, oD);
     }
+}
+
+template <typename R, bool CPLX>
+__global__ void __launch_bounds__(256) k_warpdot(GenParams p, const void* A, const void* B, const void* C, void* D)
+{
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t i = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < p.sizeF; i += warps)
+        warp_element<R, CPLX>(p, A, B, C, D, i, threadIdx.x & 31);
 }
 
 // Many independent products of the same compute domain in one launch:
@@ -512,7 +519,7 @@ struct LoopSlot {
     GenParams p;
     tb_ptrs q;
     int32_t compute;
-    int32_t pad;
+    int32_t warp;    // 1: one warp per output (the kernel TAPP_execute_product would run)
     int64_t seq;     // t + 1 once the descriptor of ticket t is complete (written last)
     int64_t done;    // t + 1 once ticket t's D is written
     int64_t pad2[6];
@@ -561,8 +568,14 @@ __device__ __forceinline__ void st_release_gpu(int64_t* p, int64_t v)
 }
 
 template <typename R, bool CPLX>
-__device__ __forceinline__ void loop_product(const GenParams& p, const tb_ptrs& q)
+__device__ __forceinline__ void loop_product(const GenParams& p, const tb_ptrs& q, int warp)
 {
+    if (warp) {
+        const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+        for (int64_t i = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < p.sizeF; i += warps)
+            warp_element<R, CPLX>(p, q.A, q.B, q.C, q.D, i, threadIdx.x & 31);
+        return;
+    }
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < p.sizeF; i += stride)
         element<R, CPLX>(p, q.A, q.B, q.C, q.D, i);
@@ -572,7 +585,7 @@ __global__ void __launch_bounds__(256) k_request_loop(LoopParams lp)
 {
     __shared__ GenParams sp;
     __shared__ tb_ptrs sq;
-    __shared__ int scomp, go;
+    __shared__ int scomp, swarp, go;
     const int b = blockIdx.x;
     int64_t t = lp.next[b];
     unsigned long long last = loop_now_ns();
@@ -614,9 +627,11 @@ __global__ void __launch_bounds__(256) k_request_loop(LoopParams lp)
                 sq.C = vq->C;
                 sq.D = vq->D;
                 scomp = *(const volatile int32_t*)(b == 0 ? &hs->compute : &ds->compute);
+                swarp = *(const volatile int32_t*)(b == 0 ? &hs->warp : &ds->warp);
                 if (b == 0) {
                     ds->q = sq;
                     ds->compute = scomp;
+                    ds->warp = swarp;
                 }
             }
         }
@@ -626,10 +641,10 @@ __global__ void __launch_bounds__(256) k_request_loop(LoopParams lp)
             st_release_gpu(&lp.dseq[s], t + 1);  // the device copy is complete
         }
         switch (scomp) {
-        case TB_R32: loop_product<float, false>(sp, sq); break;
-        case TB_R64: loop_product<double, false>(sp, sq); break;
-        case TB_C32: loop_product<float, true>(sp, sq); break;
-        default: loop_product<double, true>(sp, sq); break;
+        case TB_R32: loop_product<float, false>(sp, sq, swarp); break;
+        case TB_R64: loop_product<double, false>(sp, sq, swarp); break;
+        case TB_C32: loop_product<float, true>(sp, sq, swarp); break;
+        default: loop_product<double, true>(sp, sq, swarp); break;
         }
         __syncthreads();  // this block's outputs of the product written
         if (threadIdx.x == 0) {
@@ -658,6 +673,7 @@ void loop_fill(void* slot, const tb_plan* P, const tb_ptrs* d)
     if (P->path == TB_PATH_NOOP) s->p.sizeF = 0;  // nothing to write (empty D, or a precision left as is)
     s->q = *d;
     s->compute = P->compute;
+    s->warp = warpdot_ok(s->p) ? 1 : 0;
 }
 
 // device state of a loop: the ring copy, its sequence words, the arrival

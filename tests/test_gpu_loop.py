@@ -18,6 +18,7 @@ import pytest
 import tapp_b200
 from tapp_b200.workloads import dense_contraction_case, mixed_classes_case
 from families import bounded_case
+from test_gpu_element import _matvec
 
 pytestmark = pytest.mark.gpu
 
@@ -30,6 +31,9 @@ def _small_cases():
             cases.append(dense_contraction_case(rng, extent=e, dtype=dt, prec=prec))
     for i in range(20):
         cases.append(bounded_case(rng, max_work=2e5))
+    # contraction-contiguous products: TAPP_execute_product runs them one warp per output
+    cases.append(_matvec(rng, tapp_b200.TAPP_F32, 0, k=200, m=40, h=5))
+    cases.append(_matvec(rng, tapp_b200.TAPP_C32, -1, k=96, m=30, h=4, conj=True))
     return cases
 
 
