@@ -286,6 +286,215 @@ __global__ void __launch_bounds__(256, 4) k_pack_real(PackParams p)
     }
 }
 
+// Pipelined pack for binary32 sources read 16 bytes at a time (the VEC = 4
+// case above: the fast mode has stride 1 and an extent divisible by 4, every
+// other stride keeps 16-byte alignment). Persistent blocks of 128 threads walk
+// the 64 x 64 tiles (block b: tiles b, b + grid, ...) and copy each tile into
+// a ring of PP_STAGES shared-memory slots with cp.async, PP_STAGES - 1 tiles
+// ahead of the one being written out, so a block keeps ~48 KiB of loads in
+// flight without holding them in registers (the one-tile kernel above has one
+// load phase and one store phase per block). Slot layouts, both read without
+// bank conflicts:
+//   K fast    [r][k], 68 floats per row; thread (r, g) reads k = 8g..8g+7 as
+//             two 16-byte reads, lanes 4-7 of each quarter-warp reading their
+//             second half first;
+//   rows fast [r / 4][k] of float4 (4 consecutive rows, as copied), 65 float4
+//             per row group; thread (r4, g) reads 8 float4 = rows 4 r4..4 r4 + 3
+//             at k = 8g..8g+7, quarter-warps over 8 row groups.
+// Output words and their order are those of k_pack_real (same rounding, same
+// [hi | lo] or three-segment split), so the two kernels write identical panels.
+constexpr int PP_THREADS = 128, PP_STAGES = 4, PP_PITCH = 68, PP_P4 = 65;
+constexpr int PP_SLOT = 64 * PP_PITCH;  // floats per slot (the rows-fast layout needs 16 * 65 * 4)
+struct PackTab {
+    int64_t row[64];
+    int64_t k[64];
+    const float* src;  // the tile's batch base
+    int64_t pad;
+};
+constexpr int PP_SMEM = PP_STAGES * PP_SLOT * 4 + 2 * (int)sizeof(PackTab);
+
+__device__ __forceinline__ void cp_async16_zfill(uint32_t dst, const void* src, bool in)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(in ? 16 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void pp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void pp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// eight values of row rg at columns col..col+7, every segment, as k_pack_real writes them
+template <int SPLIT, int FMT>
+__device__ __forceinline__ void pp_put8(const PackParams& p, int64_t l, int64_t rg, int64_t col, const float (&x)[8])
+{
+#pragma unroll
+    for (int seg = 0; seg < SPLIT; seg++) {
+        uint32_t w[4];
+#pragma unroll
+        for (int h = 0; h < 4; h++) {
+            float a = x[2 * h], b = x[2 * h + 1];
+            if (SPLIT == 1 && p.round_mode != TB_ROUND_NONE) {
+                a = round_in<float>(a, p.round_mode);
+                b = round_in<float>(b, p.round_mode);
+            }
+            if (SPLIT >= 2) {
+                const float ah = __bfloat162float(__float2bfloat16_rn(a));
+                const float bh = __bfloat162float(__float2bfloat16_rn(b));
+                const bool use_lo = SPLIT == 2 ? seg == 1 : p.is_B ? (seg == 1) : (seg == 2);
+                if (use_lo) { a -= ah; b -= bh; } else { a = ah; b = bh; }
+            }
+            if (FMT == 1) {
+                __half2 q = __floats2half2_rn(a, b);
+                w[h] = *(uint32_t*)&q;
+            } else {
+                __nv_bfloat162 q = __floats2bfloat162_rn(a, b);
+                w[h] = *(uint32_t*)&q;
+            }
+        }
+        const int64_t idx = ((int64_t)l * p.Rout + rg) * p.Kld + seg * p.Kseg + col;
+        *(uint4*)((uint16_t*)p.dst + idx) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+}
+
+template <int SPLIT, int FMT, bool ROWS_FAST>
+__global__ void __launch_bounds__(PP_THREADS) k_pack_pipe(PackParams p, int64_t tiles_r, int64_t tiles_k, int64_t ntiles)
+{
+    extern __shared__ __align__(16) float pp_sm[];
+    float* slots = pp_sm;
+    PackTab* tab = (PackTab*)(pp_sm + PP_STAGES * PP_SLOT);
+    const int t = threadIdx.x;
+    const int64_t first = blockIdx.x, step = gridDim.x;
+    const int64_t nloc = first < ntiles ? (ntiles - 1 - first) / step + 1 : 0;
+    auto tile_of = [&](int64_t i, int64_t& r0, int64_t& k0, int64_t& l) {
+        int64_t j = first + i * step;
+        k0 = (j % tiles_k) * 64;
+        j /= tiles_k;
+        r0 = (j % tiles_r) * 64;
+        l = j / tiles_r;
+    };
+    // source offsets of tile i's 64 rows (threads 0-63) and 64 columns (64-127)
+    auto make_tab = [&](int64_t i, PackTab& tb) {
+        if (i >= nloc) return;
+        int64_t r0, k0, l, o = 0, dummy;
+        tile_of(i, r0, k0, l);
+        if (t < 64) {
+            if (r0 + t < p.R) decode2(p.rows, r0 + t, o, dummy);
+            tb.row[t] = o;
+        } else {
+            const int kk = t - 64;
+            if (k0 + kk < p.K) decode2(p.ks, k0 + kk, o, dummy);
+            tb.k[kk] = o;
+        }
+        if (t == 0) {
+            const int64_t lsrc = p.srcs ? l % p.Lsz : l;
+            decode2(p.ls, lsrc, o, dummy);
+            tb.src = (const float*)(p.srcs ? p.srcs[l / p.Lsz] : p.src) + o;
+        }
+    };
+    // 1024 chunks of 16 bytes per tile, 8 per thread; outside the tensor: zeros
+    auto issue = [&](int64_t i, const PackTab& tb) {
+        if (i < nloc) {
+            int64_t r0, k0, l;
+            tile_of(i, r0, k0, l);
+            const uint32_t sb = smem_u32(slots + (i % PP_STAGES) * PP_SLOT);
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const int c = t + PP_THREADS * u;
+                const int fg = c % 16, sl = c / 16;
+                const int r = ROWS_FAST ? fg * 4 : sl;
+                const int kk = ROWS_FAST ? sl : fg * 4;
+                const uint32_t dst = ROWS_FAST ? sb + (uint32_t)(fg * PP_P4 + kk) * 16u
+                                               : sb + (uint32_t)(r * PP_PITCH + kk) * 4u;
+                const bool in = r0 + r < p.R && k0 + kk < p.K;
+                cp_async16_zfill(dst, in ? (const void*)(tb.src + tb.row[r] + tb.k[kk]) : (const void*)tb.src, in);
+            }
+        }
+        pp_commit();  // empty groups keep the count uniform
+    };
+    auto store = [&](int64_t i) {
+        int64_t r0, k0, l;
+        tile_of(i, r0, k0, l);
+        const float* v = slots + (i % PP_STAGES) * PP_SLOT;
+        if (ROWS_FAST) {
+            const int r4 = t % 16, g = t / 16;
+            const int64_t col = k0 + g * 8;
+            if (col >= p.Kseg || r0 + r4 * 4 >= p.R) return;
+            float4 q[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) q[j] = *(const float4*)(v + (size_t)(r4 * PP_P4 + g * 8 + j) * 4);
+#pragma unroll
+            for (int h = 0; h < 4; h++) {
+                const int64_t rg = r0 + r4 * 4 + h;
+                if (rg >= p.R) break;
+                float x[8];
+#pragma unroll
+                for (int j = 0; j < 8; j++) x[j] = h == 0 ? q[j].x : h == 1 ? q[j].y : h == 2 ? q[j].z : q[j].w;
+                pp_put8<SPLIT, FMT>(p, l, rg, col, x);
+            }
+        } else {
+#pragma unroll
+            for (int it = 0; it < 4; it++) {
+                const int e = t + PP_THREADS * it;
+                const int g = e % 8, r = e / 8;
+                const int64_t rg = r0 + r, col = k0 + g * 8;
+                if (rg >= p.R || col >= p.Kseg) continue;
+                const int h0 = (g >> 2) & 1;
+                const float4 a = *(const float4*)(v + r * PP_PITCH + g * 8 + 4 * h0);
+                const float4 b = *(const float4*)(v + r * PP_PITCH + g * 8 + 4 * (1 - h0));
+                const float4 lo4 = h0 ? b : a, hi4 = h0 ? a : b;
+                const float x[8] = {lo4.x, lo4.y, lo4.z, lo4.w, hi4.x, hi4.y, hi4.z, hi4.w};
+                pp_put8<SPLIT, FMT>(p, l, rg, col, x);
+            }
+        }
+    };
+    for (int i = 0; i < PP_STAGES - 1; i++) {
+        make_tab(i, tab[i & 1]);
+        __syncthreads();
+        issue(i, tab[i & 1]);
+    }
+    make_tab(PP_STAGES - 1, tab[(PP_STAGES - 1) & 1]);
+    for (int64_t i = 0; i < nloc; i++) {
+        pp_wait<PP_STAGES - 2>();  // this thread's copies of tile i have landed
+        __syncthreads();           // everyone's have; slot (i - 1) and table (i + S) are free
+        issue(i + PP_STAGES - 1, tab[(i + PP_STAGES - 1) & 1]);
+        make_tab(i + PP_STAGES, tab[(i + PP_STAGES) & 1]);
+        store(i);
+    }
+    pp_wait<0>();
+}
+
+static int num_sms();
+
+// false: the kernel could not be given its shared memory (the caller runs k_pack_real)
+template <int SPLIT, int FMT, bool RF>
+static bool launch_pack_pipe(const PackParams& pp, int64_t lz, cudaStream_t s)
+{
+    auto kern = k_pack_pipe<SPLIT, FMT, RF>;
+    static int attr_done[64];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64 || !attr_done[dev]) {
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, PP_SMEM) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        if (dev >= 0 && dev < 64) attr_done[dev] = 1;
+    }
+    const int64_t tiles_r = (pp.R + 63) / 64, tiles_k = (pp.Kseg + 63) / 64;
+    const int64_t ntiles = tiles_r * tiles_k * lz;
+    const int64_t grid = std::min<int64_t>(ntiles, (int64_t)num_sms() * 3);
+    if (grid > 0) kern<<<(unsigned)grid, PP_THREADS, PP_SMEM, s>>>(pp, tiles_r, tiles_k, ntiles);
+    return true;
+}
+
+template <bool RF>
+static bool launch_pack_pipe3(const PackParams& pp, int split, int fmt, int64_t lz, cudaStream_t s)
+{
+    if (split == 3) return launch_pack_pipe<3, 0, RF>(pp, lz, s);
+    if (split == 2) return launch_pack_pipe<2, 0, RF>(pp, lz, s);
+    if (fmt == 1) return launch_pack_pipe<1, 1, RF>(pp, lz, s);
+    return launch_pack_pipe<1, 0, RF>(pp, lz, s);
+}
+
 template <typename T, bool RF, int VEC>
 static void launch_pack_real3(const PackParams& pp, int split, int fmt, dim3 grid, cudaStream_t s)
 {
@@ -320,6 +529,8 @@ static void launch_pack_real(const PackParams& pp, int split, int fmt, int64_t l
         const ModeList* others[3] = {rf ? &pp.ks : &pp.rows, &pp.ls, &pp.us};
         v4 = vec4_ok(rf ? pp.rows : pp.ks, others, 2, pp.src);
     }
+    if (v4 && (rf ? launch_pack_pipe3<true>(pp, split, fmt, lz, s) : launch_pack_pipe3<false>(pp, split, fmt, lz, s)))
+        return;
     if (rf) {
         if (v4) launch_pack_real3<T, true, 4>(pp, split, fmt, grid, s);
         else launch_pack_real3<T, true, 1>(pp, split, fmt, grid, s);

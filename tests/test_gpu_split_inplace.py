@@ -132,6 +132,23 @@ def test_split_routes(tapp, oracle, gpu, name, mode):
     assert not bad.any(), (name, int(bad.sum()), got[bad][:4], D64[bad][:4], bound[bad][:4])
 
 
+@pytest.mark.parametrize("name", list(CASES))
+def test_split_routes_same_bits(tapp, gpu, name):
+    """The two routes split every value the same way (hi = bf16(x), lo =
+    bf16(x - hi)) and issue the same three MMAs per 16-deep step: the panels
+    written by the pack pass and the tiles written by the converter warps
+    give the same D bit for bit."""
+    case = CASES[name](np.random.default_rng(zlib.crc32(name.encode()) + 1))
+    outs = []
+    for mode in (3, 2):
+        ex = _executor(tapp, mode)
+        run = case.copy()
+        assert run_on_device(tapp, run, ex) == 0
+        tapp.lib.TAPP_destroy_executor(ex)
+        outs.append(run.D.buf.view(np.uint8).copy())
+    assert np.array_equal(outs[0], outs[1]), name
+
+
 def test_split_packed_when_layout_does_not_qualify(tapp, oracle, gpu):
     """A contiguous contracted mode of extent 12 (not a multiple of 8): the
     operands are packed first (three launches), same bound."""
