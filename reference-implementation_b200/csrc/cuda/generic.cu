@@ -387,8 +387,10 @@ static bool warpdot_ok(const GenParams& g)
 {
     if (g.sizeK < 64 || g.sizeK >= (1ll << 31) || g.nK < 1 || g.nF < 1) return false;
     auto a = [](int64_t x) { return x < 0 ? -x : x; };
-    const bool by_A = a(g.K_sA[0]) == 1 && a(g.F_sA[0]) > 1;
-    const bool by_B = a(g.K_sB[0]) == 1 && a(g.F_sB[0]) > 1;
+    // not when consecutive outputs already walk the other operand along its
+    // contiguous mode (threads per output read that one in whole lines)
+    const bool by_A = a(g.K_sA[0]) == 1 && a(g.F_sA[0]) > 1 && a(g.F_sB[0]) != 1;
+    const bool by_B = a(g.K_sB[0]) == 1 && a(g.F_sB[0]) > 1 && a(g.F_sA[0]) != 1;
     return by_A || by_B;
 }
 

@@ -1186,6 +1186,246 @@ __global__ void __launch_bounds__(256) k_narrow_cstream(NarrowParams np)
     cp_async_wait<0>();
 }
 
+// Register-tiled narrow kernel for A, C and D contiguous along their first
+// row mode, VR rows to one vector (binary32: VR = 4, 16 bytes, or 2 when the
+// row extents only allow pairs; binary64: VR = 2). A block of NB / 8 x 64
+// threads takes tiles of TR = 64 VR rows. Per chunk of KC contracted values
+// (16 KiB of A) the whole block copies the tile's chunk with cp.async as
+// VR-row vectors into a ring of 4 chunks laid out [k][row]; thread t always
+// copies row group t % 64, so it decodes one row offset per tile. After a
+// block barrier, thread (column group c, half h, lane) multiplies row group
+// 32 h + lane by columns 8c..8c+7: per contracted value one vector of A and
+// two (binary64: four) 16-byte broadcast reads of the B panel feed 8 VR
+// independent multiply-adds. At the start of each tile a thread copies the C
+// vectors of its own outputs into its own part of a shared-memory buffer
+// with cp.async (read back in the epilogue, ordered by cp.async.wait_group);
+// D is stored as VR-row vectors.
+// Every output sees the same fused multiply-adds in the same order as in
+// k_narrow_stream (acc = fma(a_k, b_k, acc) for k = 0, 1, ...; then
+// fma(beta, c, alpha acc)), so the two kernels give the same bits.
+template <typename T, int VR>
+struct NarrowVec;
+template <>
+struct NarrowVec<float, 4> {
+    using V = float4;
+    __device__ static void get(const V& v, float (&x)[4]) { x[0] = v.x; x[1] = v.y; x[2] = v.z; x[3] = v.w; }
+    __device__ static V put(const float (&x)[4]) { return make_float4(x[0], x[1], x[2], x[3]); }
+};
+template <>
+struct NarrowVec<float, 2> {
+    using V = float2;
+    __device__ static void get(const V& v, float (&x)[2]) { x[0] = v.x; x[1] = v.y; }
+    __device__ static V put(const float (&x)[2]) { return make_float2(x[0], x[1]); }
+};
+template <>
+struct NarrowVec<double, 2> {
+    using V = double2;
+    __device__ static void get(const V& v, double (&x)[2]) { x[0] = v.x; x[1] = v.y; }
+    __device__ static V put(const double (&x)[2]) { return make_double2(x[0], x[1]); }
+};
+
+template <int BYTES>
+__device__ __forceinline__ void cp_async_vec(uint32_t dst, const void* src)
+{
+    if (BYTES == 16) asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+    else asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
+}
+
+constexpr int NVEC_STAGES = 4, NVEC_CHUNK_BYTES = 16384, NVEC_MAX_SMEM = 200 * 1024;
+
+template <typename T, int VR>
+constexpr int nvec_kc() { return NVEC_CHUNK_BYTES / (64 * VR * (int)sizeof(T)); }
+
+template <typename T, int NB, int VR, bool RND>
+__global__ void __launch_bounds__(NB * 8) k_narrow_vec(NarrowParams np)
+{
+    constexpr int NT = NB * 8, TR = 64 * VR, KC = nvec_kc<T, VR>(), S = NVEC_STAGES;
+    using NV = NarrowVec<T, VR>;
+    using V = typename NV::V;
+    const Params& p = np.p;
+    extern __shared__ __align__(16) unsigned char nsm[];
+    T* ring = (T*)nsm;                                    // [S][KC][TR]
+    T* Cs = ring + (size_t)S * KC * TR;                   // [NB][TR] when C is read
+    T* Bs = Cs + (p.beta_zero ? 0 : (size_t)NB * TR);     // [K][NB]
+    int64_t* kA = (int64_t*)(Bs + (size_t)NB * p.K);      // [K] (NB is a multiple of 8: 8-byte aligned)
+    int64_t* nC = kA + p.K;                               // [NB]
+    int64_t* nD = nC + NB;                                // [NB]
+    const int t = threadIdx.x;
+    const int64_t l = blockIdx.y;
+    int64_t lA, lB, lC, lD, dummy;
+    decode(p.al, l, lA, dummy);
+    decode(p.bl, l, lB, dummy);
+    decode(p.cl, l, lC, lD);
+    for (int64_t k = t; k < p.K; k += NT) {
+        int64_t o;
+        decode(p.ak, k, o, dummy);
+        kA[k] = o + lA;
+    }
+    if (t < NB) {
+        int64_t oc = 0, od = 0;
+        if (t < p.N) decode(p.cn, t, oc, od);
+        nC[t] = oc + lC;
+        nD[t] = od + lD;
+    }
+    for (int64_t e = t; e < p.K * NB; e += NT) {
+        const int64_t k = e / NB;
+        const int n = (int)(e % NB);
+        T x = 0, xi = 0;
+        if (n < p.N) {
+            int64_t ob, ok;
+            decode(p.bn, n, ob, dummy);
+            decode(p.bk, k, ok, dummy);
+            load_rounded<T>(p.B, lB + ob + ok, p.tB, p.round_in, x, xi);
+        }
+        Bs[k * NB + n] = x;
+    }
+    __syncthreads();
+
+    const int64_t tiles = (p.M + TR - 1) / TR;
+    if ((int64_t)blockIdx.x >= tiles) return;
+    const int64_t my_tiles = (tiles - 1 - blockIdx.x) / gridDim.x + 1;
+    const int nchunks = (int)((p.K + KC - 1) / KC);
+    const int64_t total = my_tiles * nchunks;
+    const T* A = (const T*)p.A;
+    // offsets in A, C and D of the first row of row group rg of tile i (-1: past M;
+    // the VR rows of a group are consecutive in all three)
+    auto group_offsets = [&](int64_t i, int rg, int64_t& oA, int64_t& oC, int64_t& oD) {
+        const int64_t m = ((int64_t)blockIdx.x + i * gridDim.x) * TR + (int64_t)rg * VR;
+        oA = oC = oD = -1;
+        if (m >= p.M) return;
+        oA = oC = oD = 0;
+        uint32_t r = (uint32_t)m;
+        for (int j = 0; j < p.am.n; j++) {
+            const uint32_t q = fdiv(r, np.fm[j]);
+            const int64_t c = (int64_t)(r - q * np.fm[j].d);
+            r = q;
+            oA += c * p.am.s0[j];
+            oC += c * p.cm.s0[j];
+            oD += c * p.cm.s1[j];
+        }
+    };
+    // producer: thread t copies row group t % 64 at contracted values t / 64, t / 64 + NT / 64, ...
+    const int prg = t % 64, pk0 = t / 64;
+    constexpr int PKS = NT / 64;
+    const uint32_t ring_base = (uint32_t)__cvta_generic_to_shared(ring) + (uint32_t)(prg * VR * sizeof(T));
+    int64_t p_tile = -1, p_oA = -1;
+    int p_chunk = 0;
+    auto issue = [&](int64_t g) {
+        if (g < total) {
+            if (p_chunk == 0) {
+                p_tile++;
+                int64_t c_, d_;
+                group_offsets(p_tile, prg, p_oA, c_, d_);
+            }
+            if (p_oA >= 0) {
+                const int k0 = p_chunk * KC;
+                const uint32_t dst = ring_base + (uint32_t)((g % S) * KC * TR * sizeof(T));
+                for (int kk = pk0; kk < KC; kk += PKS)
+                    if (k0 + kk < p.K) cp_async_vec<VR * (int)sizeof(T)>(dst + kk * TR * sizeof(T), A + p_oA + kA[k0 + kk]);
+            }
+            if (++p_chunk == nchunks) p_chunk = 0;
+        }
+        cp_async_commit();  // empty groups keep the count uniform
+    };
+#pragma unroll
+    for (int g = 0; g < S - 1; g++) issue(g);
+
+    const int lane = t & 31, w = t >> 5;
+    const int cg = w >> 1, crg = (w & 1) * 32 + lane;
+    const T al = (T)p.alpha, be = (T)p.beta;
+    T acc[VR][8];
+    const uint32_t cs_base = (uint32_t)__cvta_generic_to_shared(Cs) + (uint32_t)((cg * 8 * TR + crg * VR) * sizeof(T));
+    int64_t oA = -1, oC = -1, oD = -1;
+    int c = 0;
+    int64_t ti = 0;
+    for (int64_t g = 0; g < total; g++) {
+        if (c == 0) {
+            group_offsets(ti, crg, oA, oC, oD);
+#pragma unroll
+            for (int r = 0; r < VR; r++)
+#pragma unroll
+                for (int n = 0; n < 8; n++) acc[r][n] = 0;
+        }
+        cp_async_wait<S - 2>();  // this thread's copies of chunk g have landed
+        __syncthreads();         // everyone's have; the slot of chunk g - 1 is free
+        if (c == 0 && oA >= 0 && !p.beta_zero) {
+            // this thread's C vectors join the group committed next
+#pragma unroll
+            for (int n = 0; n < 8; n++)
+                if (cg * 8 + n < p.N)
+                    cp_async_vec<VR * (int)sizeof(T)>(cs_base + (uint32_t)(n * TR * sizeof(T)),
+                                                       (const T*)p.C + oC + nC[cg * 8 + n]);
+        }
+        issue(g + S - 1);
+        const bool last = c == nchunks - 1;
+        if (oA >= 0) {
+            const T* a = ring + (size_t)(g % S) * KC * TR + crg * VR;
+            const int k0 = c * KC;
+            const int kn = p.K - k0 < KC ? (int)(p.K - k0) : KC;
+#pragma unroll 2
+            for (int kk = 0; kk < kn; kk++) {
+                T x[VR];
+                NV::get(*(const V*)(a + kk * TR), x);
+                if (RND) {
+#pragma unroll
+                    for (int r = 0; r < VR; r++) x[r] = round_in<T>(x[r], p.round_in);
+                }
+                const T* b = Bs + (k0 + kk) * NB + cg * 8;
+                T bv[8];
+                if (sizeof(T) == 4) {
+                    const float4 q0 = *(const float4*)b, q1 = *(const float4*)(b + 4);
+                    bv[0] = (T)q0.x; bv[1] = (T)q0.y; bv[2] = (T)q0.z; bv[3] = (T)q0.w;
+                    bv[4] = (T)q1.x; bv[5] = (T)q1.y; bv[6] = (T)q1.z; bv[7] = (T)q1.w;
+                } else {
+#pragma unroll
+                    for (int n = 0; n < 8; n += 2) {
+                        const double2 q = *(const double2*)((const double*)b + n);
+                        bv[n] = (T)q.x;
+                        bv[n + 1] = (T)q.y;
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < VR; r++)
+#pragma unroll
+                    for (int n = 0; n < 8; n += 2) fma2(acc[r][n], acc[r][n + 1], x[r], x[r], bv[n], bv[n + 1]);
+            }
+        }
+        if (last) {
+            if (oA >= 0) {
+                // the tile's C copies went with the group of its first chunk:
+                // at most nchunks - 1 younger groups may still be pending
+                if (!p.beta_zero && nchunks < S) {
+                    static_assert(S == 4, "the waits below cover nchunks = 1 .. S - 1");
+                    if (nchunks == 1) cp_async_wait<0>();
+                    else if (nchunks == 2) cp_async_wait<1>();
+                    else cp_async_wait<2>();
+                }
+#pragma unroll
+                for (int n = 0; n < 8; n++) {
+                    if (cg * 8 + n < p.N) {
+                        T cv[VR] = {};
+                        if (!p.beta_zero) NV::get(*(const V*)(Cs + (size_t)(cg * 8 + n) * TR + crg * VR), cv);
+                        T y[VR];
+#pragma unroll
+                        for (int r = 0; r < VR; r++) {
+                            if (RND && !p.beta_zero) cv[r] = round_in<T>(cv[r], p.round_in);
+                            T v = p.beta_zero ? al * acc[r][n] : fma(be, cv[r], al * acc[r][n]);
+                            if (p.conjD && p.conjD_f32) v = (T)(float)v;  // op_D under the F64 precision rounds as conjf
+                            y[r] = v;
+                        }
+                        *(V*)((T*)p.D + oD + nD[cg * 8 + n]) = NV::put(y);
+                    }
+                }
+            }
+            c = 0;
+            ti++;
+        } else {
+            c++;
+        }
+    }
+    cp_async_wait<0>();
+}
+
 // Split of the contraction: enough CTAs to fill the GPU when the tiles do
 // not, each split at least 4 slices long, the workspace at most 256 MiB.
 struct Split {
@@ -1400,12 +1640,36 @@ static int narrow_width(const tb_plan* P, const simt::Params& p)
 //              width 48 with D contiguous along its rows)
 //   NK_COOP    k_narrow_coop: binary32 streaming with A contiguous along the
 //              contraction and D along the columns (C staged whenever read)
-enum { NK_REG = 1, NK_STREAM = 2, NK_COOP = 3 };
+//   NK_VEC     k_narrow_vec: A, C and D contiguous along the first row mode,
+//              read and written as VR-row vectors (register tiles)
+enum { NK_REG = 1, NK_STREAM = 2, NK_COOP = 3, NK_VEC = 5 };
 struct NarrowChoice {
     int kind;
     bool rnd, stage_c;
     size_t smem;
+    int vr;  // NK_VEC: rows per vector
 };
+
+// whether k_narrow_vec can read A and C and write D as vr-row vectors: the
+// first row mode has stride 1 in all three and an extent divisible by vr,
+// every other stride and every base keeps the vector's alignment
+static bool nvec_layout(const simt::Params& p, int vr, size_t es)
+{
+    auto strides_ok = [&](const simt::Modes& m, bool d_side, int from) {
+        for (int j = from; j < m.n; j++)
+            if ((d_side ? m.s1[j] : m.s0[j]) % vr != 0) return false;
+        return true;
+    };
+    const uintptr_t vb = (uintptr_t)vr * es;
+    if (p.am.n < 1 || p.am.s0[0] != 1 || p.am.ext[0] % vr != 0 || p.cm.s1[0] != 1) return false;
+    if (!strides_ok(p.am, false, 1) || !strides_ok(p.ak, false, 0) || !strides_ok(p.al, false, 0)) return false;
+    if (!strides_ok(p.cm, true, 1) || !strides_ok(p.cn, true, 0) || !strides_ok(p.cl, true, 0)) return false;
+    if ((uintptr_t)p.A % vb != 0 || (uintptr_t)p.D % vb != 0) return false;
+    if (!p.beta_zero && (p.cm.s0[0] != 1 || !strides_ok(p.cm, false, 1) || !strides_ok(p.cn, false, 0) ||
+                         !strides_ok(p.cl, false, 0) || (uintptr_t)p.C % vb != 0))
+        return false;
+    return true;
+}
 
 static NarrowChoice narrow_choice(const simt::Params& p, int nb, size_t es)
 {
@@ -1420,6 +1684,19 @@ static NarrowChoice narrow_choice(const simt::Params& p, int nb, size_t es)
     const bool stream_ok = f32 || nb <= 48;
     const int t_own = f32 ? T_F32 : T_F64;
     c.rnd = p.round_in != TB_ROUND_NONE;  // rounding after the copy is the rounding load's for binary32 only
+    c.vr = 0;
+    if (p.tA == t_own && p.tD == t_own && (p.beta_zero || p.tC == t_own) && (f32 || !c.rnd)) {
+        const int vr = f32 ? (nvec_layout(p, 4, es) ? 4 : nvec_layout(p, 2, es) ? 2 : 0) : (nvec_layout(p, 2, es) ? 2 : 0);
+        const size_t vsmem = (size_t)NVEC_STAGES * NVEC_CHUNK_BYTES + (p.beta_zero ? 0 : es * (size_t)nb * 64 * vr) +
+                             es * (size_t)nb * (size_t)p.K + 8 * ((size_t)p.K + 2 * (size_t)nb);
+        if (vr && vsmem <= (size_t)NVEC_MAX_SMEM) {
+            c.kind = NK_VEC;
+            c.vr = vr;
+            c.stage_c = false;
+            c.smem = vsmem;
+            return c;
+        }
+    }
     const bool stream = stream_ok && p.tA == t_own && (!c.rnd || f32) && (uintptr_t)p.A % es == 0 &&
                         (f32 || p.d_rows_fast);
     c.kind = stream ? NK_STREAM : NK_REG;
@@ -1447,11 +1724,47 @@ static NarrowChoice narrow_choice(const simt::Params& p, int nb, size_t es)
 }
 
 template <typename T, int NB>
+static cudaError_t launch_narrow_vec(simt::NarrowParams& np, const NarrowChoice& ch, cudaStream_t s)
+{
+    using namespace simt;
+    const Params& p = np.p;
+    void (*kern)(NarrowParams);
+    int variant = 0;
+    if constexpr (sizeof(T) == 4) {
+        if (ch.vr == 4) kern = ch.rnd ? k_narrow_vec<float, NB, 4, true> : k_narrow_vec<float, NB, 4, false>;
+        else kern = ch.rnd ? k_narrow_vec<float, NB, 2, true> : k_narrow_vec<float, NB, 2, false>;
+        variant = (ch.vr == 4 ? 0 : 2) + (int)ch.rnd;
+    } else {
+        kern = k_narrow_vec<double, NB, 2, false>;
+    }
+    static int attr_done[64][4];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64 || !attr_done[dev][variant]) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, NVEC_MAX_SMEM);
+        if (e != cudaSuccess) return e;
+        if (dev >= 0 && dev < 64) attr_done[dev][variant] = 1;
+    }
+    const int threads = NB * 8;
+    const int64_t tiles = (p.M + 64 * ch.vr - 1) / (64 * ch.vr);
+    int per_sm = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, ch.smem) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    int64_t gx = ((int64_t)148 * per_sm + p.L - 1) / p.L;
+    if (gx > tiles) gx = tiles;
+    if (gx < 1) gx = 1;
+    kern<<<dim3((unsigned)gx, (unsigned)p.L), threads, ch.smem, s>>>(np);
+    count_launch();
+    return cudaGetLastError();
+}
+
+template <typename T, int NB>
 static cudaError_t launch_narrow_t(simt::NarrowParams& np, cudaStream_t s)
 {
     using namespace simt;
     const Params& p = np.p;
     const NarrowChoice ch = narrow_choice(p, NB, sizeof(T));
+    if (ch.kind == NK_VEC) return launch_narrow_vec<T, NB>(np, ch, s);
     const bool plain_a = p.tA == (sizeof(T) == 4 ? T_F32 : T_F64) && p.round_in == TB_ROUND_NONE;
     void (*kern)(NarrowParams) = plain_a ? k_narrow<T, NB, true> : k_narrow<T, NB, false>;
     if constexpr (sizeof(T) == 4) {
@@ -1563,10 +1876,10 @@ cudaError_t launch_simt(const tb_plan* P, const tb_ptrs* d, cudaStream_t s)
 }  // namespace tb
 
 // The CUDA-core kernel a plan of the simt path runs, for operands aligned to
-// their element size (the launcher falls back to the register-prefetch or
-// tiled kernel for others): 0 tiled, 1 narrow with register prefetch, 2
-// narrow streaming, 3 narrow cooperative, 4 complex narrow streaming. No
-// device call.
+// their element size and, for 5, to the row vector (the launcher falls back
+// to another narrow or the tiled kernel for others): 0 tiled, 1 narrow with
+// register prefetch, 2 narrow streaming, 3 narrow cooperative, 4 complex
+// narrow streaming, 5 narrow with row vectors. No device call.
 extern "C" int tbk_simt_kernel(const tb_plan* P)
 {
     using namespace tb;

@@ -313,6 +313,24 @@ struct PackTab {
 };
 constexpr int PP_SMEM = PP_STAGES * PP_SLOT * 4 + 2 * (int)sizeof(PackTab);
 
+// multiply-high divisors of the pipelined pack's index arithmetic (every
+// extent, row count, contraction length and tile count below 2^31)
+struct PackDivs {
+    FastDiv rows[TB_MAXMODES], ks[TB_MAXMODES], ls[TB_MAXMODES];
+    FastDiv tiles_k, tiles_r, lsz;
+};
+
+__device__ __forceinline__ int64_t pp_decode(const ModeList& m, const FastDiv* f, uint32_t idx)
+{
+    int64_t o = 0;
+    for (int j = 0; j < m.n; j++) {
+        const uint32_t q = fdiv(idx, f[j]);
+        o += (int64_t)(idx - q * f[j].d) * m.s0[j];
+        idx = q;
+    }
+    return o;
+}
+
 __device__ __forceinline__ void cp_async16_zfill(uint32_t dst, const void* src, bool in)
 {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(in ? 16 : 0)
@@ -356,42 +374,43 @@ __device__ __forceinline__ void pp_put8(const PackParams& p, int64_t l, int64_t 
 }
 
 template <int SPLIT, int FMT, bool ROWS_FAST>
-__global__ void __launch_bounds__(PP_THREADS) k_pack_pipe(PackParams p, int64_t tiles_r, int64_t tiles_k, int64_t ntiles)
+__global__ void __launch_bounds__(PP_THREADS) k_pack_pipe(PackParams p, PackDivs dv, int32_t ntiles)
 {
     extern __shared__ __align__(16) float pp_sm[];
     float* slots = pp_sm;
     PackTab* tab = (PackTab*)(pp_sm + PP_STAGES * PP_SLOT);
     const int t = threadIdx.x;
-    const int64_t first = blockIdx.x, step = gridDim.x;
-    const int64_t nloc = first < ntiles ? (ntiles - 1 - first) / step + 1 : 0;
-    auto tile_of = [&](int64_t i, int64_t& r0, int64_t& k0, int64_t& l) {
-        int64_t j = first + i * step;
-        k0 = (j % tiles_k) * 64;
-        j /= tiles_k;
-        r0 = (j % tiles_r) * 64;
-        l = j / tiles_r;
+    const int32_t first = blockIdx.x, step = gridDim.x;
+    const int32_t nloc = first < ntiles ? (ntiles - 1 - first) / step + 1 : 0;
+    auto tile_of = [&](int32_t i, int64_t& r0, int64_t& k0, int64_t& l) {
+        const uint32_t j = (uint32_t)(first + i * step);
+        const uint32_t jk = fdiv(j, dv.tiles_k), jr = fdiv(jk, dv.tiles_r);
+        k0 = (int64_t)(j - jk * dv.tiles_k.d) * 64;
+        r0 = (int64_t)(jk - jr * dv.tiles_r.d) * 64;
+        l = jr;
     };
     // source offsets of tile i's 64 rows (threads 0-63) and 64 columns (64-127)
-    auto make_tab = [&](int64_t i, PackTab& tb) {
+    auto make_tab = [&](int32_t i, PackTab& tb) {
         if (i >= nloc) return;
-        int64_t r0, k0, l, o = 0, dummy;
+        int64_t r0, k0, l, o = 0;
         tile_of(i, r0, k0, l);
         if (t < 64) {
-            if (r0 + t < p.R) decode2(p.rows, r0 + t, o, dummy);
+            if (r0 + t < p.R) o = pp_decode(p.rows, dv.rows, (uint32_t)(r0 + t));
             tb.row[t] = o;
         } else {
             const int kk = t - 64;
-            if (k0 + kk < p.K) decode2(p.ks, k0 + kk, o, dummy);
+            if (k0 + kk < p.K) o = pp_decode(p.ks, dv.ks, (uint32_t)(k0 + kk));
             tb.k[kk] = o;
         }
         if (t == 0) {
-            const int64_t lsrc = p.srcs ? l % p.Lsz : l;
-            decode2(p.ls, lsrc, o, dummy);
-            tb.src = (const float*)(p.srcs ? p.srcs[l / p.Lsz] : p.src) + o;
+            const uint32_t b = p.srcs ? fdiv((uint32_t)l, dv.lsz) : 0u;
+            const uint32_t lsrc = (uint32_t)l - b * dv.lsz.d;
+            o = pp_decode(p.ls, dv.ls, p.srcs ? lsrc : (uint32_t)l);
+            tb.src = (const float*)(p.srcs ? p.srcs[b] : p.src) + o;
         }
     };
     // 1024 chunks of 16 bytes per tile, 8 per thread; outside the tensor: zeros
-    auto issue = [&](int64_t i, const PackTab& tb) {
+    auto issue = [&](int32_t i, const PackTab& tb) {
         if (i < nloc) {
             int64_t r0, k0, l;
             tile_of(i, r0, k0, l);
@@ -410,7 +429,7 @@ __global__ void __launch_bounds__(PP_THREADS) k_pack_pipe(PackParams p, int64_t 
         }
         pp_commit();  // empty groups keep the count uniform
     };
-    auto store = [&](int64_t i) {
+    auto store = [&](int32_t i) {
         int64_t r0, k0, l;
         tile_of(i, r0, k0, l);
         const float* v = slots + (i % PP_STAGES) * PP_SLOT;
@@ -452,7 +471,7 @@ __global__ void __launch_bounds__(PP_THREADS) k_pack_pipe(PackParams p, int64_t 
         issue(i, tab[i & 1]);
     }
     make_tab(PP_STAGES - 1, tab[(PP_STAGES - 1) & 1]);
-    for (int64_t i = 0; i < nloc; i++) {
+    for (int32_t i = 0; i < nloc; i++) {
         pp_wait<PP_STAGES - 2>();  // this thread's copies of tile i have landed
         __syncthreads();           // everyone's have; slot (i - 1) and table (i + S) are free
         issue(i + PP_STAGES - 1, tab[(i + PP_STAGES - 1) & 1]);
@@ -482,8 +501,29 @@ static bool launch_pack_pipe(const PackParams& pp, int64_t lz, cudaStream_t s)
     const int64_t tiles_r = (pp.R + 63) / 64, tiles_k = (pp.Kseg + 63) / 64;
     const int64_t ntiles = tiles_r * tiles_k * lz;
     const int64_t grid = std::min<int64_t>(ntiles, (int64_t)num_sms() * 3);
-    if (grid > 0) kern<<<(unsigned)grid, PP_THREADS, PP_SMEM, s>>>(pp, tiles_r, tiles_k, ntiles);
+    PackDivs dv;
+    memset(&dv, 0, sizeof(dv));
+    for (int j = 0; j < pp.rows.n; j++) dv.rows[j] = make_fastdiv((uint32_t)pp.rows.ext[j]);
+    for (int j = 0; j < pp.ks.n; j++) dv.ks[j] = make_fastdiv((uint32_t)pp.ks.ext[j]);
+    for (int j = 0; j < pp.ls.n; j++) dv.ls[j] = make_fastdiv((uint32_t)pp.ls.ext[j]);
+    dv.tiles_k = make_fastdiv((uint32_t)tiles_k);
+    dv.tiles_r = make_fastdiv((uint32_t)tiles_r);
+    dv.lsz = make_fastdiv((uint32_t)std::max<int64_t>(pp.Lsz, 1));
+    if (grid > 0) kern<<<(unsigned)grid, PP_THREADS, PP_SMEM, s>>>(pp, dv, (int32_t)ntiles);
     return true;
+}
+
+// the pipelined pack's 32-bit index arithmetic covers the operand
+static bool pack_pipe_fits(const PackParams& pp, int64_t lz)
+{
+    const int64_t lim = (int64_t)1 << 31;
+    const int64_t ntiles = ((pp.R + 63) / 64) * ((pp.Kseg + 63) / 64) * lz;
+    if (pp.R >= lim || pp.Kseg >= lim || pp.K >= lim || lz >= lim || ntiles >= lim) return false;
+    const ModeList* ms[3] = {&pp.rows, &pp.ks, &pp.ls};
+    for (const ModeList* m : ms)
+        for (int j = 0; j < m->n; j++)
+            if (m->ext[j] < 1 || m->ext[j] >= lim) return false;
+    return !pp.srcs || pp.Lsz >= 1;
 }
 
 template <bool RF>
@@ -529,7 +569,8 @@ static void launch_pack_real(const PackParams& pp, int split, int fmt, int64_t l
         const ModeList* others[3] = {rf ? &pp.ks : &pp.rows, &pp.ls, &pp.us};
         v4 = vec4_ok(rf ? pp.rows : pp.ks, others, 2, pp.src);
     }
-    if (v4 && (rf ? launch_pack_pipe3<true>(pp, split, fmt, lz, s) : launch_pack_pipe3<false>(pp, split, fmt, lz, s)))
+    if (v4 && pack_pipe_fits(pp, lz) &&
+        (rf ? launch_pack_pipe3<true>(pp, split, fmt, lz, s) : launch_pack_pipe3<false>(pp, split, fmt, lz, s)))
         return;
     if (rf) {
         if (v4) launch_pack_real3<T, true, 4>(pp, split, fmt, grid, s);

@@ -120,6 +120,50 @@ static void simplify(mlist* m, int key)
     m->n = w;
 }
 
+/* Element path: one thread per output, consecutive threads on consecutive
+ * outputs in F order (D's stride order). When the larger operand holds more
+ * than twice as many elements as D and is contiguous along an output mode
+ * (stride +-1), F is put in that operand's stride order instead (modes it
+ * lacks last, stable), so that a warp reads it in whole lines rather than
+ * one line per lane. Every output is computed the same way in either order. */
+static void order_outputs(tb_plan* P)
+{
+    tb_modes* F = &P->F;
+    double nA = (double)P->K.size * (double)P->UA.size, nB = (double)P->K.size * (double)P->UB.size;
+    for (int i = 0; i < F->n; i++) {
+        if (F->sA[i]) nA *= (double)F->ext[i];
+        if (F->sB[i]) nB *= (double)F->ext[i];
+    }
+    const int useA = nA >= nB;
+    const int64_t* s = useA ? F->sA : F->sB;
+    if ((useA ? nA : nB) <= 2.0 * (double)F->size) return;
+    int unit = 0;
+    for (int i = 0; i < F->n; i++)
+        if (s[i] == 1 || s[i] == -1) unit = 1;
+    if (!unit) return;
+    int64_t key[TB_MAXMODES];
+    for (int i = 0; i < F->n; i++) key[i] = s[i] ? iabs64(s[i]) : INT64_MAX;
+    for (int i = 1; i < F->n; i++) {
+        const int64_t k = key[i], e = F->ext[i], a = F->sA[i], b = F->sB[i], c = F->sC[i], d = F->sD[i];
+        int j = i - 1;
+        while (j >= 0 && key[j] > k) {
+            key[j + 1] = key[j];
+            F->ext[j + 1] = F->ext[j];
+            F->sA[j + 1] = F->sA[j];
+            F->sB[j + 1] = F->sB[j];
+            F->sC[j + 1] = F->sC[j];
+            F->sD[j + 1] = F->sD[j];
+            j--;
+        }
+        key[j + 1] = k;
+        F->ext[j + 1] = e;
+        F->sA[j + 1] = a;
+        F->sB[j + 1] = b;
+        F->sC[j + 1] = c;
+        F->sD[j + 1] = d;
+    }
+}
+
 static int to_modes(const mlist* m, tb_modes* out)
 {
     memset(out, 0, sizeof(*out));
@@ -429,6 +473,7 @@ int tb_build_plan(const tb_tensor_view* A, const tb_tensor_view* B,
         else if (f == TB_PATH_GENERIC || f == TB_PATH_REDUCE) path = f;
     }
     P->path = path;
+    if (path == TB_PATH_GENERIC) order_outputs(P);
     return 0;
 }
 
@@ -474,9 +519,9 @@ size_t tb_describe(const tb_plan* p, size_t maxlen, char* out)
     if (p->path == TB_PATH_SLICED) at = put(out, maxlen, at, " slices=%d", p->slices);
     if (p->path == TB_PATH_GENERIC) at = put(out, maxlen, at, " kernel=%s", tbk_generic_kernel(p) ? "warpdot" : "element");
     if (p->path == TB_PATH_SIMT) {
-        static const char* kern[] = {"tiled", "narrow", "narrow_stream", "narrow_coop", "narrow_cstream"};
+        static const char* kern[] = {"tiled", "narrow", "narrow_stream", "narrow_coop", "narrow_cstream", "narrow_vec"};
         const int k = tbk_simt_kernel(p);
-        if (k >= 0 && k <= 4) at = put(out, maxlen, at, " kernel=%s", kern[k]);
+        if (k >= 0 && k <= 5) at = put(out, maxlen, at, " kernel=%s", kern[k]);
     }
     at = put_modes(out, maxlen, at, "F", &p->F);
     at = put_modes(out, maxlen, at, "K", &p->K);

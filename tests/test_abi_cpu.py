@@ -261,12 +261,17 @@ def test_wait_selftest_argument_checks(tapp):
 
 
 @pytest.mark.parametrize("core,mode,rank,storage,prec,kernel", [
-    ([64, 40, 32, 32], 1, 38, 0, 0, "narrow_stream"),     # rows contiguous in A and D
+    ([64, 40, 32, 32], 1, 38, 0, 0, "narrow_vec"),        # rows contiguous in A, C and D: 4-row vectors
+    ([62, 40, 32, 32], 1, 38, 0, 0, "narrow_vec"),        # row extent even: 2-row vectors
+    ([63, 40, 32, 32], 1, 38, 0, 0, "narrow_stream"),     # odd row extent: a row per thread
     ([64, 40, 32, 32], 0, 38, 0, 0, "narrow_coop"),       # A along the contraction, D along the rank
-    ([64, 40, 32, 32], 1, 24, 0, 6, "narrow_stream"),     # bf16 precision: rounding after the copy
-    ([64, 40, 32, 32], 1, 24, 1, -1, "narrow_stream"),    # binary64, rows contiguous
+    ([64, 40, 32, 32], 1, 24, 0, 6, "narrow_vec"),        # bf16 precision: rounding after the copy
+    ([63, 40, 32, 32], 1, 24, 0, 6, "narrow_stream"),
+    ([64, 40, 32, 32], 1, 24, 1, -1, "narrow_vec"),       # binary64, rows contiguous
+    ([63, 40, 32, 32], 1, 24, 1, -1, "narrow_stream"),
     ([64, 40, 32, 32], 0, 38, 1, -1, "narrow"),           # binary64 with D along the rank
-    ([64, 40, 32, 32], 1, 60, 1, -1, "narrow"),           # binary64 wider than 48
+    ([64, 40, 32, 32], 1, 60, 1, -1, "narrow_vec"),       # binary64 wider than 48
+    ([63, 40, 32, 32], 1, 60, 1, -1, "narrow"),
     ([64, 40, 32, 32], 1, 24, 2, -1, "narrow_cstream"),   # complex float
     ([64, 40, 32, 32], 1, 24, 3, -1, "tiled"),            # complex double
 ])
@@ -294,4 +299,20 @@ def test_planner_reports_tiled_kernel_for_wide_products(tapp):
     D = alloc(0, [512, 384], [1, 512], [0, 1])
     plan, infos = _plan(tapp, Case(A, B, Cc, D, scalar(0, 1.0), scalar(0, 1.0), 0))
     assert " kernel=tiled " in tapp.describe(plan)
+    tapp.lib.TAPP_destroy_tensor_product(plan)
+
+
+def test_element_path_walks_the_larger_operand(tapp):
+    """Element-path Hadamard product whose A (5x D's size) is contiguous along
+    a batch mode while D is contiguous along A's last free mode: the plan
+    orders the outputs by A's strides (A's stride-1 mode first), so that
+    consecutive threads read consecutive elements of A."""
+    A = alloc(0, [8, 4, 5, 6, 7], [1, 8, 32, 160, 960], [0, 1, 4, 2, 3])
+    B = alloc(0, [6, 5, 8, 4], [1, 6, 30, 240], [2, 4, 0, 1])
+    Cc = alloc(0, [7, 6, 4, 8], [1, 7, 42, 168], [3, 2, 1, 0])
+    D = alloc(0, [7, 6, 4, 8], [1, 7, 42, 168], [3, 2, 1, 0])
+    plan, infos = _plan(tapp, Case(A, B, Cc, D, scalar(0, 1.0), scalar(0, 0.5), 0))
+    d = tapp.describe(plan)
+    assert "path=generic" in d and "kernel=element" in d, d
+    assert " F=[(8:1,30," in d, d
     tapp.lib.TAPP_destroy_tensor_product(plan)

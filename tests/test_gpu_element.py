@@ -77,3 +77,52 @@ def test_warpdot(tapp, oracle, gpu, name, dtype, prec, kw):
     bound = error_bound(case, scale, D64)
     bad = np.abs(d_values(runs[0].D) - D64) > bound
     assert not bad.any(), (name, int(bad.sum()))
+
+
+def _hadamard(rng, d_order, ext=(72, 8, 20, 30, 16)):
+    """D[l3,l2,l1,l0] = 0.9 sum_k A[l0,l1,k,l2,l3] B[l2,k,l0,l1] - 0.3 C (the
+    served mix's batched matrix-vector Hadamard kind): A contiguous along l0;
+    D's modes stored in the order d_order (labels)."""
+    e0, e1, ek, e2, e3 = ext
+    A = _t(rng, tapp_b200.TAPP_F32, [e0, e1, ek, e2, e3], "abkcd", [0, 1, 2, 3, 4])
+    B = _t(rng, tapp_b200.TAPP_F32, [e2, ek, e0, e1], "ckab", [0, 1, 2, 3])
+    ext_of = {"a": e0, "b": e1, "c": e2, "d": e3}
+    idx = "".join(d_order)
+    Cc = _t(rng, tapp_b200.TAPP_F32, [ext_of[c] for c in idx], idx, list(range(4)))
+    D = _t(rng, tapp_b200.TAPP_F32, [ext_of[c] for c in idx], idx, list(range(4)))
+    return Case(A, B, Cc, D, scalar(tapp_b200.TAPP_F32, 0.9), scalar(tapp_b200.TAPP_F32, -0.3), 0, False, "hadamard")
+
+
+def _logical(t, order):
+    """t's values as an array indexed in the label order `order`."""
+    import itertools
+    pos = {c: i for i, c in enumerate("".join(chr(x) for x in t.idx))}
+    out = np.empty([t.extents[pos[c]] for c in order], dtype=t.buf.dtype)
+    for coords in itertools.product(*[range(n) for n in out.shape]):
+        off = t.base + sum(coords[k] * t.strides[pos[c]] for k, c in enumerate(order))
+        out[coords] = t.buf[off]
+    return out
+
+
+def test_element_path_walks_the_larger_operand(tapp, oracle, gpu):
+    """Outputs walked in A's stride order (A contiguous along a batch mode, D
+    along another): within the oracle bound, and bit-identical to the same
+    product with D stored in A's order (outputs walked in D's order)."""
+    ext = (72, 8, 6, 10, 5)
+    walked = _hadamard(np.random.default_rng(91), "dcba", ext)
+    plain = _hadamard(np.random.default_rng(91), "abcd", ext)
+    # the same values in both (A and B are drawn alike; C copied in logical order)
+    plain.C.buf[plain.C.base + plain.C.offsets()] = _logical(walked.C, "abcd").reshape(-1, order="F")
+    assert "kernel=element" in _describe(tapp, walked) and " F=[(72:1," in _describe(tapp, walked)
+    runs = {}
+    for name, case in (("walked", walked), ("plain", plain)):
+        run = case.copy()
+        assert run_on_device(tapp, run) == 0
+        runs[name] = _logical(run.D, "abcd")
+    assert np.array_equal(runs["walked"].view(np.uint8), runs["plain"].view(np.uint8))
+    e64, D64, scale = oracle.execute_f64(walked.copy())
+    assert e64 == 0
+    run = walked.copy()
+    assert run_on_device(tapp, run) == 0
+    bound = error_bound(walked, scale, D64)
+    assert not (np.abs(d_values(run.D) - D64) > bound).any()

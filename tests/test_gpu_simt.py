@@ -12,6 +12,7 @@ import tapp_b200
 from tapp_b200.workloads import dense_contraction_case, large_dense_case
 from families import bounded_case
 from test_gpu_parity import check_against_f64
+from helpers import run_on_device
 
 pytestmark = pytest.mark.gpu
 
@@ -222,6 +223,59 @@ def test_first_mode_products_beta_zero_and_aliased_c(tapp, oracle, gpu, prec, ra
     torch.cuda.synchronize()
     assert torch.equal(aliased, dev[3])
     tapp.lib.TAPP_destroy_tensor_product(plan)
+    tapp.lib.TAPP_destroy_executor(ex)
+
+
+def _padded_rows(case):
+    """The same product with every tensor's first mode padded by one element
+    (leading stride extent + 1): values unchanged, row vectors impossible."""
+    from tapp_b200.case import alloc
+    out = case.copy()
+    for name in ("A", "C", "D"):
+        t = getattr(case, name)
+        if t.strides[0] != 1:
+            continue
+        strides, acc = [], 1
+        for j, e in enumerate(t.extents):
+            strides.append(acc)
+            acc *= e + 1 if j == 0 else e
+        u = alloc(t.dtype, list(t.extents), strides, list(t.idx))
+        u.op = t.op
+        u.buf[u.base + u.offsets()] = t.buf[t.base + t.offsets()]
+        setattr(out, name, u)
+    return out
+
+
+@pytest.mark.parametrize("storage,prec", [(0, 0), (0, 6), (1, -1)])
+@pytest.mark.parametrize("core,mode,rank", [([64, 40, 36], 1, 38), ([64, 40, 36], 2, 24), ([62, 33, 40], 1, 8),
+                                            ([62, 33, 40], 2, 60), ([32, 48, 64], 1, 64)])
+def test_mode_n_products_row_vectors(tapp, oracle, gpu, storage, prec, core, mode, rank):
+    """Mode-n products on an inner mode with A, C and D contiguous along their
+    rows (the register-tiled kernel, 4- or 2-row vectors; widths 8 to 64,
+    beta = 0 too): within the binary64 bound, and bit-identical to the same
+    product with padded rows, which runs a one-row-per-thread kernel with the
+    same summation order."""
+    from tapp_b200.case import scalar
+    rng = np.random.default_rng(400 + rank + 7 * storage + prec + mode)
+    d_ext = list(core)
+    d_ext[mode] = rank
+    d_idx = [0, 1, 2]
+    d_idx[mode] = 3
+    case = spec_case(rng, storage, prec, ([*core], [rank, core[mode]], d_ext, d_ext),
+                     ([0, 1, 2], [3, mode], d_idx, d_idx), "tucker")
+    if rank == 8:
+        case.beta = scalar(case.D.dtype, 0.0)
+    ex = tapp.create_executor()
+    assert "kernel=narrow_vec" in describe(tapp, case, ex), describe(tapp, case, ex)
+    padded = _padded_rows(case)
+    assert "kernel=narrow_vec" not in describe(tapp, padded, ex)
+    check_against_f64(tapp, oracle, case, device=True, executor=ex)
+    runs = []
+    for c in (case, padded):
+        run = c.copy()
+        assert run_on_device(tapp, run, ex) == 0
+        runs.append(run.D.buf[run.D.base + run.D.offsets()].copy())
+    assert np.array_equal(runs[0].view(np.uint8), runs[1].view(np.uint8))
     tapp.lib.TAPP_destroy_executor(ex)
 
 
