@@ -81,6 +81,9 @@ def parse():
     ap.add_argument("--only-chain", action="store_true", help="print only the Tucker-chain measurement")
     ap.add_argument("--only-tucker", action="store_true", help="print only the Tucker mode-n measurement")
     ap.add_argument("--only-tiny", action="store_true", help="print only the small-product latency measurement")
+    ap.add_argument("--only-small", action="store_true",
+                    help="print only the small configurations and the element-path measurement")
+    ap.add_argument("--only-element", action="store_true", help="print only the element-path measurement")
     ap.add_argument("--slices", type=str, default="7,8", help="digit slices of the sliced binary64 runs")
     ap.add_argument("--double-ab", type=int, default=160, help="extent of a, b, e, f in the binary64 workload")
     ap.add_argument("--double-ij", type=int, default=40, help="extent of i, j in the binary64 workload")
@@ -528,6 +531,47 @@ def small_configs_measure(lib, torch, with_cpu=True, steps=200, e2e_calls=50):
     return out
 
 
+def element_measure(lib, torch, steps=20, warmup=3):
+    """Element-path products through the C ABI, operands in HBM; device time
+    per product (CUDA events) and algorithmic bytes (A + B + C + D spans):
+      hadamard  the served mix's largest batched Hadamard product of the first
+                140 requests: D[l3,l2,l1,l0] = sum_k A[l0,l1,k,l2,l3]
+                B[l2,k,l0,l1] + C, extents l0..l3 = 72, 8, 74, 67, k = 69,
+                float32 (A 790 MB, contiguous along l0; D along l3): the
+                outputs are walked in A's stride order;
+      matvec    batched matrix-vector D[m,h] = sum_k A[k,m,h] B[k,h] + C,
+                k = 300, m = 2000, h = 64, A contiguous along k: one warp per
+                output (k_warpdot);
+      c2        the mixed-class complex product (element kernel)."""
+    from tapp_b200.workloads import RequestSpec, case_from_spec, mixed_classes_case
+    stream = torch.cuda.current_stream().cuda_stream
+    specs = {
+        "hadamard": RequestSpec("hadamard", 0, 0, ([72, 8, 69, 74, 67], [74, 69, 72, 8], [67, 74, 8, 72], [67, 74, 8, 72]),
+                                ([0, 1, 4, 2, 3], [2, 4, 0, 1], [3, 2, 1, 0], [3, 2, 1, 0]), 0.9, -0.3),
+        "matvec": RequestSpec("hadamard", 0, 0, ([300, 2000, 64], [300, 64], [2000, 64], [2000, 64]),
+                              ([0, 1, 2], [0, 2], [1, 2], [1, 2]), 0.9, -0.3),
+    }
+    out = {}
+    for name in ("hadamard", "matvec", "c2"):
+        if name == "c2":
+            case = mixed_classes_case(np.random.default_rng(0x7A990002))
+            nbytes = sum(t.buf.nbytes for t in (case.A, case.B, case.C, case.D))
+        else:
+            case = case_from_spec(np.random.default_rng(11), specs[name])
+            nbytes = sum(specs[name].nbytes(k) for k in range(4))
+        dev = [to_device(t, torch) for t in (case.A, case.B, case.C, case.D)]
+        ex = make_executor(lib, stream)
+        prod = Product(lib, case, [d[1] for d in dev], ex)
+        desc = lib.describe(prod.plan)
+        ms = time_device(torch, prod, steps, warmup, lambda: None)
+        out[name] = {"kernel": desc.split("kernel=")[1].split()[0] if "kernel=" in desc else desc.split()[0],
+                     "us": ms * 1e3, "bytes": nbytes, "gbs": nbytes / (ms * 1e-3) / 1e9}
+        prod.close()
+        lib.lib.TAPP_destroy_executor(ex)
+        del dev
+    return out
+
+
 def tiny_latency_measure(lib, torch, n=2000):
     """Latency of small products (the element path: the mixed-class
     configuration, complex float with Hadamard, diagonal and unary modes, and
@@ -942,6 +986,15 @@ def run_b200(args):
         if rank == 0:
             print(json.dumps(tiny_latency_measure(lib, torch)), flush=True)
         return
+    if args.only_element:
+        if rank == 0:
+            print(json.dumps(element_measure(lib, torch)), flush=True)
+        return
+    if args.only_small:
+        if rank == 0:
+            print(json.dumps({"small_configs": small_configs_measure(lib, torch, with_cpu=False),
+                              "element": element_measure(lib, torch)}), flush=True)
+        return
     if args.only_batched:
         if rank == 0:
             print(json.dumps(batched_measure(lib, torch)), flush=True)
@@ -1055,6 +1108,7 @@ def run_b200(args):
 
     small = small_configs_measure(lib, torch, with_cpu=(rank == 0 and not args.no_cpu)) \
         if world == 1 and not args.no_modes else None
+    element = element_measure(lib, torch) if world == 1 and not args.no_modes else None
 
     served = None
     if world == 1 and args.served > 0:
@@ -1087,7 +1141,7 @@ def run_b200(args):
                 "max_abs_err_rel_to_max": head_err,
                 "error_reference": "binary64 evaluation of D[:,:,:,0:2] from the same stored inputs",
                 "vs_plain_gpu": (value / world / plain) if plain else None,
-                "modes": modes, "small_configs": small, "batched": batched, "tucker_chain": chain,
+                "modes": modes, "small_configs": small, "element": element, "batched": batched, "tucker_chain": chain,
                 "tucker": tucker, "tiny_latency": tiny, "double": double, "served": served, "roofline": roofline, "e2e": e2e,
                 "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": gpu_launches}
         print(json.dumps(line), flush=True)
