@@ -22,6 +22,7 @@ struct GenParams {
     int32_t nF, nK, nUA, nUB;
     int32_t tA, tB, tC, tD;
     int32_t round_in, conjA, conjB, conjC, conjD, conjD_f32, beta_zero, small_F;
+    int32_t warp, pad_;  // warp: one warp per output (warp_element), else one thread (element)
     int64_t sizeF, sizeK, sizeUA, sizeUB;
     double alpha_re, alpha_im, beta_re, beta_im;
     FastDiv fF[TB_MAXMODES];
@@ -155,7 +156,35 @@ __device__ __forceinline__ void element(const GenParams& p, const void* A, const
     int64_t kc[TB_MAXMODES];
     for (int j = 0; j < p.nK; j++) kc[j] = 0;
     int64_t kA = oA, kB = oB;
-    for (int64_t k = 0; k < p.sizeK; k++) {
+    int64_t k0 = 0;
+    if (p.nUA == 0 && p.nUB == 0) {
+        // no unary modes: UNR terms' loads issued together, then their
+        // multiply-adds in order (the same values and order as below)
+        constexpr int UNR = (CPLX || sizeof(R) == 8) ? 4 : 8;
+        for (; k0 + UNR <= p.sizeK; k0 += UNR) {
+            R ar[UNR], ai[UNR], br[UNR], bi[UNR];
+#pragma unroll
+            for (int u = 0; u < UNR; u++) {
+                load_rounded<R>(A, kA, p.tA, p.round_in, ar[u], ai[u]);
+                load_rounded<R>(B, kB, p.tB, p.round_in, br[u], bi[u]);
+                for (int j = 0; j < p.nK; j++) {
+                    kA += p.K_sA[j];
+                    kB += p.K_sB[j];
+                    if (++kc[j] < p.K_ext[j]) break;
+                    kA -= p.K_sA[j] * p.K_ext[j];
+                    kB -= p.K_sB[j] * p.K_ext[j];
+                    kc[j] = 0;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < UNR; u++) {
+                if (p.conjA) ai[u] = -ai[u];
+                if (p.conjB) bi[u] = -bi[u];
+                cmac<R, CPLX>(sr, si, ar[u], ai[u], br[u], bi[u]);
+            }
+        }
+    }
+    for (int64_t k = k0; k < p.sizeK; k++) {
         R ar, ai, br, bi;
         unary_sum<R, CPLX>(A, kA, p.tA, p.conjA, p.round_in, p.nUA, p.sizeUA, p.UA_ext, p.UA_s, ar, ai);
         unary_sum<R, CPLX>(B, kB, p.tB, p.conjB, p.round_in, p.nUB, p.sizeUB, p.UB_ext, p.UB_s, br, bi);
@@ -195,8 +224,9 @@ __device__ __forceinline__ void warp_element(const GenParams& p, const void* A, 
         int64_t oA, oB, oC, oD;
         free_offsets(p, i, oA, oB, oC, oD);
         R sr = 0, si = 0;
-        for (int64_t k = lane; k < p.sizeK; k += 32) {
-            int64_t kA = oA, kB = oB;
+        auto term_offsets = [&](int64_t k, int64_t& kA, int64_t& kB) {
+            kA = oA;
+            kB = oB;
             uint32_t r = (uint32_t)k;
             for (int j = 0; j < p.nK; j++) {
                 const uint32_t q = j + 1 < p.nK ? fdiv(r, p.fK[j]) : 0;
@@ -205,6 +235,30 @@ __device__ __forceinline__ void warp_element(const GenParams& p, const void* A, 
                 kA += c * p.K_sA[j];
                 kB += c * p.K_sB[j];
             }
+        };
+        int64_t k0 = lane;
+        if (p.nUA == 0 && p.nUB == 0) {
+            // the lane's next 4 terms loaded together, then added in order
+            for (; k0 + 3 * 32 < p.sizeK; k0 += 4 * 32) {
+                R ar[4], ai[4], br[4], bi[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    int64_t kA, kB;
+                    term_offsets(k0 + 32 * u, kA, kB);
+                    load_rounded<R>(A, kA, p.tA, p.round_in, ar[u], ai[u]);
+                    load_rounded<R>(B, kB, p.tB, p.round_in, br[u], bi[u]);
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    if (p.conjA) ai[u] = -ai[u];
+                    if (p.conjB) bi[u] = -bi[u];
+                    cmac<R, CPLX>(sr, si, ar[u], ai[u], br[u], bi[u]);
+                }
+            }
+        }
+        for (int64_t k = k0; k < p.sizeK; k += 32) {
+            int64_t kA, kB;
+            term_offsets(k, kA, kB);
             R ar, ai, br, bi;
             unary_sum<R, CPLX>(A, kA, p.tA, p.conjA, p.round_in, p.nUA, p.sizeUA, p.UA_ext, p.UA_s, ar, ai);
             unary_sum<R, CPLX>(B, kB, p.tB, p.conjB, p.round_in, p.nUB, p.sizeUB, p.UB_ext, p.UB_s, br, bi);
@@ -244,6 +298,13 @@ __global__ void __launch_bounds__(256) k_elementwise_group(const GenParams* __re
     const GenParams& p = params[lo];
     const tb_ptrs q = ptrs[lo];
     const int64_t nb = first[lo + 1] - first[lo];
+    if (p.warp) {
+        const int64_t warps = nb * (blockDim.x >> 5);
+        for (int64_t i = ((int64_t)blockIdx.x - first[lo]) * (blockDim.x >> 5) + (threadIdx.x >> 5); i < p.sizeF;
+             i += warps)
+            warp_element<R, CPLX>(p, q.A, q.B, q.C, q.D, i, threadIdx.x & 31);
+        return;
+    }
     const int64_t stride = nb * blockDim.x;
     for (int64_t i = ((int64_t)blockIdx.x - first[lo]) * blockDim.x + threadIdx.x; i < p.sizeF; i += stride)
         element<R, CPLX>(p, q.A, q.B, q.C, q.D, i);
@@ -352,6 +413,8 @@ size_t reduce_scratch_bytes(const tb_plan* P, size_t real_bytes)
     return S > 1 ? (size_t)S * (size_t)P->F.size * 2 * real_bytes : 0;
 }
 
+static bool warpdot_ok(const GenParams& g);
+
 static void fill_params(const tb_plan* P, GenParams& g)
 {
     memset(&g, 0, sizeof(g));
@@ -377,15 +440,22 @@ static void fill_params(const tb_plan* P, GenParams& g)
     }
     for (int j = 0; j < P->UA.n; j++) { g.UA_ext[j] = P->UA.ext[j]; g.UA_s[j] = P->UA.sA[j]; }
     for (int j = 0; j < P->UB.n; j++) { g.UB_ext[j] = P->UB.ext[j]; g.UB_s[j] = P->UB.sB[j]; }
+    g.warp = warpdot_ok(g) ? 1 : 0;
 }
 
-// Element path kernel: the warp per output (k_warpdot) when an operand is
-// contiguous along the contraction while consecutive outputs step it by a
-// stride other than 0 or 1 (one thread per output would read it a row apart
-// from lane to lane), for contractions of at least 64 terms.
+// Element path kernel: the warp per output (k_warpdot)
+//   - when an operand is contiguous along the contraction while consecutive
+//     outputs step it by a stride other than 0 or 1 (one thread per output
+//     would read it a row apart from lane to lane), for contractions of at
+//     least 64 terms;
+//   - when one thread per output makes less than a wave (fewer than 148 x 256
+//     outputs) and each output sums at least 8 terms with at least 64 loads
+//     in all (unary sums included): the lanes share the terms.
 static bool warpdot_ok(const GenParams& g)
 {
-    if (g.sizeK < 64 || g.sizeK >= (1ll << 31) || g.nK < 1 || g.nF < 1) return false;
+    if (g.sizeK >= (1ll << 31) || g.nK < 1 || g.nF < 1) return false;
+    if (g.sizeF < 148 * 256 && g.sizeK >= 8 && (double)g.sizeK * (double)(g.sizeUA + g.sizeUB) >= 64.0) return true;
+    if (g.sizeK < 64) return false;
     auto a = [](int64_t x) { return x < 0 ? -x : x; };
     // not when consecutive outputs already walk the other operand along its
     // contiguous mode (threads per output read that one in whole lines)
@@ -423,7 +493,7 @@ static cudaError_t launch_typed(const GenParams& g, int path, const tb_ptrs* d, 
         count_launch(2);
         cudaFreeAsync(ws, s);
         return e;
-    } else if (warpdot_ok(g)) {
+    } else if (g.warp) {
         int64_t blocks = (g.sizeF + 7) / 8;  // 8 warps, one output each
         if (blocks > 148 * 32) blocks = 148 * 32;
         if (blocks < 1) blocks = 1;
@@ -459,7 +529,8 @@ cudaError_t launch_generic_group(const tb_plan* const* P, const tb_ptrs* d, int 
         fill_params(P[j], hp[j]);
         hq[j] = d[j];
         hf[j] = blocks;
-        int64_t b = (P[j]->F.size + 255) / 256;
+        // warp-per-output products: 8 outputs per block
+        int64_t b = hp[j].warp ? (P[j]->F.size + 7) / 8 : (P[j]->F.size + 255) / 256;
         if (b > 148 * 8) b = 148 * 8;
         if (b < 1) b = 1;
         blocks += b;
@@ -675,7 +746,7 @@ void loop_fill(void* slot, const tb_plan* P, const tb_ptrs* d)
     if (P->path == TB_PATH_NOOP) s->p.sizeF = 0;  // nothing to write (empty D, or a precision left as is)
     s->q = *d;
     s->compute = P->compute;
-    s->warp = warpdot_ok(s->p) ? 1 : 0;
+    s->warp = s->p.warp;
 }
 
 // device state of a loop: the ring copy, its sequence words, the arrival
@@ -711,5 +782,5 @@ extern "C" int tbk_generic_kernel(const tb_plan* P)
 {
     tb::GenParams g;
     tb::fill_params(P, g);
-    return tb::warpdot_ok(g) ? 1 : 0;
+    return g.warp;
 }

@@ -1188,13 +1188,15 @@ __global__ void __launch_bounds__(256) k_narrow_cstream(NarrowParams np)
 
 // Register-tiled narrow kernel for A, C and D contiguous along their first
 // row mode, VR rows to one vector (binary32: VR = 4, 16 bytes, or 2 when the
-// row extents only allow pairs; binary64: VR = 2). A block of NB / 8 x 64
-// threads takes tiles of TR = 64 VR rows. Per chunk of KC contracted values
-// (16 KiB of A) the whole block copies the tile's chunk with cp.async as
-// VR-row vectors into a ring of 4 chunks laid out [k][row]; thread t always
-// copies row group t % 64, so it decodes one row offset per tile. After a
-// block barrier, thread (column group c, half h, lane) multiplies row group
-// 32 h + lane by columns 8c..8c+7: per contracted value one vector of A and
+// row extents only allow pairs; binary64: VR = 2). A block of NB / 8 x H
+// warps (H = 2 for binary32, 4 for binary64, whose tiles hold half as many
+// rows per byte) takes tiles of TR = 32 H VR rows. Per chunk of KC
+// contracted values (16 KiB of A) the whole block copies the tile's chunk
+// with cp.async as VR-row vectors into a ring of S chunks (4; 3 for
+// binary64, so that two blocks fit an SM) laid out [k][row]; thread t always
+// copies row group t % 32H, so it decodes one row offset per tile. After a
+// block barrier, thread (column group c, warp h of c, lane) multiplies row
+// group 32 h + lane by columns 8c..8c+7: per contracted value one vector of A and
 // two (binary64: four) 16-byte broadcast reads of the B panel feed 8 VR
 // independent multiply-adds. At the start of each tile a thread copies the C
 // vectors of its own outputs into its own part of a shared-memory buffer
@@ -1231,15 +1233,23 @@ __device__ __forceinline__ void cp_async_vec(uint32_t dst, const void* src)
     else asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
 }
 
-constexpr int NVEC_STAGES = 4, NVEC_CHUNK_BYTES = 16384, NVEC_MAX_SMEM = 200 * 1024;
+constexpr int NVEC_CHUNK_BYTES = 16384, NVEC_MAX_SMEM = 200 * 1024;
 
-template <typename T, int VR>
-constexpr int nvec_kc() { return NVEC_CHUNK_BYTES / (64 * VR * (int)sizeof(T)); }
+// H: warps per column group (TR = 32 H VR rows per tile); S: chunks in the
+// ring. Binary64 up to width 32 takes 4 warps per column group (at most 512
+// threads of about 80 registers) and 3 chunks, so that two blocks fit an SM.
+template <typename T, int NB>
+struct NarrowVecShape {
+    static constexpr bool WIDE = sizeof(T) == 8 && NB <= 32;
+    static constexpr int H = WIDE ? 4 : 2;
+    static constexpr int S = WIDE ? 3 : 4;
+};
 
 template <typename T, int NB, int VR, bool RND>
-__global__ void __launch_bounds__(NB * 8) k_narrow_vec(NarrowParams np)
+__global__ void __launch_bounds__(NB * 4 * NarrowVecShape<T, NB>::H) k_narrow_vec(NarrowParams np)
 {
-    constexpr int NT = NB * 8, TR = 64 * VR, KC = nvec_kc<T, VR>(), S = NVEC_STAGES;
+    constexpr int H = NarrowVecShape<T, NB>::H, S = NarrowVecShape<T, NB>::S;
+    constexpr int RG = 32 * H, NT = NB / 8 * RG, TR = RG * VR, KC = NVEC_CHUNK_BYTES / (TR * (int)sizeof(T));
     using NV = NarrowVec<T, VR>;
     using V = typename NV::V;
     const Params& p = np.p;
@@ -1304,9 +1314,9 @@ __global__ void __launch_bounds__(NB * 8) k_narrow_vec(NarrowParams np)
             oD += c * p.cm.s1[j];
         }
     };
-    // producer: thread t copies row group t % 64 at contracted values t / 64, t / 64 + NT / 64, ...
-    const int prg = t % 64, pk0 = t / 64;
-    constexpr int PKS = NT / 64;
+    // producer: thread t copies row group t % RG at contracted values t / RG, t / RG + NT / RG, ...
+    const int prg = t % RG, pk0 = t / RG;
+    constexpr int PKS = NT / RG;
     const uint32_t ring_base = (uint32_t)__cvta_generic_to_shared(ring) + (uint32_t)(prg * VR * sizeof(T));
     int64_t p_tile = -1, p_oA = -1;
     int p_chunk = 0;
@@ -1331,7 +1341,7 @@ __global__ void __launch_bounds__(NB * 8) k_narrow_vec(NarrowParams np)
     for (int g = 0; g < S - 1; g++) issue(g);
 
     const int lane = t & 31, w = t >> 5;
-    const int cg = w >> 1, crg = (w & 1) * 32 + lane;
+    const int cg = w / H, crg = (w % H) * 32 + lane;
     const T al = (T)p.alpha, be = (T)p.beta;
     T acc[VR][8];
     const uint32_t cs_base = (uint32_t)__cvta_generic_to_shared(Cs) + (uint32_t)((cg * 8 * TR + crg * VR) * sizeof(T));
@@ -1395,7 +1405,7 @@ __global__ void __launch_bounds__(NB * 8) k_narrow_vec(NarrowParams np)
                 // the tile's C copies went with the group of its first chunk:
                 // at most nchunks - 1 younger groups may still be pending
                 if (!p.beta_zero && nchunks < S) {
-                    static_assert(S == 4, "the waits below cover nchunks = 1 .. S - 1");
+                    static_assert(S <= 4, "the waits below cover nchunks = 1 .. 3");
                     if (nchunks == 1) cp_async_wait<0>();
                     else if (nchunks == 2) cp_async_wait<1>();
                     else cp_async_wait<2>();
@@ -1687,7 +1697,9 @@ static NarrowChoice narrow_choice(const simt::Params& p, int nb, size_t es)
     c.vr = 0;
     if (p.tA == t_own && p.tD == t_own && (p.beta_zero || p.tC == t_own) && (f32 || !c.rnd)) {
         const int vr = f32 ? (nvec_layout(p, 4, es) ? 4 : nvec_layout(p, 2, es) ? 2 : 0) : (nvec_layout(p, 2, es) ? 2 : 0);
-        const size_t vsmem = (size_t)NVEC_STAGES * NVEC_CHUNK_BYTES + (p.beta_zero ? 0 : es * (size_t)nb * 64 * vr) +
+        const bool wide = !f32 && nb <= 32;  // NarrowVecShape
+        const int H = wide ? 4 : 2, S = wide ? 3 : 4;
+        const size_t vsmem = (size_t)S * NVEC_CHUNK_BYTES + (p.beta_zero ? 0 : es * (size_t)nb * 32 * H * vr) +
                              es * (size_t)nb * (size_t)p.K + 8 * ((size_t)p.K + 2 * (size_t)nb);
         if (vr && vsmem <= (size_t)NVEC_MAX_SMEM) {
             c.kind = NK_VEC;
@@ -1745,8 +1757,9 @@ static cudaError_t launch_narrow_vec(simt::NarrowParams& np, const NarrowChoice&
         if (e != cudaSuccess) return e;
         if (dev >= 0 && dev < 64) attr_done[dev][variant] = 1;
     }
-    const int threads = NB * 8;
-    const int64_t tiles = (p.M + 64 * ch.vr - 1) / (64 * ch.vr);
+    constexpr int H = NarrowVecShape<T, NB>::H;
+    const int threads = NB * 4 * H;
+    const int64_t tiles = (p.M + 32 * H * ch.vr - 1) / (32 * H * ch.vr);
     int per_sm = 1;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, ch.smem) != cudaSuccess || per_sm < 1)
         per_sm = 1;

@@ -295,12 +295,12 @@ static int tc_groupable(const struct tb_server* s, const srv_req* r)
     return s->settings.tile ? s->settings.tile : tb_tile_choice(P);
 }
 
-/* element-path products of modest work that the grouped element kernel
- * computes with the same bits as their own launch (not those that run one
- * warp per output alone) */
+/* element-path products of modest work: the grouped element kernel runs
+ * each with its own launch's per-output function (a thread, or a warp, per
+ * output), so the bits are those of its own launch */
 static int groupable(const tb_plan* P)
 {
-    return P->path == TB_PATH_GENERIC && !tbk_generic_kernel(P) && P->F.size <= SRV_GROUP_MAX_OUT &&
+    return P->path == TB_PATH_GENERIC && P->F.size <= SRV_GROUP_MAX_OUT &&
            (double)P->F.size * (double)P->K.size * (double)(P->UA.size + P->UB.size) <= (double)SRV_GROUP_MAX_WORK;
 }
 

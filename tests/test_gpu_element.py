@@ -126,3 +126,23 @@ def test_element_path_walks_the_larger_operand(tapp, oracle, gpu):
     assert run_on_device(tapp, run) == 0
     bound = error_bound(walked, scale, D64)
     assert not (np.abs(d_values(run.D) - D64) > bound).any()
+
+
+def test_small_grid_runs_a_warp_per_output(tapp, oracle, gpu):
+    """The mixed-class complex product (17,280 outputs, less than a wave of
+    threads; 24 diagonal terms with unary sums of 6 and 5 values each): one
+    warp per output, lanes over the terms. Within the oracle bound, and the
+    same bits in two runs."""
+    from tapp_b200.workloads import mixed_classes_case
+    case = mixed_classes_case(np.random.default_rng(0x7A990002))
+    assert "kernel=warpdot" in _describe(tapp, case)
+    runs = []
+    for _ in range(2):
+        run = case.copy()
+        assert run_on_device(tapp, run) == 0
+        runs.append(run)
+    assert np.array_equal(runs[0].D.buf.view(np.uint8), runs[1].D.buf.view(np.uint8))
+    e64, D64, scale = oracle.execute_f64(case.copy())
+    assert e64 == 0
+    bound = error_bound(case, scale, D64)
+    assert not (np.abs(d_values(runs[0].D) - D64) > bound).any()

@@ -247,7 +247,7 @@ def _padded_rows(case):
 
 
 @pytest.mark.parametrize("storage,prec", [(0, 0), (0, 6), (1, -1)])
-@pytest.mark.parametrize("core,mode,rank", [([64, 40, 36], 1, 38), ([64, 40, 36], 2, 24), ([62, 33, 40], 1, 8),
+@pytest.mark.parametrize("core,mode,rank", [([64, 40, 36], 1, 38), ([64, 40, 36], 2, 24), ([62, 33, 80], 1, 8),
                                             ([62, 33, 40], 2, 60), ([32, 48, 64], 1, 64)])
 def test_mode_n_products_row_vectors(tapp, oracle, gpu, storage, prec, core, mode, rank):
     """Mode-n products on an inner mode with A, C and D contiguous along their
