@@ -286,25 +286,25 @@ __global__ void __launch_bounds__(256, 4) k_pack_real(PackParams p)
     }
 }
 
-// Pipelined pack for binary32 sources read 16 bytes at a time (the VEC = 4
-// case above: the fast mode has stride 1 and an extent divisible by 4, every
-// other stride keeps 16-byte alignment). Persistent blocks of 128 threads walk
-// the 64 x 64 tiles (block b: tiles b, b + grid, ...) and copy each tile into
-// a ring of PP_STAGES shared-memory slots with cp.async, PP_STAGES - 1 tiles
+// Pipelined pack for binary32 sources contiguous along the contraction and
+// read 16 bytes at a time (the VEC = 4, K-fast case above: the first
+// contracted mode has stride 1 and an extent divisible by 4, every other
+// stride keeps 16-byte alignment). Persistent blocks of 128 threads walk the
+// 64 x 64 tiles (block b: tiles b, b + grid, ...) and copy each tile into a
+// ring of PP_STAGES shared-memory slots with cp.async, PP_STAGES - 1 tiles
 // ahead of the one being written out, so a block keeps ~48 KiB of loads in
 // flight without holding them in registers (the one-tile kernel above has one
-// load phase and one store phase per block). Slot layouts, both read without
-// bank conflicts:
-//   K fast    [r][k], 68 floats per row; thread (r, g) reads k = 8g..8g+7 as
-//             two 16-byte reads, lanes 4-7 of each quarter-warp reading their
-//             second half first;
-//   rows fast [r / 4][k] of float4 (4 consecutive rows, as copied), 65 float4
-//             per row group; thread (r4, g) reads 8 float4 = rows 4 r4..4 r4 + 3
-//             at k = 8g..8g+7, quarter-warps over 8 row groups.
-// Output words and their order are those of k_pack_real (same rounding, same
-// [hi | lo] or three-segment split), so the two kernels write identical panels.
-constexpr int PP_THREADS = 128, PP_STAGES = 4, PP_PITCH = 68, PP_P4 = 65;
-constexpr int PP_SLOT = 64 * PP_PITCH;  // floats per slot (the rows-fast layout needs 16 * 65 * 4)
+// load phase and one store phase per block). Slot layout [r][k], 68 floats
+// per row, read without bank conflicts: thread (r, g) reads k = 8g..8g+7 as
+// two 16-byte reads, lanes 4-7 of each quarter-warp reading their second half
+// first. Output words and their order are those of k_pack_real (same
+// rounding, same [hi | lo] or three-segment split), so the two kernels write
+// identical panels. On the 64^4 contraction's B operand: 23.2 us against
+// 26.9 us for k_pack_real; for sources contiguous along the rows the
+// transposed reads made it slower than k_pack_real (41.8 against 28.0 us),
+// so those keep k_pack_real.
+constexpr int PP_THREADS = 128, PP_STAGES = 4, PP_PITCH = 68;
+constexpr int PP_SLOT = 64 * PP_PITCH;  // floats per slot
 struct PackTab {
     int64_t row[64];
     int64_t k[64];
@@ -373,7 +373,7 @@ __device__ __forceinline__ void pp_put8(const PackParams& p, int64_t l, int64_t 
     }
 }
 
-template <int SPLIT, int FMT, bool ROWS_FAST>
+template <int SPLIT, int FMT>
 __global__ void __launch_bounds__(PP_THREADS) k_pack_pipe(PackParams p, PackDivs dv, int32_t ntiles)
 {
     extern __shared__ __align__(16) float pp_sm[];
@@ -418,11 +418,8 @@ __global__ void __launch_bounds__(PP_THREADS) k_pack_pipe(PackParams p, PackDivs
 #pragma unroll
             for (int u = 0; u < 8; u++) {
                 const int c = t + PP_THREADS * u;
-                const int fg = c % 16, sl = c / 16;
-                const int r = ROWS_FAST ? fg * 4 : sl;
-                const int kk = ROWS_FAST ? sl : fg * 4;
-                const uint32_t dst = ROWS_FAST ? sb + (uint32_t)(fg * PP_P4 + kk) * 16u
-                                               : sb + (uint32_t)(r * PP_PITCH + kk) * 4u;
+                const int r = c / 16, kk = (c % 16) * 4;
+                const uint32_t dst = sb + (uint32_t)(r * PP_PITCH + kk) * 4u;
                 const bool in = r0 + r < p.R && k0 + kk < p.K;
                 cp_async16_zfill(dst, in ? (const void*)(tb.src + tb.row[r] + tb.k[kk]) : (const void*)tb.src, in);
             }
@@ -433,36 +430,18 @@ __global__ void __launch_bounds__(PP_THREADS) k_pack_pipe(PackParams p, PackDivs
         int64_t r0, k0, l;
         tile_of(i, r0, k0, l);
         const float* v = slots + (i % PP_STAGES) * PP_SLOT;
-        if (ROWS_FAST) {
-            const int r4 = t % 16, g = t / 16;
-            const int64_t col = k0 + g * 8;
-            if (col >= p.Kseg || r0 + r4 * 4 >= p.R) return;
-            float4 q[8];
 #pragma unroll
-            for (int j = 0; j < 8; j++) q[j] = *(const float4*)(v + (size_t)(r4 * PP_P4 + g * 8 + j) * 4);
-#pragma unroll
-            for (int h = 0; h < 4; h++) {
-                const int64_t rg = r0 + r4 * 4 + h;
-                if (rg >= p.R) break;
-                float x[8];
-#pragma unroll
-                for (int j = 0; j < 8; j++) x[j] = h == 0 ? q[j].x : h == 1 ? q[j].y : h == 2 ? q[j].z : q[j].w;
-                pp_put8<SPLIT, FMT>(p, l, rg, col, x);
-            }
-        } else {
-#pragma unroll
-            for (int it = 0; it < 4; it++) {
-                const int e = t + PP_THREADS * it;
-                const int g = e % 8, r = e / 8;
-                const int64_t rg = r0 + r, col = k0 + g * 8;
-                if (rg >= p.R || col >= p.Kseg) continue;
-                const int h0 = (g >> 2) & 1;
-                const float4 a = *(const float4*)(v + r * PP_PITCH + g * 8 + 4 * h0);
-                const float4 b = *(const float4*)(v + r * PP_PITCH + g * 8 + 4 * (1 - h0));
-                const float4 lo4 = h0 ? b : a, hi4 = h0 ? a : b;
-                const float x[8] = {lo4.x, lo4.y, lo4.z, lo4.w, hi4.x, hi4.y, hi4.z, hi4.w};
-                pp_put8<SPLIT, FMT>(p, l, rg, col, x);
-            }
+        for (int it = 0; it < 4; it++) {
+            const int e = t + PP_THREADS * it;
+            const int g = e % 8, r = e / 8;
+            const int64_t rg = r0 + r, col = k0 + g * 8;
+            if (rg >= p.R || col >= p.Kseg) continue;
+            const int h0 = (g >> 2) & 1;
+            const float4 a = *(const float4*)(v + r * PP_PITCH + g * 8 + 4 * h0);
+            const float4 b = *(const float4*)(v + r * PP_PITCH + g * 8 + 4 * (1 - h0));
+            const float4 lo4 = h0 ? b : a, hi4 = h0 ? a : b;
+            const float x[8] = {lo4.x, lo4.y, lo4.z, lo4.w, hi4.x, hi4.y, hi4.z, hi4.w};
+            pp_put8<SPLIT, FMT>(p, l, rg, col, x);
         }
     };
     for (int i = 0; i < PP_STAGES - 1; i++) {
@@ -484,10 +463,10 @@ __global__ void __launch_bounds__(PP_THREADS) k_pack_pipe(PackParams p, PackDivs
 static int num_sms();
 
 // false: the kernel could not be given its shared memory (the caller runs k_pack_real)
-template <int SPLIT, int FMT, bool RF>
+template <int SPLIT, int FMT>
 static bool launch_pack_pipe(const PackParams& pp, int64_t lz, cudaStream_t s)
 {
-    auto kern = k_pack_pipe<SPLIT, FMT, RF>;
+    auto kern = k_pack_pipe<SPLIT, FMT>;
     static int attr_done[64];
     int dev = 0;
     cudaGetDevice(&dev);
@@ -526,13 +505,12 @@ static bool pack_pipe_fits(const PackParams& pp, int64_t lz)
     return !pp.srcs || pp.Lsz >= 1;
 }
 
-template <bool RF>
 static bool launch_pack_pipe3(const PackParams& pp, int split, int fmt, int64_t lz, cudaStream_t s)
 {
-    if (split == 3) return launch_pack_pipe<3, 0, RF>(pp, lz, s);
-    if (split == 2) return launch_pack_pipe<2, 0, RF>(pp, lz, s);
-    if (fmt == 1) return launch_pack_pipe<1, 1, RF>(pp, lz, s);
-    return launch_pack_pipe<1, 0, RF>(pp, lz, s);
+    if (split == 3) return launch_pack_pipe<3, 0>(pp, lz, s);
+    if (split == 2) return launch_pack_pipe<2, 0>(pp, lz, s);
+    if (fmt == 1) return launch_pack_pipe<1, 1>(pp, lz, s);
+    return launch_pack_pipe<1, 0>(pp, lz, s);
 }
 
 template <typename T, bool RF, int VEC>
@@ -569,9 +547,7 @@ static void launch_pack_real(const PackParams& pp, int split, int fmt, int64_t l
         const ModeList* others[3] = {rf ? &pp.ks : &pp.rows, &pp.ls, &pp.us};
         v4 = vec4_ok(rf ? pp.rows : pp.ks, others, 2, pp.src);
     }
-    if (v4 && pack_pipe_fits(pp, lz) &&
-        (rf ? launch_pack_pipe3<true>(pp, split, fmt, lz, s) : launch_pack_pipe3<false>(pp, split, fmt, lz, s)))
-        return;
+    if (v4 && !rf && pack_pipe_fits(pp, lz) && launch_pack_pipe3(pp, split, fmt, lz, s)) return;
     if (rf) {
         if (v4) launch_pack_real3<T, true, 4>(pp, split, fmt, grid, s);
         else launch_pack_real3<T, true, 1>(pp, split, fmt, grid, s);
