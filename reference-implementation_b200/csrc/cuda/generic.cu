@@ -554,17 +554,117 @@ cudaError_t launch_generic_group(const tb_plan* const* P, const tb_ptrs* d, int 
     return cudaGetLastError();
 }
 
-cudaError_t launch_generic(const tb_plan* P, const tb_ptrs* d, cudaStream_t s)
+// Copy of one operand (its free, contracted and unary modes) into a dense
+// buffer whose first mode is the first output mode and whose other modes
+// follow in free, contracted, unary order, so that the element kernel reads
+// it along its walk of the outputs instead of one line per lane. Element
+// values are copied as stored (2-byte elements, or 4-byte words).
+struct StageParams {
+    const unsigned char* src;
+    unsigned char* dst;
+    int32_t n, words;  // modes; 4-byte words per element (0: one 2-byte element)
+    int64_t size;
+    int64_t s[3 * TB_MAXMODES];  // source strides, in elements
+    FastDiv f[3 * TB_MAXMODES];
+};
+
+__global__ void __launch_bounds__(256) k_stage(StageParams p)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < p.size; i += (int64_t)gridDim.x * blockDim.x) {
+        uint32_t r = (uint32_t)i;
+        int64_t o = 0;
+        for (int j = 0; j < p.n; j++) {
+            const uint32_t q = fdiv(r, p.f[j]);
+            o += (int64_t)(r - q * p.f[j].d) * p.s[j];
+            r = q;
+        }
+        if (p.words == 0) {
+            ((uint16_t*)p.dst)[i] = __ldg((const uint16_t*)p.src + o);
+        } else {
+            for (int w = 0; w < p.words; w++)
+                ((uint32_t*)p.dst)[i * p.words + w] = __ldg((const uint32_t*)p.src + o * p.words + w);
+        }
+    }
+}
+
+static int stored_bytes(int t)
+{
+    switch (t) {
+    case T_F32: return 4;
+    case T_F64: return 8;
+    case T_C32: return 8;
+    case T_C64: return 16;
+    default: return 2;
+    }
+}
+
+// The operand `side` (0 A, 1 B) of the element path copied into scratch in
+// the order of the output walk; g's strides and d's pointer then refer to
+// the copy. *ws: the scratch, to be freed after the element kernel.
+static cudaError_t stage_operand(const tb_plan* P, int side, GenParams& g, tb_ptrs& d, void** ws, cudaStream_t s)
+{
+    StageParams sp;
+    memset(&sp, 0, sizeof(sp));
+    int64_t* F_s = side ? g.F_sB : g.F_sA;
+    int64_t* K_s = side ? g.K_sB : g.K_sA;
+    int64_t* U_s = side ? g.UB_s : g.UA_s;
+    const tb_modes& U = side ? P->UB : P->UA;
+    int n = 0;
+    int64_t acc = 1;
+    auto add = [&](int64_t ext, int64_t& stride) {
+        sp.s[n] = stride;
+        sp.f[n] = make_fastdiv((uint32_t)ext);
+        n++;
+        stride = acc;
+        acc *= ext;
+    };
+    for (int j = 0; j < P->F.n; j++)
+        if (F_s[j] != 0) add(P->F.ext[j], F_s[j]);
+    for (int j = 0; j < P->K.n; j++) add(P->K.ext[j], K_s[j]);
+    for (int j = 0; j < U.n; j++) add(U.ext[j], U_s[j]);
+    if (acc >= (1ll << 31)) return cudaErrorInvalidValue;
+    const int tY = side ? P->tB : P->tA;
+    const int eb = stored_bytes(tY);
+    sp.n = n;
+    sp.words = eb / 4;
+    sp.size = acc;
+    sp.src = (const unsigned char*)(side ? d.B : d.A);
+    cudaError_t e = pool_alloc(ws, (size_t)acc * (size_t)eb, s);
+    if (e != cudaSuccess) return e;
+    sp.dst = (unsigned char*)*ws;
+    int64_t blocks = (acc + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_stage<<<(unsigned)blocks, 256, 0, s>>>(sp);
+    count_launch();
+    if (side) d.B = *ws;
+    else d.A = *ws;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_generic(const tb_plan* P, const tb_ptrs* d, cudaStream_t s, int* kernels)
 {
     GenParams g;
     fill_params(P, g);
-    switch (P->compute) {
-    case TB_R32: return launch_typed<float, false>(g, P->path, d, s);
-    case TB_R64: return launch_typed<double, false>(g, P->path, d, s);
-    case TB_C32: return launch_typed<float, true>(g, P->path, d, s);
-    case TB_C64: return launch_typed<double, true>(g, P->path, d, s);
+    *kernels = 1;
+    tb_ptrs dd = *d;
+    void* ws = nullptr;
+    if (P->path == TB_PATH_GENERIC && P->elem_stage && !g.warp) {
+        cudaError_t e = stage_operand(P, P->elem_stage - 1, g, dd, &ws, s);
+        if (e != cudaSuccess) {
+            if (ws) cudaFreeAsync(ws, s);
+            return e;
+        }
+        *kernels = 2;
     }
-    return cudaErrorInvalidValue;
+    cudaError_t e = cudaErrorInvalidValue;
+    switch (P->compute) {
+    case TB_R32: e = launch_typed<float, false>(g, P->path, &dd, s); break;
+    case TB_R64: e = launch_typed<double, false>(g, P->path, &dd, s); break;
+    case TB_C32: e = launch_typed<float, true>(g, P->path, &dd, s); break;
+    case TB_C64: e = launch_typed<double, true>(g, P->path, &dd, s); break;
+    }
+    if (ws) cudaFreeAsync(ws, s);
+    return e;
 }
 
 }  // namespace tb

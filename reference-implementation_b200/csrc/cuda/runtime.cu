@@ -122,7 +122,7 @@ cudaError_t stage_copy(void* dev_dst, const void* src, size_t bytes, cudaStream_
     return e;
 }
 
-cudaError_t launch_generic(const tb_plan* P, const tb_ptrs* d, cudaStream_t s);
+cudaError_t launch_generic(const tb_plan* P, const tb_ptrs* d, cudaStream_t s, int* kernels);
 cudaError_t launch_simt(const tb_plan* P, const tb_ptrs* d, cudaStream_t s);
 cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t s, int* kernels, void** main_timer);
 size_t group_descriptor_bytes(int n);
@@ -280,9 +280,8 @@ int tbk_run_plan(const tb_plan* plan, const tb_ptrs* ptrs, void* stream, int* ke
         break;
     default:
         if (main_timer) tbk_timer_begin(stream, main_timer);
-        e = tb::launch_generic(plan, ptrs, s);
+        e = tb::launch_generic(plan, ptrs, s, kernels);
         if (main_timer) tbk_timer_end(stream, *main_timer);
-        *kernels = 1;
         break;
     }
     return (int)e;

@@ -29,7 +29,6 @@
 #include "tc_device.cuh"
 
 namespace tb {
-cudaError_t launch_generic(const tb_plan* P, const tb_ptrs* d, cudaStream_t s);
 int* device_error_word();
 cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t s);
 cudaError_t stage_copy(void* dev_dst, const void* src, size_t bytes, cudaStream_t s);

@@ -120,6 +120,8 @@ static void simplify(mlist* m, int key)
     m->n = w;
 }
 
+static void reorder_by(tb_modes* F, const int64_t* s);
+
 /* Element path: one thread per output, consecutive threads on consecutive
  * outputs in F order (D's stride order). When the larger operand holds more
  * than twice as many elements as D and is contiguous along an output mode
@@ -141,6 +143,21 @@ static void order_outputs(tb_plan* P)
     for (int i = 0; i < F->n; i++)
         if (s[i] == 1 || s[i] == -1) unit = 1;
     if (!unit) return;
+    reorder_by(F, s);
+    /* The other operand, when consecutive outputs would read it far apart
+     * (one line per lane) and it is at most half the size of the walked one
+     * and at least 64 Ki elements: copied once into the walk's order before
+     * the element kernel runs (its values, and so every output, unchanged). */
+    const int64_t* o = useA ? F->sB : F->sA;
+    const double nO = useA ? nB : nA;
+    if (F->n >= 1 && o[0] != 0 && o[0] != 1 && o[0] != -1 && nO * 2.0 <= (useA ? nA : nB) && nO >= 65536.0 &&
+        nO < 2147483648.0)
+        P->elem_stage = useA ? 2 : 1;
+}
+
+/* stable sort of F's modes by |s| (modes with s = 0 last) */
+static void reorder_by(tb_modes* F, const int64_t* s)
+{
     int64_t key[TB_MAXMODES];
     for (int i = 0; i < F->n; i++) key[i] = s[i] ? iabs64(s[i]) : INT64_MAX;
     for (int i = 1; i < F->n; i++) {
@@ -517,7 +534,11 @@ size_t tb_describe(const tb_plan* p, size_t maxlen, char* out)
     if (p->path == TB_PATH_TC && p->tc_mode == TB_TC_SPLIT_BF16)
         at = put(out, maxlen, at, " operands=%s", tbk_tc_split_in_place(p) ? "in_place" : "packed");
     if (p->path == TB_PATH_SLICED) at = put(out, maxlen, at, " slices=%d", p->slices);
-    if (p->path == TB_PATH_GENERIC) at = put(out, maxlen, at, " kernel=%s", tbk_generic_kernel(p) ? "warpdot" : "element");
+    if (p->path == TB_PATH_GENERIC) {
+        const int warp = tbk_generic_kernel(p);
+        at = put(out, maxlen, at, " kernel=%s", warp ? "warpdot" : "element");
+        if (!warp && p->elem_stage) at = put(out, maxlen, at, " staged=%s", p->elem_stage == 1 ? "A" : "B");
+    }
     if (p->path == TB_PATH_SIMT) {
         static const char* kern[] = {"tiled", "narrow", "narrow_stream", "narrow_coop", "narrow_cstream", "narrow_vec",
                                      "narrow_kt"};

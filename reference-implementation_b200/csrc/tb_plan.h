@@ -68,7 +68,8 @@ typedef struct tb_plan {
     int32_t slices;               /* TB_PATH_SLICED: digit slices per operand */
     int32_t split_route;          /* TB_TC_SPLIT_BF16 operands: 1 automatic, 2 packed hi/lo panels,
                                    * 3 read in place by converter warps */
-    int32_t reserved_;
+    int32_t elem_stage;           /* element path: 1 (2) when A (B) is first copied into the
+                                   * order in which the outputs are walked */
     double alpha_re, alpha_im;    /* scalars, already rounded per precision */
     double beta_re, beta_im;
     tb_modes F;                   /* free modes, sorted by |stride in D| */

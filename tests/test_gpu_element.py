@@ -146,3 +146,24 @@ def test_small_grid_runs_a_warp_per_output(tapp, oracle, gpu):
     assert e64 == 0
     bound = error_bound(case, scale, D64)
     assert not (np.abs(d_values(runs[0].D) - D64) > bound).any()
+
+
+def test_element_path_stages_the_small_operand(tapp, oracle, gpu):
+    """Batched Hadamard product whose small operand B would be read 600
+    elements apart by consecutive outputs: B is first copied into the order
+    of the output walk (plan: staged=B). Within the oracle bound, and the same
+    bits as the grouped element launch of a batched product, which reads B in
+    place."""
+    from test_gpu_tc import _batched_against_single
+    case = _hadamard(np.random.default_rng(93), "dcba", (72, 8, 20, 30, 16))
+    d = _describe(tapp, case)
+    assert "kernel=element staged=B" in d, d
+    run = case.copy()
+    assert run_on_device(tapp, run) == 0
+    e64, D64, scale = oracle.execute_f64(case.copy())
+    assert e64 == 0
+    bound = error_bound(case, scale, D64)
+    assert not (np.abs(d_values(run.D) - D64) > bound).any()
+    ex = tapp.create_executor()
+    _batched_against_single(tapp, [case, case.copy()], ex)
+    tapp.lib.TAPP_destroy_executor(ex)
