@@ -130,7 +130,19 @@ __global__ void __launch_bounds__(256) k_exponents(SliceParams p, int64_t kchunk
         int c = 0;
         if (r0 + r < p.R) {
             const int64_t ro = p.roff[r0 + r] + lo;
-            for (int64_t k = kb + kq; k < ke; k += 8) {
+            int64_t k = kb + kq;
+            // four loads in flight before their exponents are taken
+            for (; k + 24 < ke; k += 32) {
+                double re[4], im[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) load_elem<double>(p.src, ro + p.koff[k + 8 * u], p.type, re[u], im[u]);
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    c = max(c, exp_code(re[u]));
+                    if (p.cplx) c = max(c, exp_code(im[u]));
+                }
+            }
+            for (; k < ke; k += 8) {
                 double re, im;
                 load_elem<double>(p.src, ro + p.koff[k], p.type, re, im);
                 c = max(c, exp_code(re));
@@ -151,7 +163,18 @@ __global__ void __launch_bounds__(256) k_exponents(SliceParams p, int64_t kchunk
             int c = 0;
             if (r0 + r < p.R) {
                 const int64_t ro = p.roff[r0 + r] + lo;
-                for (int64_t k = kb + lane; k < ke; k += 32) {
+                int64_t k = kb + lane;
+                for (; k + 96 < ke; k += 128) {
+                    double re[4], im[4];
+#pragma unroll
+                    for (int u = 0; u < 4; u++) load_elem<double>(p.src, ro + p.koff[k + 32 * u], p.type, re[u], im[u]);
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        c = max(c, exp_code(re[u]));
+                        if (p.cplx) c = max(c, exp_code(im[u]));
+                    }
+                }
+                for (; k < ke; k += 32) {
                     double re, im;
                     load_elem<double>(p.src, ro + p.koff[k], p.type, re, im);
                     c = max(c, exp_code(re));
@@ -197,13 +220,26 @@ __global__ void __launch_bounds__(256) k_slice(SliceParams p)
     const int64_t l = blockIdx.z;
     const int64_t ks0 = kt * TKS;
     const int64_t lo = mode_offset(p.ls, l);
-    for (int e = t; e < TR * TKS; e += 256) {
+    // all of this thread's loads in flight before the shared-memory stores
+    constexpr int PER = TR * TKS / 256;
+    double lre[PER], lim[PER];
+#pragma unroll
+    for (int u = 0; u < PER; u++) {
+        const int e = t + 256 * u;
         const int r = RF ? e % TR : e / TKS;
         const int kk = RF ? e / TR : e % TKS;
-        double re = 0.0, im = 0.0;
-        if (r0 + r < p.R && ks0 + kk < p.K) load_elem<double>(p.src, p.roff[r0 + r] + lo + p.koff[ks0 + kk], p.type, re, im);
-        tre[r][kk] = re;
-        if (CPLX) tim[r][kk] = p.conj ? -im : im;
+        lre[u] = 0.0;
+        lim[u] = 0.0;
+        if (r0 + r < p.R && ks0 + kk < p.K)
+            load_elem<double>(p.src, p.roff[r0 + r] + lo + p.koff[ks0 + kk], p.type, lre[u], lim[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < PER; u++) {
+        const int e = t + 256 * u;
+        const int r = RF ? e % TR : e / TKS;
+        const int kk = RF ? e / TR : e % TKS;
+        tre[r][kk] = lre[u];
+        if (CPLX) tim[r][kk] = p.conj ? -lim[u] : lim[u];
     }
     __syncthreads();
     const int r = t >> 3, kc = (t & 7) * 8;
