@@ -273,8 +273,9 @@ def measured_peaks():
 
 
 def profiled_traffic():
-    """dram bytes per GEMM launch from the committed ncu summary, if any."""
-    path = os.path.join(REPO, "profiles", "k_gemm_dense_4index_64.md")  # written from an ncu capture
+    """dram bytes per launch of the headline's GEMM (split bfloat16, panels) from
+    the committed ncu summary, if any."""
+    path = os.path.join(REPO, "profiles", "k_gemm_split_panels_64.md")  # written from an ncu capture
     try:
         for line in open(path):
             if line.startswith("traffic_bytes_per_launch:"):
