@@ -1367,6 +1367,19 @@ __global__ void __launch_bounds__(NB * 4 * NarrowVecShape<T, NB>::H) k_narrow_ve
                                                        (const T*)p.C + oC + nC[cg * 8 + n]);
         }
         issue(g + S - 1);
+        if (RND) {
+            // the chunk rounded once in place, each value by one thread
+            float4* ch = (float4*)(ring + (size_t)(g % S) * KC * TR);
+            for (int e = t; e < KC * TR * (int)sizeof(T) / 16; e += NT) {
+                float4 v = ch[e];
+                v.x = round_in<float>(v.x, p.round_in);
+                v.y = round_in<float>(v.y, p.round_in);
+                v.z = round_in<float>(v.z, p.round_in);
+                v.w = round_in<float>(v.w, p.round_in);
+                ch[e] = v;
+            }
+            __syncthreads();
+        }
         const bool last = c == nchunks - 1;
         if (oA >= 0) {
             const T* a = ring + (size_t)(g % S) * KC * TR + crg * VR;
@@ -1376,10 +1389,6 @@ __global__ void __launch_bounds__(NB * 4 * NarrowVecShape<T, NB>::H) k_narrow_ve
             for (int kk = 0; kk < kn; kk++) {
                 T x[VR];
                 NV::get(*(const V*)(a + kk * TR), x);
-                if (RND) {
-#pragma unroll
-                    for (int r = 0; r < VR; r++) x[r] = round_in<T>(x[r], p.round_in);
-                }
                 const T* b = Bs + (k0 + kk) * NB + cg * 8;
                 T bv[8];
                 if (sizeof(T) == 4) {
@@ -1582,6 +1591,19 @@ __global__ void __launch_bounds__(NB * 4) k_narrow_kt(NarrowParams np)
                         cp_async_elem4(ts_base + (uint32_t)((r * NP1 + n) * 4), (const float*)p.C + rowC[r] + nC[n]);
         }
         issue(g + S - 1);
+        if (RND) {
+            // the chunk rounded once in place, each value by one thread
+            float4* ch = (float4*)(ring + (size_t)(g % S) * TR * KC);
+            for (int e = t; e < TR * KC / 4; e += NT) {
+                float4 v = ch[e];
+                v.x = round_in<float>(v.x, p.round_in);
+                v.y = round_in<float>(v.y, p.round_in);
+                v.z = round_in<float>(v.z, p.round_in);
+                v.w = round_in<float>(v.w, p.round_in);
+                ch[e] = v;
+            }
+            __syncthreads();
+        }
         const bool last = c == nchunks - 1;
         {
             const float* slot = ring + (size_t)(g % S) * TR * KC;
@@ -1602,7 +1624,7 @@ __global__ void __launch_bounds__(NB * 4) k_narrow_kt(NarrowParams np)
                     const float bv[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
 #pragma unroll
                     for (int j = 0; j < 4; j++) {
-                        const float x = RND ? round_in<float>(a[j][kk], p.round_in) : a[j][kk];
+                        const float x = a[j][kk];
 #pragma unroll
                         for (int n = 0; n < 8; n += 2) fma2(acc[j][n], acc[j][n + 1], x, x, bv[n], bv[n + 1]);
                     }
