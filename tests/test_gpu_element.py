@@ -165,5 +165,6 @@ def test_element_path_stages_the_small_operand(tapp, oracle, gpu):
     bound = error_bound(case, scale, D64)
     assert not (np.abs(d_values(run.D) - D64) > bound).any()
     ex = tapp.create_executor()
+    tapp.set_int(ex, tapp_b200.ATTR_WANT_STATUS, 1)
     _batched_against_single(tapp, [case, case.copy()], ex)
     tapp.lib.TAPP_destroy_executor(ex)
