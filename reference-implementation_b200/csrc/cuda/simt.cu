@@ -70,7 +70,7 @@ struct Params {
 // D = op_D(alpha * acc + beta * op_C(C)) for one element whose C value
 // (cr, ci) is already loaded (rounded, not yet conjugated)
 template <typename T, bool CPLX>
-__device__ __forceinline__ void epilogue_store_c(const Params& p, T xr, T xi, T cr, T ci, int64_t od)
+__device__ __forceinline__ void epilogue_value(const Params& p, T xr, T xi, T cr, T ci, T& out_r, T& out_i)
 {
     const T ar = (T)p.alpha, ai = (T)p.alpha_im, br = (T)p.beta, bi = (T)p.beta_im;
     T vr = ar * xr - (CPLX ? ai * xi : (T)0);
@@ -90,6 +90,15 @@ __device__ __forceinline__ void epilogue_store_c(const Params& p, T xr, T xi, T 
         }
         vi = -vi;
     }
+    out_r = vr;
+    out_i = vi;
+}
+
+template <typename T, bool CPLX>
+__device__ __forceinline__ void epilogue_store_c(const Params& p, T xr, T xi, T cr, T ci, int64_t od)
+{
+    T vr, vi;
+    epilogue_value<T, CPLX>(p, xr, xi, cr, ci, vr, vi);
     store_elem<T>(p.D, od, p.tD, vr, vi);
 }
 
@@ -1445,6 +1454,189 @@ __global__ void __launch_bounds__(NB * 4 * NarrowVecShape<T, NB>::H) k_narrow_ve
     cp_async_wait<0>();
 }
 
+// Complex-float form of k_narrow_vec: A, C and D stored as complex float and
+// contiguous along the first row mode (2 rows per 16-byte vector, other
+// strides even, bases 16-byte aligned). Tiles of 128 rows, chunks of 16
+// contracted values (16 KiB) copied by cp.async into a ring [k][row]; a
+// thread owns 2 rows x 8 columns: per contracted value one vector of A and
+// four broadcast vectors of B (op_B applied when the panel is built) feed
+// 16 complex multiply-adds as paired (re, im) fused multiply-adds in the
+// order of k_narrow_cstream (re: a_r b_r then -a_i b_i; im: a_r b_i then
+// a_i b_r), so the two kernels give the same bits. C is copied per thread at
+// the tile's start; the epilogue is k_narrow_cstream's (epilogue_value) and
+// D is stored as 2-row vectors.
+template <int NB>
+__global__ void __launch_bounds__(NB * 8) k_narrow_cvec(NarrowParams np)
+{
+    constexpr int H = 2, VR = 2, RG = 32 * H, NT = NB / 8 * RG, TR = RG * VR, S = 4;
+    constexpr int KC = NVEC_CHUNK_BYTES / (TR * 8);
+    const Params& p = np.p;
+    extern __shared__ __align__(16) unsigned char nsm[];
+    float2* ring = (float2*)nsm;                            // [S][KC][TR]
+    float2* Cs = ring + (size_t)S * KC * TR;                // [NB][TR] when C is read
+    float2* Bs = Cs + (p.beta_zero ? 0 : (size_t)NB * TR);  // [K][NB]
+    int64_t* kA = (int64_t*)(Bs + (size_t)NB * p.K);        // [K]
+    int64_t* nC = kA + p.K;                                 // [NB]
+    int64_t* nD = nC + NB;                                  // [NB]
+    const int t = threadIdx.x;
+    const int64_t l = blockIdx.y;
+    int64_t lA, lB, lC, lD, dummy;
+    decode(p.al, l, lA, dummy);
+    decode(p.bl, l, lB, dummy);
+    decode(p.cl, l, lC, lD);
+    for (int64_t k = t; k < p.K; k += NT) {
+        int64_t o;
+        decode(p.ak, k, o, dummy);
+        kA[k] = o + lA;
+    }
+    if (t < NB) {
+        int64_t oc = 0, od = 0;
+        if (t < p.N) decode(p.cn, t, oc, od);
+        nC[t] = oc + lC;
+        nD[t] = od + lD;
+    }
+    for (int64_t e = t; e < p.K * NB; e += NT) {
+        const int64_t k = e / NB;
+        const int n = (int)(e % NB);
+        float x = 0, xi = 0;
+        if (n < p.N) {
+            int64_t ob, ok;
+            decode(p.bn, n, ob, dummy);
+            decode(p.bk, k, ok, dummy);
+            load_rounded<float>(p.B, lB + ob + ok, p.tB, p.round_in, x, xi);
+            if (p.conjB) xi = -xi;
+        }
+        Bs[k * NB + n] = make_float2(x, xi);
+    }
+    __syncthreads();
+
+    const int64_t tiles = (p.M + TR - 1) / TR;
+    if ((int64_t)blockIdx.x >= tiles) return;
+    const int64_t my_tiles = (tiles - 1 - blockIdx.x) / gridDim.x + 1;
+    const int nchunks = (int)((p.K + KC - 1) / KC);
+    const int64_t total = my_tiles * nchunks;
+    const float* A = (const float*)p.A;
+    auto group_offsets = [&](int64_t i, int rg, int64_t& oA, int64_t& oC, int64_t& oD) {
+        const int64_t m = ((int64_t)blockIdx.x + i * gridDim.x) * TR + (int64_t)rg * VR;
+        oA = oC = oD = -1;
+        if (m >= p.M) return;
+        oA = oC = oD = 0;
+        uint32_t r = (uint32_t)m;
+        for (int j = 0; j < p.am.n; j++) {
+            const uint32_t q = fdiv(r, np.fm[j]);
+            const int64_t c = (int64_t)(r - q * np.fm[j].d);
+            r = q;
+            oA += c * p.am.s0[j];
+            oC += c * p.cm.s0[j];
+            oD += c * p.cm.s1[j];
+        }
+    };
+    const int prg = t % RG, pk0 = t / RG;
+    constexpr int PKS = NT / RG;
+    const uint32_t ring_base = (uint32_t)__cvta_generic_to_shared(ring) + (uint32_t)(prg * VR * 8);
+    int64_t p_tile = -1, p_oA = -1;
+    int p_chunk = 0;
+    auto issue = [&](int64_t g) {
+        if (g < total) {
+            if (p_chunk == 0) {
+                p_tile++;
+                int64_t c_, d_;
+                group_offsets(p_tile, prg, p_oA, c_, d_);
+            }
+            if (p_oA >= 0) {
+                const int k0 = p_chunk * KC;
+                const uint32_t dst = ring_base + (uint32_t)((g % S) * KC * TR * 8);
+                for (int kk = pk0; kk < KC; kk += PKS)
+                    if (k0 + kk < p.K) cp_async_vec<16>(dst + kk * TR * 8, A + 2 * (p_oA + kA[k0 + kk]));
+            }
+            if (++p_chunk == nchunks) p_chunk = 0;
+        }
+        cp_async_commit();  // empty groups keep the count uniform
+    };
+#pragma unroll
+    for (int g = 0; g < S - 1; g++) issue(g);
+
+    const int lane = t & 31, w = t >> 5;
+    const int cg = w / H, crg = (w % H) * 32 + lane;
+    float ar_[VR][8], ai_[VR][8];
+    const uint32_t cs_base = (uint32_t)__cvta_generic_to_shared(Cs) + (uint32_t)((cg * 8 * TR + crg * VR) * 8);
+    int64_t oA = -1, oC = -1, oD = -1;
+    int c = 0;
+    int64_t ti = 0;
+    for (int64_t g = 0; g < total; g++) {
+        if (c == 0) {
+            group_offsets(ti, crg, oA, oC, oD);
+#pragma unroll
+            for (int r = 0; r < VR; r++)
+#pragma unroll
+                for (int n = 0; n < 8; n++) ar_[r][n] = ai_[r][n] = 0.f;
+        }
+        cp_async_wait<S - 2>();  // this thread's copies of chunk g have landed
+        __syncthreads();         // everyone's have; the slot of chunk g - 1 is free
+        if (c == 0 && oA >= 0 && !p.beta_zero) {
+#pragma unroll
+            for (int n = 0; n < 8; n++)
+                if (cg * 8 + n < p.N)
+                    cp_async_vec<16>(cs_base + (uint32_t)(n * TR * 8), (const float*)p.C + 2 * (oC + nC[cg * 8 + n]));
+        }
+        issue(g + S - 1);
+        const bool last = c == nchunks - 1;
+        if (oA >= 0) {
+            const float2* a = ring + (size_t)(g % S) * KC * TR + crg * VR;
+            const int k0 = c * KC;
+            const int kn = p.K - k0 < KC ? (int)(p.K - k0) : KC;
+#pragma unroll 2
+            for (int kk = 0; kk < kn; kk++) {
+                const float4 av = *(const float4*)(a + kk * TR);
+                const float xr[2] = {av.x, av.z};
+                const float xi[2] = {p.conjA ? -av.y : av.y, p.conjA ? -av.w : av.w};
+                const float4* b = (const float4*)(Bs + (size_t)(k0 + kk) * NB + cg * 8);
+                float br[8], bi[8];
+#pragma unroll
+                for (int h = 0; h < 4; h++) {
+                    const float4 q = b[h];
+                    br[2 * h] = q.x;
+                    bi[2 * h] = q.y;
+                    br[2 * h + 1] = q.z;
+                    bi[2 * h + 1] = q.w;
+                }
+#pragma unroll
+                for (int r = 0; r < VR; r++)
+#pragma unroll
+                    for (int n = 0; n < 8; n++) {
+                        fma2(ar_[r][n], ai_[r][n], xr[r], xr[r], br[n], bi[n]);
+                        fma2(ar_[r][n], ai_[r][n], -xi[r], xi[r], bi[n], br[n]);
+                    }
+            }
+        }
+        if (last) {
+            if (oA >= 0) {
+                if (!p.beta_zero && nchunks < S) {
+                    if (nchunks == 1) cp_async_wait<0>();
+                    else if (nchunks == 2) cp_async_wait<1>();
+                    else cp_async_wait<2>();
+                }
+#pragma unroll
+                for (int n = 0; n < 8; n++) {
+                    if (cg * 8 + n < p.N) {
+                        float4 cv = make_float4(0.f, 0.f, 0.f, 0.f);
+                        if (!p.beta_zero) cv = *(const float4*)(Cs + (size_t)(cg * 8 + n) * TR + crg * VR);
+                        float v0r, v0i, v1r, v1i;
+                        epilogue_value<float, true>(p, ar_[0][n], ai_[0][n], cv.x, cv.y, v0r, v0i);
+                        epilogue_value<float, true>(p, ar_[1][n], ai_[1][n], cv.z, cv.w, v1r, v1i);
+                        *(float4*)((float*)p.D + 2 * (oD + nD[cg * 8 + n])) = make_float4(v0r, v0i, v1r, v1i);
+                    }
+                }
+            }
+            c = 0;
+            ti++;
+        } else {
+            c++;
+        }
+    }
+    cp_async_wait<0>();
+}
+
 // Split of the contraction: enough CTAs to fill the GPU when the tiles do
 // not, each split at least 4 slices long, the workspace at most 256 MiB.
 struct Split {
@@ -1821,11 +2013,54 @@ static cudaError_t launch_narrow_t(simt::NarrowParams& np, cudaStream_t s)
     return cudaGetLastError();
 }
 
+// complex float in 2-row vectors (k_narrow_cvec): complex-float A, C and D,
+// rows contiguous and 16-byte aligned, no operand rounding
+static size_t cvec_smem(const simt::Params& p, int nb)
+{
+    return (size_t)4 * simt::NVEC_CHUNK_BYTES + (p.beta_zero ? 0 : (size_t)8 * nb * 128) + (size_t)8 * nb * (size_t)p.K +
+           8 * ((size_t)p.K + 2 * (size_t)nb);
+}
+
+static bool cvec_ok(const simt::Params& p, int nb)
+{
+    return p.tA == T_C32 && p.tD == T_C32 && (p.beta_zero || p.tC == T_C32) && p.round_in == TB_ROUND_NONE &&
+           nvec_layout(p, 2, 8) && cvec_smem(p, nb) <= (size_t)simt::NVEC_MAX_SMEM;
+}
+
+template <int NB>
+static cudaError_t launch_narrow_cvec(simt::NarrowParams& np, cudaStream_t s)
+{
+    using namespace simt;
+    const Params& p = np.p;
+    const size_t smem = cvec_smem(p, NB);
+    auto kern = k_narrow_cvec<NB>;
+    static int attr_done[64];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64 || !attr_done[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, NVEC_MAX_SMEM);
+        if (e != cudaSuccess) return e;
+        if (dev >= 0 && dev < 64) attr_done[dev] = 1;
+    }
+    const int threads = NB * 8;
+    const int64_t tiles = (p.M + 127) / 128;
+    int per_sm = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    int64_t gx = ((int64_t)148 * per_sm + p.L - 1) / p.L;
+    if (gx > tiles) gx = tiles;
+    if (gx < 1) gx = 1;
+    kern<<<dim3((unsigned)gx, (unsigned)p.L), threads, smem, s>>>(np);
+    count_launch();
+    return cudaGetLastError();
+}
+
 template <int NB>
 static cudaError_t launch_narrow_c(simt::NarrowParams& np, cudaStream_t s)
 {
     using namespace simt;
     const Params& p = np.p;
+    if (cvec_ok(p, NB)) return launch_narrow_cvec<NB>(np, s);
     const size_t smem = sizeof(float2) * (size_t)(3 * 8 * 256) + sizeof(float2) * NB * (size_t)p.K +
                         8 * ((size_t)p.K + 2 * NB);
     auto kern = k_narrow_cstream<NB>;
@@ -1901,7 +2136,8 @@ cudaError_t launch_simt(const tb_plan* P, const tb_ptrs* d, cudaStream_t s)
 // their element size and, for 5, to the row vector (the launcher falls back
 // to another narrow or the tiled kernel for others): 0 tiled, 1 narrow with
 // register prefetch, 2 narrow streaming, 3 narrow cooperative, 4 complex
-// narrow streaming, 5 narrow with row vectors. No device call.
+// narrow streaming, 5 narrow with row vectors, 6 complex narrow with row
+// vectors. No device call.
 extern "C" int tbk_simt_kernel(const tb_plan* P)
 {
     using namespace tb;
@@ -1910,6 +2146,6 @@ extern "C" int tbk_simt_kernel(const tb_plan* P)
     simt_params(P, &d, p);
     const int nb = narrow_width(P, p);
     if (!nb) return 0;
-    if (P->compute == TB_C32) return 4;
+    if (P->compute == TB_C32) return cvec_ok(p, nb) ? 6 : 4;
     return narrow_choice(p, nb, P->compute == TB_R32 ? 4 : 8).kind;
 }

@@ -540,9 +540,10 @@ size_t tb_describe(const tb_plan* p, size_t maxlen, char* out)
         if (!warp && p->elem_stage) at = put(out, maxlen, at, " staged=%s", p->elem_stage == 1 ? "A" : "B");
     }
     if (p->path == TB_PATH_SIMT) {
-        static const char* kern[] = {"tiled", "narrow", "narrow_stream", "narrow_coop", "narrow_cstream", "narrow_vec"};
+        static const char* kern[] = {"tiled", "narrow", "narrow_stream", "narrow_coop", "narrow_cstream", "narrow_vec",
+                                     "narrow_cvec"};
         const int k = tbk_simt_kernel(p);
-        if (k >= 0 && k <= 5) at = put(out, maxlen, at, " kernel=%s", kern[k]);
+        if (k >= 0 && k <= 6) at = put(out, maxlen, at, " kernel=%s", kern[k]);
     }
     at = put_modes(out, maxlen, at, "F", &p->F);
     at = put_modes(out, maxlen, at, "K", &p->K);

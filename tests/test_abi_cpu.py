@@ -272,7 +272,8 @@ def test_wait_selftest_argument_checks(tapp):
     ([64, 40, 32, 32], 0, 38, 1, -1, "narrow"),           # binary64 with D along the rank
     ([64, 40, 32, 32], 1, 60, 1, -1, "narrow_vec"),       # binary64 wider than 48
     ([63, 40, 32, 32], 1, 60, 1, -1, "narrow"),
-    ([64, 40, 32, 32], 1, 24, 2, -1, "narrow_cstream"),   # complex float
+    ([64, 40, 32, 32], 1, 24, 2, -1, "narrow_cvec"),      # complex float, rows in 2-row vectors
+    ([63, 40, 32, 32], 1, 24, 2, -1, "narrow_cstream"),   # complex float, odd row extent
     ([64, 40, 32, 32], 1, 24, 3, -1, "tiled"),            # complex double
 ])
 def test_planner_reports_the_cuda_core_kernel(tapp, core, mode, rank, storage, prec, kernel):

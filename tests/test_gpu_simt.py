@@ -246,6 +246,37 @@ def _padded_rows(case):
     return out
 
 
+@pytest.mark.parametrize("ops", [(0, 0, 0, 0), (1, 1, 1, 1), (0, 1, 0, 1)])
+@pytest.mark.parametrize("core,mode,rank", [([64, 40, 36], 1, 24), ([62, 33, 80], 1, 8), ([64, 40, 36], 2, 30)])
+def test_complex_mode_n_products_row_vectors(tapp, oracle, gpu, ops, core, mode, rank):
+    """Complex-float mode-n products with A, C and D contiguous along their
+    rows (the complex register-tiled kernel, 2-row vectors), with op_A, op_B,
+    op_C and op_D: within the binary64 bound, and bit-identical to the same
+    product with padded rows (the complex streaming kernel, the same
+    multiply-add order)."""
+    rng = np.random.default_rng(600 + rank + 7 * sum(ops) + mode)
+    d_ext = list(core)
+    d_ext[mode] = rank
+    d_idx = [0, 1, 2]
+    d_idx[mode] = 3
+    case = spec_case(rng, 2, -1, ([*core], [rank, core[mode]], d_ext, d_ext), ([0, 1, 2], [3, mode], d_idx, d_idx),
+                     "tucker")
+    for t, o in zip((case.A, case.B, case.C, case.D), ops):
+        t.op = o
+    ex = tapp.create_executor()
+    assert "kernel=narrow_cvec" in describe(tapp, case, ex), describe(tapp, case, ex)
+    padded = _padded_rows(case)
+    assert "kernel=narrow_cstream" in describe(tapp, padded, ex), describe(tapp, padded, ex)
+    check_against_f64(tapp, oracle, case, device=True, executor=ex)
+    runs = []
+    for c in (case, padded):
+        run = c.copy()
+        assert run_on_device(tapp, run, ex) == 0
+        runs.append(run.D.buf[run.D.base + run.D.offsets()].copy())
+    assert np.array_equal(runs[0].view(np.uint8), runs[1].view(np.uint8))
+    tapp.lib.TAPP_destroy_executor(ex)
+
+
 @pytest.mark.parametrize("storage,prec", [(0, 0), (0, 6), (1, -1)])
 @pytest.mark.parametrize("core,mode,rank", [([64, 40, 36], 1, 38), ([64, 40, 36], 2, 24), ([62, 33, 80], 1, 8),
                                             ([62, 33, 40], 2, 60), ([32, 48, 64], 1, 64)])
