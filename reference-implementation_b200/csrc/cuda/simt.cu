@@ -1254,6 +1254,43 @@ struct NarrowVecShape {
     static constexpr int S = WIDE ? 3 : 4;
 };
 
+// The multiply-adds of one chunk for the first NP column pairs of a thread's
+// 8 columns (kn contracted values; a: the thread's rows in the ring, b: the
+// B panel at the chunk's first value and the group's first column).
+template <typename T, int NB, int VR, int NP>
+__device__ __forceinline__ void nvec_chunk(T (&acc)[VR][8], const T* a, const T* b, int kn)
+{
+    using NV = NarrowVec<T, VR>;
+    using V = typename NV::V;
+    constexpr int TR = 32 * NarrowVecShape<T, NB>::H * VR;
+#pragma unroll 2
+    for (int kk = 0; kk < kn; kk++) {
+        T x[VR];
+        NV::get(*(const V*)(a + kk * TR), x);
+        const T* bk = b + (size_t)kk * NB;
+        T bv[8];
+        if (sizeof(T) == 4) {
+            const float4 q0 = *(const float4*)bk;
+            bv[0] = (T)q0.x; bv[1] = (T)q0.y; bv[2] = (T)q0.z; bv[3] = (T)q0.w;
+            if (NP > 2) {
+                const float4 q1 = *(const float4*)(bk + 4);
+                bv[4] = (T)q1.x; bv[5] = (T)q1.y; bv[6] = (T)q1.z; bv[7] = (T)q1.w;
+            }
+        } else {
+#pragma unroll
+            for (int n = 0; n < 2 * NP; n += 2) {
+                const double2 q = *(const double2*)((const double*)bk + n);
+                bv[n] = (T)q.x;
+                bv[n + 1] = (T)q.y;
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < VR; r++)
+#pragma unroll
+            for (int n = 0; n < 2 * NP; n += 2) fma2(acc[r][n], acc[r][n + 1], x[r], x[r], bv[n], bv[n + 1]);
+    }
+}
+
 template <typename T, int NB, int VR, bool RND>
 __global__ void __launch_bounds__(NB * 4 * NarrowVecShape<T, NB>::H) k_narrow_vec(NarrowParams np)
 {
@@ -1394,29 +1431,13 @@ __global__ void __launch_bounds__(NB * 4 * NarrowVecShape<T, NB>::H) k_narrow_ve
             const T* a = ring + (size_t)(g % S) * KC * TR + crg * VR;
             const int k0 = c * KC;
             const int kn = p.K - k0 < KC ? (int)(p.K - k0) : KC;
-#pragma unroll 2
-            for (int kk = 0; kk < kn; kk++) {
-                T x[VR];
-                NV::get(*(const V*)(a + kk * TR), x);
-                const T* b = Bs + (k0 + kk) * NB + cg * 8;
-                T bv[8];
-                if (sizeof(T) == 4) {
-                    const float4 q0 = *(const float4*)b, q1 = *(const float4*)(b + 4);
-                    bv[0] = (T)q0.x; bv[1] = (T)q0.y; bv[2] = (T)q0.z; bv[3] = (T)q0.w;
-                    bv[4] = (T)q1.x; bv[5] = (T)q1.y; bv[6] = (T)q1.z; bv[7] = (T)q1.w;
-                } else {
-#pragma unroll
-                    for (int n = 0; n < 8; n += 2) {
-                        const double2 q = *(const double2*)((const double*)b + n);
-                        bv[n] = (T)q.x;
-                        bv[n + 1] = (T)q.y;
-                    }
-                }
-#pragma unroll
-                for (int r = 0; r < VR; r++)
-#pragma unroll
-                    for (int n = 0; n < 8; n += 2) fma2(acc[r][n], acc[r][n + 1], x[r], x[r], bv[n], bv[n + 1]);
-            }
+            // column pairs of this warp's group that hold outputs (the last
+            // group of a padded width has fewer): warp-uniform choice
+            const int pairs = (int)((p.N - cg * 8 + 1) / 2);
+            if (pairs >= 4) nvec_chunk<T, NB, VR, 4>(acc, a, Bs + (size_t)k0 * NB + cg * 8, kn);
+            else if (pairs == 3) nvec_chunk<T, NB, VR, 3>(acc, a, Bs + (size_t)k0 * NB + cg * 8, kn);
+            else if (pairs == 2) nvec_chunk<T, NB, VR, 2>(acc, a, Bs + (size_t)k0 * NB + cg * 8, kn);
+            else nvec_chunk<T, NB, VR, 1>(acc, a, Bs + (size_t)k0 * NB + cg * 8, kn);
         }
         if (last) {
             if (oA >= 0) {
