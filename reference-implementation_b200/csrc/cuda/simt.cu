@@ -1433,11 +1433,19 @@ __global__ void __launch_bounds__(NB * 4 * NarrowVecShape<T, NB>::H) k_narrow_ve
             const int kn = p.K - k0 < KC ? (int)(p.K - k0) : KC;
             // column pairs of this warp's group that hold outputs (the last
             // group of a padded width has fewer): warp-uniform choice
+            // (4-row binary32 tiles only: the other forms ran slower with the
+            // extra code paths)
             const int pairs = (int)((p.N - cg * 8 + 1) / 2);
-            if (pairs >= 4) nvec_chunk<T, NB, VR, 4>(acc, a, Bs + (size_t)k0 * NB + cg * 8, kn);
-            else if (pairs == 3) nvec_chunk<T, NB, VR, 3>(acc, a, Bs + (size_t)k0 * NB + cg * 8, kn);
-            else if (pairs == 2) nvec_chunk<T, NB, VR, 2>(acc, a, Bs + (size_t)k0 * NB + cg * 8, kn);
-            else nvec_chunk<T, NB, VR, 1>(acc, a, Bs + (size_t)k0 * NB + cg * 8, kn);
+            const T* b = Bs + (size_t)k0 * NB + cg * 8;
+            if constexpr (sizeof(T) == 4 && VR == 4) {
+                if (pairs >= 4) nvec_chunk<T, NB, VR, 4>(acc, a, b, kn);
+                else if (pairs == 3) nvec_chunk<T, NB, VR, 3>(acc, a, b, kn);
+                else if (pairs == 2) nvec_chunk<T, NB, VR, 2>(acc, a, b, kn);
+                else nvec_chunk<T, NB, VR, 1>(acc, a, b, kn);
+            } else {
+                (void)pairs;
+                nvec_chunk<T, NB, VR, 4>(acc, a, b, kn);
+            }
         }
         if (last) {
             if (oA >= 0) {
