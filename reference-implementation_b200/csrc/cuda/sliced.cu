@@ -305,7 +305,8 @@ __global__ void __launch_bounds__(256) k_sliced_finish(FinishParams p)
             m = (e / p.N) % p.M;
         }
         l = e / (p.M * p.N);
-        const double* w = p.W + (l * p.M + m) * p.Nout + (CPLX ? 2 * n : n);
+        // W is laid out [l][n][m] (n over the Nout real columns)
+        const double* w = p.W + (l * p.Nout + (CPLX ? 2 * n : n)) * p.M + m;
         const int Ea = p.expA[l * p.M + m], Fb = p.expB[l * p.N + n];
         double xr, xi = 0.0;
         if (Ea >= EXP_BAD || Fb >= EXP_BAD) {
@@ -316,7 +317,7 @@ __global__ void __launch_bounds__(256) k_sliced_finish(FinishParams p)
         } else {
             const int sh = Ea + Fb - 2 * EXP_BIAS;
             xr = scalbn(w[0], sh);
-            if (CPLX) xi = scalbn(w[1], sh);
+            if (CPLX) xi = scalbn(w[p.M], sh);
         }
         double vr = p.alpha_re * xr - (CPLX ? p.alpha_im * xi : 0.0);
         double vi = CPLX ? p.alpha_re * xi + p.alpha_im * xr : 0.0;

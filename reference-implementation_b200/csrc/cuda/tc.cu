@@ -1080,7 +1080,9 @@ __global__ void __launch_bounds__(LOAD == 1 ? 512 : NTHREADS, 1)
             }
             if (EPI == EPI_I32) {
                 // integer products of one level of slices: scaled exactly by a
-                // power of two and added into the binary64 workspace row m
+                // power of two and added into the binary64 workspace W, laid
+                // out [l][n][m] so that the 32 lanes (32 consecutive rows m)
+                // read and write 256 contiguous bytes per column
                 if (et == 0) *epi_ok = mbar_wait(&tfull[acc], aph, abort_flag) ? 1 : 0;
                 epi_bar();
                 const bool ok = *epi_ok != 0;
@@ -1088,8 +1090,7 @@ __global__ void __launch_bounds__(LOAD == 1 ? 512 : NTHREADS, 1)
                 if (ok) {
                     const double sc = e.level_scale;
                     const bool first = e.w_first != 0;
-                    double* wrow = e.W + ((int64_t)l * e.M + m) * e.N;
-                    const bool pairs = (e.N & 1) == 0;
+                    double* wl = e.W + (int64_t)l * e.N * e.M + m;
 #pragma unroll 1
                     for (int t = 0; t < BN / 32 / CS; t++) {
                         const int ch = half + CS * t;
@@ -1097,30 +1098,22 @@ __global__ void __launch_bounds__(LOAD == 1 ? 512 : NTHREADS, 1)
                         __syncwarp();
                         tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + acc * BN + ch * 32, r);
                         const int64_t c0 = (int64_t)tn * BN + ch * 32;
-                        if (!mok || c0 >= e.N) {
-                        } else if (pairs && c0 + 32 <= e.N) {
-                            double2* w2 = (double2*)(wrow + c0);
-                            double2 old[16];
-                            if (!first) {
+                        if (!mok || c0 >= e.N) continue;
+                        const int nj = e.N - c0 < 32 ? (int)(e.N - c0) : 32;
 #pragma unroll
-                                for (int j = 0; j < 16; j++) old[j] = w2[j];
-                            }
+                        for (int h = 0; h < 2; h++) {
+                            // 16 columns: their old values loaded together, then added in column order
+                            double old[16];
+#pragma unroll
+                            for (int j = 0; j < 16; j++)
+                                old[j] = (!first && 16 * h + j < nj) ? wl[(c0 + 16 * h + j) * e.M] : 0.0;
 #pragma unroll
                             for (int j = 0; j < 16; j++) {
-                                double2 v;
-                                v.x = (double)(int)r[2 * j] * sc;
-                                v.y = (double)(int)r[2 * j + 1] * sc;
-                                if (!first) {
-                                    v.x += old[j].x;
-                                    v.y += old[j].y;
+                                if (16 * h + j < nj) {
+                                    double v = (double)(int)r[16 * h + j] * sc;
+                                    if (!first) v += old[j];
+                                    wl[(c0 + 16 * h + j) * e.M] = v;
                                 }
-                                w2[j] = v;
-                            }
-                        } else {
-                            for (int j = 0; j < 32 && c0 + j < e.N; j++) {
-                                double v = (double)(int)r[j] * sc;
-                                if (!first) v += wrow[c0 + j];
-                                wrow[c0 + j] = v;
                             }
                         }
                     }
