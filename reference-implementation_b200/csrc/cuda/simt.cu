@@ -1853,12 +1853,15 @@ size_t simt_scratch_bytes(const tb_plan* P)
 }
 
 // padded width of the narrow kernel for a turned view, or 0 when it does not apply
+static bool vec_choice_ok(const simt::Params& p, int nb, size_t es);
+static bool cvec_ok(const simt::Params& p, int nb);
+
 static int narrow_width(const tb_plan* P, const simt::Params& p)
 {
-    // complex float: the streaming kernel only (A read as stored, rows
-    // contiguous in A and D, at most 32 columns)
+    // complex float: the streaming kernels (A read as stored, rows contiguous
+    // in A and D); more than 32 columns only in 2-row vectors (k_narrow_cvec)
     const bool cplx = P->compute == TB_C32;
-    if (cplx && (p.N > 32 || p.tA != T_C32 || p.round_in != TB_ROUND_NONE || !p.a_rows_fast || !p.d_rows_fast ||
+    if (cplx && (p.N > 64 || p.tA != T_C32 || p.round_in != TB_ROUND_NONE || !p.a_rows_fast || !p.d_rows_fast ||
                  (uintptr_t)p.A % 8 != 0))
         return 0;
     if (P->compute != TB_R32 && P->compute != TB_R64 && !cplx) return 0;
@@ -1867,8 +1870,10 @@ static int narrow_width(const tb_plan* P, const simt::Params& p)
     const size_t es = P->compute == TB_R32 ? 4 : 8;
     const size_t smem = es * (size_t)nb * (size_t)p.K + 8 * ((size_t)p.K + 2 * (size_t)nb);
     if (smem > (size_t)simt::NARROW_MAX_SMEM) return 0;
-    // worth it only where a 64-wide tile wastes work or the contraction is short
-    if (p.N > 48 && p.K > 64) return 0;
+    if (cplx) return p.N <= 32 || cvec_ok(p, nb) ? nb : 0;
+    // the one-row-per-thread kernels pay only where a 64-wide tile wastes
+    // work or the contraction is short; the register tiles also beyond
+    if (p.N > 48 && p.K > 64 && !vec_choice_ok(p, nb, es)) return 0;
     return nb;
 }
 
@@ -1964,6 +1969,9 @@ static NarrowChoice narrow_choice(const simt::Params& p, int nb, size_t es)
     c.smem = smem;
     return c;
 }
+
+// whether the row-vector kernel takes a product of this width
+static bool vec_choice_ok(const simt::Params& p, int nb, size_t es) { return narrow_choice(p, nb, es).kind == NK_VEC; }
 
 template <typename T, int NB>
 static cudaError_t launch_narrow_vec(simt::NarrowParams& np, const NarrowChoice& ch, cudaStream_t s)
@@ -2130,7 +2138,12 @@ cudaError_t launch_simt(const tb_plan* P, const tb_ptrs* d, cudaStream_t s)
             case 8: return launch_narrow_c<8>(np, s);
             case 16: return launch_narrow_c<16>(np, s);
             case 24: return launch_narrow_c<24>(np, s);
-            default: return launch_narrow_c<32>(np, s);
+            case 32: return launch_narrow_c<32>(np, s);
+            // wider: 2-row vectors only (narrow_width checked cvec_ok)
+            case 40: return launch_narrow_cvec<40>(np, s);
+            case 48: return launch_narrow_cvec<48>(np, s);
+            case 56: return launch_narrow_cvec<56>(np, s);
+            default: return launch_narrow_cvec<64>(np, s);
             }
         }
         if (P->compute == TB_R32) {

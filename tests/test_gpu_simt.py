@@ -246,6 +246,26 @@ def _padded_rows(case):
     return out
 
 
+@pytest.mark.parametrize("storage,prec", [(0, 0), (0, 6), (2, -1)])
+@pytest.mark.parametrize("core,mode,rank", [([64, 100, 36], 1, 60), ([48, 40, 130], 2, 52)])
+def test_wide_mode_n_products_row_vectors(tapp, oracle, gpu, storage, prec, core, mode, rank):
+    """Mode-n products with more than 48 columns and a contraction over more
+    than 64 terms, rows contiguous in A, C and D: the register-tiled kernels
+    (real and complex) take them, within the binary64 bound."""
+    rng = np.random.default_rng(700 + rank + 7 * storage + prec + mode)
+    d_ext = list(core)
+    d_ext[mode] = rank
+    d_idx = [0, 1, 2]
+    d_idx[mode] = 3
+    case = spec_case(rng, storage, prec, ([*core], [rank, core[mode]], d_ext, d_ext),
+                     ([0, 1, 2], [3, mode], d_idx, d_idx), "tucker")
+    ex = tapp.create_executor()
+    want = "kernel=narrow_cvec" if storage == 2 else "kernel=narrow_vec"
+    assert want in describe(tapp, case, ex), describe(tapp, case, ex)
+    check_against_f64(tapp, oracle, case, device=True, executor=ex)
+    tapp.lib.TAPP_destroy_executor(ex)
+
+
 @pytest.mark.parametrize("ops", [(0, 0, 0, 0), (1, 1, 1, 1), (0, 1, 0, 1)])
 @pytest.mark.parametrize("core,mode,rank", [([64, 40, 36], 1, 24), ([62, 33, 80], 1, 8), ([64, 40, 36], 2, 30)])
 def test_complex_mode_n_products_row_vectors(tapp, oracle, gpu, ops, core, mode, rank):
