@@ -40,7 +40,7 @@ cudaError_t launch_gemm_i8(const void* A8, const void* B8, int64_t row_bytes, in
 namespace sl {
 
 constexpr int TR = 32;                  // source rows per slicing tile
-constexpr int TK = 128;                 // digit bytes per slice row per tile (one 128-byte line)
+constexpr int TK = 64;                  // digit bytes per slice row per tile
 // Row exponents are kept as code = e + EXP_BIAS (0 for a zero row, EXP_BAD
 // when the row holds a non-finite value), so that a zeroed array and
 // atomicMax over blocks that each see part of a row give the row's code.
@@ -187,22 +187,22 @@ __global__ void __launch_bounds__(256) k_exponents(SliceParams p, int64_t kchunk
     }
 }
 
-// the S digits of 16 values, written as 16-byte groups of one slice row
-// each (B's slices in reverse order)
-__device__ __forceinline__ void put_digits(const SliceParams& p, int64_t out_row, int64_t kbyte, double (&y)[16])
+// the S digits of 8 values, written as 8-byte groups of one slice row each
+// (B's slices in reverse order)
+__device__ __forceinline__ void put_digits(const SliceParams& p, int64_t out_row, int64_t kbyte, double (&y)[8])
 {
     int8_t* base = p.dst + out_row * p.S * p.Kp + kbyte;
     for (int s = 0; s < p.S; s++) {
         const int pos = p.is_B ? p.S - 1 - s : s;
-        uint32_t w[4] = {0u, 0u, 0u, 0u};
+        uint32_t w[2] = {0u, 0u};
 #pragma unroll
-        for (int j = 0; j < 16; j++) {
+        for (int j = 0; j < 8; j++) {
             y[j] *= 128.0;
             const int d = (int)y[j];  // truncation toward zero, |d| <= 127
             y[j] -= (double)d;
             w[j >> 2] |= (uint32_t)(uint8_t)(int8_t)d << (8 * (j & 3));
         }
-        *(uint4*)(base + (int64_t)pos * p.Kp) = make_uint4(w[0], w[1], w[2], w[3]);
+        *(uint2*)(base + (int64_t)pos * p.Kp) = make_uint2(w[0], w[1]);
     }
 }
 
@@ -242,28 +242,28 @@ __global__ void __launch_bounds__(256) k_slice(SliceParams p)
         if (CPLX) tim[r][kk] = p.conj ? -lim[u] : lim[u];
     }
     __syncthreads();
-    const int r = t >> 3, kc = (t & 7) * 16;
+    const int r = t >> 3, kc = (t & 7) * 8;
     const int64_t kbyte = kt * TK + kc;
     if (r0 + r >= p.R || kbyte >= p.Kp) return;
     const double inv = row_inverse(p.expo[l * p.R + r0 + r]);
     if (!CPLX) {
-        double y[16];
+        double y[8];
 #pragma unroll
-        for (int j = 0; j < 16; j++) y[j] = tre[r][kc + j] * inv;
+        for (int j = 0; j < 8; j++) y[j] = tre[r][kc + j] * inv;
         put_digits(p, l * p.Rout + r0 + r, kbyte, y);
     } else if (!p.is_B) {
-        double y[16];
+        double y[8];
 #pragma unroll
-        for (int j = 0; j < 16; j++) {
+        for (int j = 0; j < 8; j++) {
             const int kk = (kc + j) >> 1;
             y[j] = ((kc + j) & 1 ? tim[r][kk] : tre[r][kk]) * inv;
         }
         put_digits(p, l * p.Rout + r0 + r, kbyte, y);
     } else {
         // rows 2c: (re, -im), 2c + 1: (im, re)
-        double y0[16], y1[16];
+        double y0[8], y1[8];
 #pragma unroll
-        for (int j = 0; j < 16; j++) {
+        for (int j = 0; j < 8; j++) {
             const int kk = (kc + j) >> 1;
             const bool odd = (kc + j) & 1;
             y0[j] = (odd ? -tim[r][kk] : tre[r][kk]) * inv;
