@@ -1666,6 +1666,207 @@ __global__ void __launch_bounds__(NB * 8) k_narrow_cvec(NarrowParams np)
     cp_async_wait<0>();
 }
 
+// Register-tiled narrow kernel for binary32 A contiguous along the
+// contraction (mode-n products on the first mode: each row of A is a run of
+// K values; D's rows run along the columns). Tiles of 128 rows; per chunk of
+// 32 contracted values the block copies the tile's chunk with cp.async in
+// 16-byte units (8 consecutive threads on one row's 128 bytes) into a ring
+// of 2 chunks laid out [row][unit], unit u of row r stored at u ^ ((r / 4) %
+// 8), so that the 8 row groups a quarter-warp reads at one unit fall on 8
+// different bank groups. Thread (column group c, lane) takes rows
+// 4 lane..4 lane + 3 and columns 8c..8c+7: per 4 contracted values four
+// 16-byte reads of A and eight broadcast reads of the B panel feed 128
+// multiply-adds. C is read and D written directly from the registers (each
+// thread 8 consecutive columns of its rows), so a block needs about 55 KiB
+// of shared memory and four blocks (20 warps at width 40) share an SM. Every
+// output sees the fused multiply-adds of k_narrow_stream in the same order,
+// so the kernels give the same bits.
+constexpr int NKT_TR = 128, NKT_KC = 32, NKT_S = 2;
+
+template <int NB>
+struct NktShape {
+    static constexpr int MIN_BLOCKS = NB <= 40 ? 4 : NB <= 48 ? 3 : 2;
+};
+
+template <int NB, bool RND>
+__global__ void __launch_bounds__(NB * 4, NktShape<NB>::MIN_BLOCKS) k_narrow_kt(NarrowParams np)
+{
+    constexpr int NT = NB * 4, TR = NKT_TR, KC = NKT_KC, S = NKT_S, UNITS = KC / 4;
+    const Params& p = np.p;
+    extern __shared__ __align__(16) unsigned char nsm[];
+    float* ring = (float*)nsm;                            // [S][TR][KC]
+    float* Bs = ring + (size_t)S * TR * KC;               // [K][NB]
+    int64_t* kA = (int64_t*)(Bs + (size_t)NB * p.K);      // [K]
+    int64_t* nC = kA + p.K;                               // [NB]
+    int64_t* nD = nC + NB;                                // [NB]
+    const int t = threadIdx.x;
+    const int64_t l = blockIdx.y;
+    int64_t lA, lB, lC, lD, dummy;
+    decode(p.al, l, lA, dummy);
+    decode(p.bl, l, lB, dummy);
+    decode(p.cl, l, lC, lD);
+    for (int64_t k = t; k < p.K; k += NT) {
+        int64_t o;
+        decode(p.ak, k, o, dummy);
+        kA[k] = o + lA;
+    }
+    if (t < NB) {
+        int64_t oc = 0, od = 0;
+        if (t < p.N) decode(p.cn, t, oc, od);
+        nC[t] = oc + lC;
+        nD[t] = od + lD;
+    }
+    for (int64_t e = t; e < p.K * NB; e += NT) {
+        const int64_t k = e / NB;
+        const int n = (int)(e % NB);
+        float x = 0, xi = 0;
+        if (n < p.N) {
+            int64_t ob, ok;
+            decode(p.bn, n, ob, dummy);
+            decode(p.bk, k, ok, dummy);
+            load_rounded<float>(p.B, lB + ob + ok, p.tB, p.round_in, x, xi);
+        }
+        Bs[k * NB + n] = x;
+    }
+    __syncthreads();
+
+    const int64_t tiles = (p.M + TR - 1) / TR;
+    if ((int64_t)blockIdx.x >= tiles) return;
+    const int64_t my_tiles = (tiles - 1 - blockIdx.x) / gridDim.x + 1;
+    const int nchunks = (int)((p.K + KC - 1) / KC);
+    const int64_t total = my_tiles * nchunks;
+    const float* A = (const float*)p.A;
+    // offsets of row m in A, C and D (-1: past M)
+    auto row_offsets = [&](int64_t m, int64_t& oA, int64_t& oC, int64_t& oD) {
+        oA = oC = oD = -1;
+        if (m >= p.M) return;
+        oA = oC = oD = 0;
+        uint32_t r = (uint32_t)m;
+        for (int j = 0; j < p.am.n; j++) {
+            const uint32_t q = fdiv(r, np.fm[j]);
+            const int64_t c = (int64_t)(r - q * np.fm[j].d);
+            r = q;
+            oA += c * p.am.s0[j];
+            oC += c * p.cm.s0[j];
+            oD += c * p.cm.s1[j];
+        }
+    };
+    auto tile_row0 = [&](int64_t i) { return ((int64_t)blockIdx.x + i * gridDim.x) * TR; };
+    // producer: unit c = t + NT u of the chunk is row c / UNITS, unit c % UNITS;
+    // NT is a multiple of UNITS, so a thread keeps its unit and walks rows
+    const int pu = t % UNITS, pr0 = t / UNITS;
+    constexpr int PRS = NT / UNITS;
+    const uint32_t ring_base = (uint32_t)__cvta_generic_to_shared(ring);
+    int64_t p_tile = -1;
+    int p_chunk = 0;
+    auto issue = [&](int64_t g) {
+        if (g < total) {
+            if (p_chunk == 0) p_tile++;
+            const int k0 = p_chunk * KC;
+            const int k = k0 + 4 * pu;
+            if (k < p.K) {
+                const uint32_t slot = ring_base + (uint32_t)((g % S) * TR * KC * 4);
+                for (int r = pr0; r < TR; r += PRS) {
+                    int64_t oA, oC_, oD_;
+                    row_offsets(tile_row0(p_tile) + r, oA, oC_, oD_);
+                    if (oA < 0) break;
+                    const uint32_t dst = slot + (uint32_t)((r * UNITS + (pu ^ ((r >> 2) & 7))) * 16);
+                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(A + oA + kA[k]) : "memory");
+                }
+            }
+            if (++p_chunk == nchunks) p_chunk = 0;
+        }
+        cp_async_commit();  // empty groups keep the count uniform
+    };
+    issue(0);
+
+    const int lane = t & 31, cg = t >> 5;
+    const float al = (float)p.alpha, be = (float)p.beta;
+    float acc[4][8];
+    int c = 0;
+    int64_t ti = 0;
+    for (int64_t g = 0; g < total; g++) {
+        cp_async_wait<0>();  // this thread's copies of chunk g have landed
+        __syncthreads();     // everyone's have; the other slot (chunk g - 1) is free
+        issue(g + 1);
+        if (RND) {
+            // the chunk rounded once in place, each value by one thread
+            float4* ch = (float4*)(ring + (size_t)(g % S) * TR * KC);
+            for (int e = t; e < TR * KC / 4; e += NT) {
+                float4 v = ch[e];
+                v.x = round_in<float>(v.x, p.round_in);
+                v.y = round_in<float>(v.y, p.round_in);
+                v.z = round_in<float>(v.z, p.round_in);
+                v.w = round_in<float>(v.w, p.round_in);
+                ch[e] = v;
+            }
+            __syncthreads();
+        }
+        if (c == 0) {
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+#pragma unroll
+                for (int n = 0; n < 8; n++) acc[j][n] = 0.f;
+        }
+        {
+            const float* slot = ring + (size_t)(g % S) * TR * KC;
+            const int k0 = c * KC;
+            const int kn = p.K - k0 < KC ? (int)(p.K - k0) : KC;
+            for (int u = 0; u < kn / 4; u++) {
+                float a[4][4];
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const int r = 4 * lane + j;
+                    const float4 q = *(const float4*)(slot + (size_t)(r * UNITS + (u ^ (lane & 7))) * 4);
+                    a[j][0] = q.x; a[j][1] = q.y; a[j][2] = q.z; a[j][3] = q.w;
+                }
+#pragma unroll
+                for (int kk = 0; kk < 4; kk++) {
+                    const float* b = Bs + (size_t)(k0 + 4 * u + kk) * NB + cg * 8;
+                    const float4 q0 = *(const float4*)b, q1 = *(const float4*)(b + 4);
+                    const float bv[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        const float x = a[j][kk];
+#pragma unroll
+                        for (int n = 0; n < 8; n += 2) fma2(acc[j][n], acc[j][n + 1], x, x, bv[n], bv[n + 1]);
+                    }
+                }
+            }
+        }
+        if (++c == nchunks) {
+            // D = alpha acc + beta C for this thread's 4 rows x 8 columns,
+            // straight from and to global memory
+            const int64_t m0 = tile_row0(ti);
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                int64_t oA_, oC, oD;
+                row_offsets(m0 + 4 * lane + j, oA_, oC, oD);
+                if (oA_ < 0) break;
+                float cv[8];
+#pragma unroll
+                for (int n = 0; n < 8; n++) {
+                    cv[n] = 0.f;
+                    if (!p.beta_zero && cg * 8 + n < p.N) cv[n] = ((const float*)p.C)[oC + nC[cg * 8 + n]];
+                }
+#pragma unroll
+                for (int n = 0; n < 8; n++) {
+                    if (cg * 8 + n < p.N) {
+                        float c1 = cv[n];
+                        if (RND && !p.beta_zero) c1 = round_in<float>(c1, p.round_in);
+                        float v = p.beta_zero ? al * acc[j][n] : fmaf(be, c1, al * acc[j][n]);
+                        if (p.conjD && p.conjD_f32) v = (float)v;
+                        ((float*)p.D)[oD + nD[cg * 8 + n]] = v;
+                    }
+                }
+            }
+            c = 0;
+            ti++;
+        }
+    }
+    cp_async_wait<0>();
+}
+
 // Split of the contraction: enough CTAs to fill the GPU when the tiles do
 // not, each split at least 4 slices long, the workspace at most 256 MiB.
 struct Split {
@@ -1887,7 +2088,9 @@ static int narrow_width(const tb_plan* P, const simt::Params& p)
 //              contraction and D along the columns (C staged whenever read)
 //   NK_VEC     k_narrow_vec: A, C and D contiguous along the first row mode,
 //              read and written as VR-row vectors (register tiles)
-enum { NK_REG = 1, NK_STREAM = 2, NK_COOP = 3, NK_VEC = 5 };
+//   NK_KT      k_narrow_kt: binary32 A contiguous along the contraction in
+//              16-byte runs (register tiles, swizzled shared-memory ring)
+enum { NK_REG = 1, NK_STREAM = 2, NK_COOP = 3, NK_VEC = 5, NK_KT = 7 };
 struct NarrowChoice {
     int kind;
     bool rnd, stage_c;
@@ -1916,6 +2119,26 @@ static bool nvec_layout(const simt::Params& p, int vr, size_t es)
     return true;
 }
 
+// whether k_narrow_kt can copy A's rows in 16-byte runs along the
+// contraction: the first contracted mode has stride 1 and an extent
+// divisible by 4, every other stride of A and its base keep 16-byte alignment
+static bool nkt_layout(const simt::Params& p)
+{
+    auto strides_ok = [&](const simt::Modes& m, int from) {
+        for (int j = from; j < m.n; j++)
+            if (m.s0[j] % 4 != 0) return false;
+        return true;
+    };
+    return p.ak.n >= 1 && p.ak.s0[0] == 1 && p.ak.ext[0] % 4 == 0 && strides_ok(p.ak, 1) && strides_ok(p.am, 0) &&
+           strides_ok(p.al, 0) && (uintptr_t)p.A % 16 == 0;
+}
+
+static size_t nkt_smem(const simt::Params& p, int nb)
+{
+    using namespace simt;
+    return (size_t)NKT_S * NKT_TR * NKT_KC * 4 + 4 * (size_t)nb * (size_t)p.K + 8 * ((size_t)p.K + 2 * (size_t)nb);
+}
+
 static NarrowChoice narrow_choice(const simt::Params& p, int nb, size_t es)
 {
     using namespace simt;
@@ -1941,6 +2164,13 @@ static NarrowChoice narrow_choice(const simt::Params& p, int nb, size_t es)
             c.vr = vr;
             c.stage_c = false;
             c.smem = vsmem;
+            return c;
+        }
+        // widths of 24 and more: at least 3 warps a block
+        if (f32 && nb >= 24 && nkt_layout(p) && nkt_smem(p, nb) <= (size_t)NVEC_MAX_SMEM) {
+            c.kind = NK_KT;
+            c.stage_c = false;
+            c.smem = nkt_smem(p, nb);
             return c;
         }
     }
@@ -2009,6 +2239,33 @@ static cudaError_t launch_narrow_vec(simt::NarrowParams& np, const NarrowChoice&
     return cudaGetLastError();
 }
 
+template <int NB>
+static cudaError_t launch_narrow_kt(simt::NarrowParams& np, const NarrowChoice& ch, cudaStream_t s)
+{
+    using namespace simt;
+    const Params& p = np.p;
+    void (*kern)(NarrowParams) = ch.rnd ? k_narrow_kt<NB, true> : k_narrow_kt<NB, false>;
+    static int attr_done[64][2];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64 || !attr_done[dev][ch.rnd]) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, NVEC_MAX_SMEM);
+        if (e != cudaSuccess) return e;
+        if (dev >= 0 && dev < 64) attr_done[dev][ch.rnd] = 1;
+    }
+    const int threads = NB * 4;
+    const int64_t tiles = (p.M + NKT_TR - 1) / NKT_TR;
+    int per_sm = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, ch.smem) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    int64_t gx = ((int64_t)148 * per_sm + p.L - 1) / p.L;
+    if (gx > tiles) gx = tiles;
+    if (gx < 1) gx = 1;
+    kern<<<dim3((unsigned)gx, (unsigned)p.L), threads, ch.smem, s>>>(np);
+    count_launch();
+    return cudaGetLastError();
+}
+
 template <typename T, int NB>
 static cudaError_t launch_narrow_t(simt::NarrowParams& np, cudaStream_t s)
 {
@@ -2016,6 +2273,9 @@ static cudaError_t launch_narrow_t(simt::NarrowParams& np, cudaStream_t s)
     const Params& p = np.p;
     const NarrowChoice ch = narrow_choice(p, NB, sizeof(T));
     if (ch.kind == NK_VEC) return launch_narrow_vec<T, NB>(np, ch, s);
+    if constexpr (sizeof(T) == 4 && NB >= 24) {
+        if (ch.kind == NK_KT) return launch_narrow_kt<NB>(np, ch, s);
+    }
     const bool plain_a = p.tA == (sizeof(T) == 4 ? T_F32 : T_F64) && p.round_in == TB_ROUND_NONE;
     void (*kern)(NarrowParams) = plain_a ? k_narrow<T, NB, true> : k_narrow<T, NB, false>;
     if constexpr (sizeof(T) == 4) {
@@ -2179,7 +2439,7 @@ cudaError_t launch_simt(const tb_plan* P, const tb_ptrs* d, cudaStream_t s)
 // to another narrow or the tiled kernel for others): 0 tiled, 1 narrow with
 // register prefetch, 2 narrow streaming, 3 narrow cooperative, 4 complex
 // narrow streaming, 5 narrow with row vectors, 6 complex narrow with row
-// vectors. No device call.
+// vectors, 7 narrow with contraction runs. No device call.
 extern "C" int tbk_simt_kernel(const tb_plan* P)
 {
     using namespace tb;

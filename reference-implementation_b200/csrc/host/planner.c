@@ -541,9 +541,9 @@ size_t tb_describe(const tb_plan* p, size_t maxlen, char* out)
     }
     if (p->path == TB_PATH_SIMT) {
         static const char* kern[] = {"tiled", "narrow", "narrow_stream", "narrow_coop", "narrow_cstream", "narrow_vec",
-                                     "narrow_cvec"};
+                                     "narrow_cvec", "narrow_kt"};
         const int k = tbk_simt_kernel(p);
-        if (k >= 0 && k <= 6) at = put(out, maxlen, at, " kernel=%s", kern[k]);
+        if (k >= 0 && k <= 7) at = put(out, maxlen, at, " kernel=%s", kern[k]);
     }
     at = put_modes(out, maxlen, at, "F", &p->F);
     at = put_modes(out, maxlen, at, "K", &p->K);

@@ -264,7 +264,9 @@ def test_wait_selftest_argument_checks(tapp):
     ([64, 40, 32, 32], 1, 38, 0, 0, "narrow_vec"),        # rows contiguous in A, C and D: 4-row vectors
     ([62, 40, 32, 32], 1, 38, 0, 0, "narrow_vec"),        # row extent even: 2-row vectors
     ([63, 40, 32, 32], 1, 38, 0, 0, "narrow_stream"),     # odd row extent: a row per thread
-    ([64, 40, 32, 32], 0, 38, 0, 0, "narrow_coop"),       # A along the contraction, D along the rank
+    ([64, 40, 32, 32], 0, 38, 0, 0, "narrow_kt"),         # A along the contraction in 16-byte runs
+    ([62, 40, 32, 32], 0, 38, 0, 0, "narrow_coop"),       # A along the contraction, D along the rank
+    ([64, 40, 32, 32], 0, 8, 0, 0, "narrow_coop"),        # too narrow for the register tiles
     ([64, 40, 32, 32], 1, 24, 0, 6, "narrow_vec"),        # bf16 precision: rounding after the copy
     ([63, 40, 32, 32], 1, 24, 0, 6, "narrow_stream"),
     ([64, 40, 32, 32], 1, 24, 1, -1, "narrow_vec"),       # binary64, rows contiguous

@@ -246,6 +246,33 @@ def _padded_rows(case):
     return out
 
 
+@pytest.mark.parametrize("prec", [0, 6])
+@pytest.mark.parametrize("rank", [24, 40, 60])
+def test_first_mode_products_contraction_runs(tapp, oracle, gpu, prec, rank):
+    """Mode-n products on the first mode with A's rows read in 16-byte runs
+    along the contraction (the register-tiled kernel with a swizzled ring):
+    within the binary64 bound, and bit-identical to the same product with A's
+    first mode padded, which runs the cooperative kernel with the same
+    summation order."""
+    rng = np.random.default_rng(500 + rank + prec)
+    core = [60, 77, 43]
+    d_ext = [rank, 77, 43]
+    case = spec_case(rng, 0, prec, (core, [rank, 60], d_ext, d_ext), ([0, 1, 2], [3, 0], [3, 1, 2], [3, 1, 2]),
+                     "tucker")
+    ex = tapp.create_executor()
+    assert "kernel=narrow_kt" in describe(tapp, case, ex), describe(tapp, case, ex)
+    padded = _padded_rows(case)
+    assert "kernel=narrow_coop" in describe(tapp, padded, ex), describe(tapp, padded, ex)
+    check_against_f64(tapp, oracle, case, device=True, executor=ex)
+    runs = []
+    for c in (case, padded):
+        run = c.copy()
+        assert run_on_device(tapp, run, ex) == 0
+        runs.append(run.D.buf[run.D.base + run.D.offsets()].copy())
+    assert np.array_equal(runs[0].view(np.uint8), runs[1].view(np.uint8))
+    tapp.lib.TAPP_destroy_executor(ex)
+
+
 @pytest.mark.parametrize("storage,prec", [(0, 0), (0, 6), (2, -1)])
 @pytest.mark.parametrize("core,mode,rank", [([64, 100, 36], 1, 60), ([48, 40, 130], 2, 52)])
 def test_wide_mode_n_products_row_vectors(tapp, oracle, gpu, storage, prec, core, mode, rank):
