@@ -2200,8 +2200,12 @@ static NarrowChoice narrow_choice(const simt::Params& p, int nb, size_t es)
     return c;
 }
 
-// whether the row-vector kernel takes a product of this width
-static bool vec_choice_ok(const simt::Params& p, int nb, size_t es) { return narrow_choice(p, nb, es).kind == NK_VEC; }
+// whether a register-tiled kernel takes a product of this width
+static bool vec_choice_ok(const simt::Params& p, int nb, size_t es)
+{
+    const int k = narrow_choice(p, nb, es).kind;
+    return k == NK_VEC || k == NK_KT;
+}
 
 template <typename T, int NB>
 static cudaError_t launch_narrow_vec(simt::NarrowParams& np, const NarrowChoice& ch, cudaStream_t s)
