@@ -72,7 +72,7 @@ def parse():
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-modes", action="store_true", help="skip the non-headline precision modes")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
-    ap.add_argument("--served", type=int, default=1000,
+    ap.add_argument("--served", type=int, default=20000,
                     help="requests in the served-stream measurement (0 skips it)")
     ap.add_argument("--only-served", action="store_true", help="print only the served-stream measurement")
     ap.add_argument("--no-double", action="store_true", help="skip the binary64 / complex-double measurement")
@@ -261,6 +261,29 @@ class ClockSampler:
         return {"sm_mhz": statistics.median([r[1] for r in use]) if use else None,
                 "sm_max_mhz": use[-1][2] if use else None, "reasons": sorted(reasons),
                 "samples": len(use), "samples_in_timed_region": len(inside), "source": "NVML"}
+
+
+def max_sm_mhz(device=0):
+    """The GPU's maximum SM clock from NVML (read only); 1965 MHz, B200's
+    maximum, when NVML cannot be read."""
+    try:
+        import pynvml as nv
+        nv.nvmlInit()
+        return float(nv.nvmlDeviceGetMaxClockInfo(nv.nvmlDeviceGetHandleByIndex(device), nv.NVML_CLOCK_SM))
+    except Exception:
+        return 1965.0
+
+
+def nominal_cuda_core_tflops(torch, fma_lanes_per_sm):
+    """Nominal CUDA-core peak in TFLOP/s: SMs x FMA lanes per SM x 2 flops x
+    maximum SM clock (B200: 128 binary32 and 64 binary64 FMA lanes per SM).
+    A nominal figure: the plain comparators' fractions are quoted against
+    it ("of nominal"), since no measured CUDA-core peak exists here."""
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    return sms * fma_lanes_per_sm * 2 * max_sm_mhz() * 1e6 / 1e12
+
+
+INT8_DENSE_NOMINAL_TOPS = 4500.0   # B200 dense int8 tensor rate, nominal
 
 
 def measured_peaks():
@@ -871,6 +894,7 @@ def double_measure(lib, torch, slices_list=(7, 8), steps=2, samples=256, ab=C4_A
                 r["slices"] = f64_mode
                 r["int8_gemm_ms"] = main_us / 1e3
                 r["int8_tops"] = int8_ops / (main_us * 1e-6) / 1e12
+                r["int8_frac_of_nominal"] = r["int8_tops"] / INT8_DENSE_NOMINAL_TOPS
             prod.close()
             prod_s.close()
             lib.lib.TAPP_destroy_executor(ex)
@@ -878,6 +902,7 @@ def double_measure(lib, torch, slices_list=(7, 8), steps=2, samples=256, ab=C4_A
             return r
 
         res = {"native": run("native", 0)}
+        res["native"]["fp64_pipe_frac_of_nominal"] = res["native"]["tflops"] / nominal_cuda_core_tflops(torch, 64)
         for S in slices_list:
             res[f"sliced_{S}"] = run(f"sliced_{S}", S)
             res[f"sliced_{S}"]["vs_native"] = res[f"sliced_{S}"]["tflops"] / res["native"]["tflops"]
@@ -898,9 +923,10 @@ def double_measure(lib, torch, slices_list=(7, 8), steps=2, samples=256, ab=C4_A
 
 
 def served_measure(lib, torch, n, seed=5, max_tensor_bytes=1 << 30, load=1.05):
-    """The served configuration on a reduced stream: n requests of the served
-    mix (every tensor at most max_tensor_bytes; the full configuration moves
-    about 34 TB, hours of HBM traffic), operands resident in HBM. A first
+    """The served configuration: n requests (20,000 by default) of the served
+    mix with every tensor at most max_tensor_bytes (with tensors up to the
+    64 GB budget the configuration moves about 34 TB, hours of HBM traffic),
+    operands resident in HBM. A first
     plain pass measures each request's service time; Poisson arrivals at
     `load` times the plain path's capacity (past its saturation) then drive
     both arms, and both arms' latencies are measured:
@@ -949,8 +975,9 @@ def served_measure(lib, torch, n, seed=5, max_tensor_bytes=1 << 30, load=1.05):
                     "40% f32, 30% bf16-accum-f32, 20% f64, 10% c32; HBM budget 64 GB",
         "requests": n, "requests_by_kind": kinds, "max_tensor_bytes": max_tensor_bytes,
         "total_gflop": flops / 1e9,
-        "reduction": f"{n} of 20000 requests; every tensor <= {max_tensor_bytes >> 20} MiB (the configuration as "
-                     "stated moves ~34 TB, 1.5 h or more at HBM speed)",
+        "reduction": (f"{n} of 20000 requests; " if n < 20000 else "all 20000 requests; ") +
+                     f"every tensor <= {max_tensor_bytes >> 20} MiB (the configuration as stated, with tensors up "
+                     "to the 64 GB budget, moves ~34 TB, 1.5 h or more at HBM speed)",
         "arrival_rate_per_s": rate, "load_vs_plain_capacity": load,
         "plain": plain,
         "served_poisson": srv_p,
@@ -1087,6 +1114,8 @@ def run_b200(args):
             lib.lib.TAPP_destroy_executor(mex)
             del mdev
     plain = modes.get("plain_f32", {}).get("tflops")
+    if plain:
+        modes["plain_f32"]["fp32_pipe_frac_of_nominal"] = plain / nominal_cuda_core_tflops(torch, 128)
 
     # ---------------- end to end through host buffers ----------------
     pinned = []

@@ -62,6 +62,10 @@ __device__ __forceinline__ float q16(float v, int fmt)
 
 __global__ void __launch_bounds__(256) k_pack(PackParams p)
 {
+    // a GEMM launched after this pack as a programmatic dependent may start
+    // its set-up once every block of this grid has begun; it reads nothing
+    // of the panels before this grid has finished (griddepcontrol.wait)
+    asm volatile("griddepcontrol.launch_dependents;");
     __shared__ float vr[PR][PK + 1];
     __shared__ float vi[PR][PK + 1];
     __shared__ int64_t rowOff[PR];
@@ -198,6 +202,10 @@ __device__ __forceinline__ float load_as_float<__nv_bfloat16>(const void* base, 
 template <typename T, int SPLIT, int FMT, bool ROWS_FAST, int VEC>
 __global__ void __launch_bounds__(256, 4) k_pack_real(PackParams p)
 {
+    // a GEMM launched after this pack as a programmatic dependent may start
+    // its set-up once every block of this grid has begun; it reads nothing
+    // of the panels before this grid has finished (griddepcontrol.wait)
+    asm volatile("griddepcontrol.launch_dependents;");
     __shared__ float v[FR][FK + 1];
     __shared__ int64_t rowOff[FR];
     __shared__ int64_t kOff[FK];
@@ -283,6 +291,10 @@ __global__ void __launch_bounds__(256, 4) k_pack_real(PackParams p)
         const int64_t idx = ((int64_t)l * p.Rout + rg) * p.Kld + seg * p.Kseg + col;
         *(uint4*)((uint16_t*)p.dst + idx) = make_uint4(w[0], w[1], w[2], w[3]);
     }
+    // launched as a programmatic dependent of the pack before it (the first
+    // operand's), this grid ends only after that one has: whoever waits for
+    // this grid's completion then has both operands' panels
+    asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
 // Pipelined pack for binary32 sources contiguous along the contraction and
@@ -375,6 +387,10 @@ __device__ __forceinline__ void pp_put8(const PackParams& p, int64_t l, int64_t 
 template <int SPLIT, int FMT>
 __global__ void __launch_bounds__(PP_THREADS) k_pack_pipe(PackParams p, PackDivs dv, int32_t ntiles)
 {
+    // a GEMM launched after this pack as a programmatic dependent may start
+    // its set-up once every block of this grid has begun; it reads nothing
+    // of the panels before this grid has finished (griddepcontrol.wait)
+    asm volatile("griddepcontrol.launch_dependents;");
     extern __shared__ __align__(16) float pp_sm[];
     float* slots = pp_sm;
     PackTab* tab = (PackTab*)(pp_sm + PP_STAGES * PP_SLOT);
@@ -457,13 +473,38 @@ __global__ void __launch_bounds__(PP_THREADS) k_pack_pipe(PackParams p, PackDivs
         store(i);
     }
     pp_wait<0>();
+    // launched as a programmatic dependent of the pack before it (the first
+    // operand's), this grid ends only after that one has: whoever waits for
+    // this grid's completion then has both operands' panels
+    asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
 static int num_sms();
 
+// Launches a pack kernel; pdl: as a programmatic dependent of the pack just
+// before it in the stream (the other operand's, same product), so that its
+// blocks start while that pack's last blocks drain. The packs read only the
+// product's operands, which the stream work before the first pack produced.
+template <typename K, typename... Args>
+static void launch_pack_kernel(K kern, dim3 grid, unsigned threads, size_t smem, cudaStream_t s, bool pdl,
+                               Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(threads, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    (void)cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 // false: the kernel could not be given its shared memory (the caller runs k_pack_real)
 template <int SPLIT, int FMT>
-static bool launch_pack_pipe(const PackParams& pp, int64_t lz, cudaStream_t s)
+static bool launch_pack_pipe(const PackParams& pp, int64_t lz, cudaStream_t s, bool pdl)
 {
     auto kern = k_pack_pipe<SPLIT, FMT>;
     static int attr_done[64];
@@ -487,7 +528,7 @@ static bool launch_pack_pipe(const PackParams& pp, int64_t lz, cudaStream_t s)
     dv.tiles_k = make_fastdiv((uint32_t)tiles_k);
     dv.tiles_r = make_fastdiv((uint32_t)tiles_r);
     dv.lsz = make_fastdiv((uint32_t)std::max<int64_t>(pp.Lsz, 1));
-    if (grid > 0) kern<<<(unsigned)grid, PP_THREADS, PP_SMEM, s>>>(pp, dv, (int32_t)ntiles);
+    if (grid > 0) launch_pack_kernel(kern, dim3((unsigned)grid), PP_THREADS, PP_SMEM, s, pdl, pp, dv, (int32_t)ntiles);
     return true;
 }
 
@@ -504,21 +545,21 @@ static bool pack_pipe_fits(const PackParams& pp, int64_t lz)
     return !pp.srcs || pp.Lsz >= 1;
 }
 
-static bool launch_pack_pipe3(const PackParams& pp, int split, int fmt, int64_t lz, cudaStream_t s)
+static bool launch_pack_pipe3(const PackParams& pp, int split, int fmt, int64_t lz, cudaStream_t s, bool pdl)
 {
-    if (split == 3) return launch_pack_pipe<3, 0>(pp, lz, s);
-    if (split == 2) return launch_pack_pipe<2, 0>(pp, lz, s);
-    if (fmt == 1) return launch_pack_pipe<1, 1>(pp, lz, s);
-    return launch_pack_pipe<1, 0>(pp, lz, s);
+    if (split == 3) return launch_pack_pipe<3, 0>(pp, lz, s, pdl);
+    if (split == 2) return launch_pack_pipe<2, 0>(pp, lz, s, pdl);
+    if (fmt == 1) return launch_pack_pipe<1, 1>(pp, lz, s, pdl);
+    return launch_pack_pipe<1, 0>(pp, lz, s, pdl);
 }
 
 template <typename T, bool RF, int VEC>
-static void launch_pack_real3(const PackParams& pp, int split, int fmt, dim3 grid, cudaStream_t s)
+static void launch_pack_real3(const PackParams& pp, int split, int fmt, dim3 grid, cudaStream_t s, bool pdl)
 {
-    if (split == 3) k_pack_real<T, 3, 0, RF, VEC><<<grid, 256, 0, s>>>(pp);
-    else if (split == 2) k_pack_real<T, 2, 0, RF, VEC><<<grid, 256, 0, s>>>(pp);
-    else if (fmt == 1) k_pack_real<T, 1, 1, RF, VEC><<<grid, 256, 0, s>>>(pp);
-    else k_pack_real<T, 1, 0, RF, VEC><<<grid, 256, 0, s>>>(pp);
+    if (split == 3) launch_pack_kernel(k_pack_real<T, 3, 0, RF, VEC>, grid, 256, 0, s, pdl, pp);
+    else if (split == 2) launch_pack_kernel(k_pack_real<T, 2, 0, RF, VEC>, grid, 256, 0, s, pdl, pp);
+    else if (fmt == 1) launch_pack_kernel(k_pack_real<T, 1, 1, RF, VEC>, grid, 256, 0, s, pdl, pp);
+    else launch_pack_kernel(k_pack_real<T, 1, 0, RF, VEC>, grid, 256, 0, s, pdl, pp);
 }
 
 // whether a mode list's first mode has stride 1 and extent % 4 == 0 and all
@@ -537,7 +578,8 @@ static bool vec4_ok(const ModeList& fast, const ModeList* others[], int nothers,
 // grid.z = lz panel batches (the batch modes, times the batches of a batched
 // product); aligned: every source base of a batched product is 16-byte aligned
 template <typename T>
-static void launch_pack_real(const PackParams& pp, int split, int fmt, int64_t lz, bool aligned, cudaStream_t s)
+static void launch_pack_real(const PackParams& pp, int split, int fmt, int64_t lz, bool aligned, cudaStream_t s,
+                             bool pdl = false)
 {
     dim3 grid((unsigned)((pp.R + FR - 1) / FR), (unsigned)((pp.Kseg + FK - 1) / FK), (unsigned)lz);
     const bool rf = pp.rows_fast != 0;
@@ -546,13 +588,13 @@ static void launch_pack_real(const PackParams& pp, int split, int fmt, int64_t l
         const ModeList* others[3] = {rf ? &pp.ks : &pp.rows, &pp.ls, &pp.us};
         v4 = vec4_ok(rf ? pp.rows : pp.ks, others, 2, pp.src);
     }
-    if (v4 && !rf && pack_pipe_fits(pp, lz) && launch_pack_pipe3(pp, split, fmt, lz, s)) return;
+    if (v4 && !rf && pack_pipe_fits(pp, lz) && launch_pack_pipe3(pp, split, fmt, lz, s, pdl)) return;
     if (rf) {
-        if (v4) launch_pack_real3<T, true, 4>(pp, split, fmt, grid, s);
-        else launch_pack_real3<T, true, 1>(pp, split, fmt, grid, s);
+        if (v4) launch_pack_real3<T, true, 4>(pp, split, fmt, grid, s, pdl);
+        else launch_pack_real3<T, true, 1>(pp, split, fmt, grid, s, pdl);
     } else {
-        if (v4) launch_pack_real3<T, false, 4>(pp, split, fmt, grid, s);
-        else launch_pack_real3<T, false, 1>(pp, split, fmt, grid, s);
+        if (v4) launch_pack_real3<T, false, 4>(pp, split, fmt, grid, s, pdl);
+        else launch_pack_real3<T, false, 1>(pp, split, fmt, grid, s, pdl);
     }
 }
 
@@ -653,6 +695,10 @@ __global__ void __launch_bounds__(LOAD == 1 ? 512 : NTHREADS, 1)
     else __syncthreads();
     fence_after();
     const uint32_t tmem_base = *tmem_slot;
+    // launched as a programmatic dependent of the operand pack: everything
+    // above touched only shared and tensor memory; wait for the pack's grid
+    // (and its writes) before any global access (a no-op otherwise)
+    asm volatile("griddepcontrol.wait;" ::: "memory");
 
     // tiles: one CTA walks 128x256 tiles; a pair walks 256x256 tiles together
     const int unit = CTA2 ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;
@@ -1402,7 +1448,7 @@ struct Workspace {
 // load 2: the split-bfloat16 GEMM from [hi | lo] panels (both pairs only).
 static cudaError_t launch_gemm(int kind, bool cta2, int grid, const CUtensorMap& tmA, const CUtensorMap& tmB,
                                const GemmParams& gp, uint32_t idesc, const CUtensorMap& tmC, const CUtensorMap& tmD,
-                               cudaStream_t s, int load = 0)
+                               cudaStream_t s, int load = 0, bool pdl = false)
 {
     void (*kern)(CUtensorMap, CUtensorMap, GemmParams, uint32_t, CUtensorMap, CUtensorMap);
     if (load == 1)
@@ -1430,13 +1476,15 @@ static cudaError_t launch_gemm(int kind, bool cta2, int grid, const CUtensorMap&
     cfg.blockDim = dim3(load == 1 ? 512 : NTHREADS, 1, 1);
     cfg.dynamicSmemBytes = SMEM_BYTES;
     cfg.stream = s;
-    cudaLaunchAttribute attr[1];
+    cudaLaunchAttribute attr[2];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = cta2 ? 2 : 1;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
+    attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[1].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = pdl ? 2 : 1;
     return cudaLaunchKernelEx(&cfg, kern, tmA, tmB, gp, idesc, tmC, tmD);
 }
 
@@ -1746,27 +1794,44 @@ bool group_item(const tb_plan* P, const tb_ptrs* d, bool cta2, tc::GroupItem* g)
 int tc_sm_count() { return tc::num_sms(); }
 
 // A last round that fills at most half the units runs its tiles as two
-// half-contraction items each (partial sums handed over in memory).
-static void plan_split_round(tc::GemmParams& gp, int kind, int units, void** split_ws, cudaStream_t s)
+// half-contraction items each (partial sums handed over in memory). Only the
+// binary32 epilogues (EPI_TMA, EPI_F32) hand over partial sums. The hand-over
+// counters are zeroed here, before the operand packs are launched, so that
+// nothing stands between the last pack and the GEMM in the stream.
+struct SplitRound {
+    int r = 0;
+    void* ws = nullptr;
+};
+
+static SplitRound plan_split_round(bool f32_epi, int num_tiles, int num_kb, int units, cudaStream_t s)
 {
     using namespace tc;
-    *split_ws = nullptr;
-    if (!((kind == EPI_TMA || kind == EPI_F32) && gp.num_tiles > units && gp.num_kb >= 2)) return;
-    const int r = gp.num_tiles % units;
-    if (r == 0 || 2 * r > units) return;
+    SplitRound sr;
+    if (!(f32_epi && num_tiles > units && num_kb >= 2)) return sr;
+    const int r = num_tiles % units;
+    if (r == 0 || 2 * r > units) return sr;
     const size_t pbytes = (size_t)r * 2 * BN * BM * sizeof(float);
     const size_t fbytes = (size_t)r * 2 * 2 * sizeof(int);
-    if (pool_alloc(split_ws, pbytes + fbytes, s) == cudaSuccess &&
-        cudaMemsetAsync((char*)*split_ws + pbytes, 0, fbytes, s) == cudaSuccess) {
-        gp.split_tiles = r;
-        gp.partial = (float*)*split_ws;
-        gp.pcount = (int*)((char*)*split_ws + pbytes);
-        gp.pready = gp.pcount + r * 2;
-    } else if (*split_ws) {
-        cudaFreeAsync(*split_ws, s);
-        *split_ws = nullptr;
+    if (pool_alloc(&sr.ws, pbytes + fbytes, s) == cudaSuccess &&
+        cudaMemsetAsync((char*)sr.ws + pbytes, 0, fbytes, s) == cudaSuccess) {
+        sr.r = r;
+    } else if (sr.ws) {
+        cudaFreeAsync(sr.ws, s);
+        sr.ws = nullptr;
     }
     (void)cudaGetLastError();
+    return sr;
+}
+
+static void use_split_round(tc::GemmParams& gp, const SplitRound& sr)
+{
+    using namespace tc;
+    if (!sr.r) return;
+    const size_t pbytes = (size_t)sr.r * 2 * BN * BM * sizeof(float);
+    gp.split_tiles = sr.r;
+    gp.partial = (float*)sr.ws;
+    gp.pcount = (int*)((char*)sr.ws + pbytes);
+    gp.pready = gp.pcount + sr.r * 2;
 }
 
 cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t s, int* kernels, void** main_timer)
@@ -1865,6 +1930,14 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
                                             side == 0 ? BM : (cta2 ? Geo<true>::b_rows : BN), &dmn[side], &de0[side],
                                             &dk0[side], &dbox[side], &dmask[side]);
 
+        // the split last round's counters, zeroed before the packs
+        const bool f32_epi = !cplx && P->tD == T_F32 && (P->beta_zero || P->tC == T_F32) && !P->conjD;
+        const int units = cta2 ? num_sms() / 2 : num_sms();
+        const int64_t g_tiles = ((M + (cta2 ? 2 * BM : BM) - 1) / (cta2 ? 2 * BM : BM)) * ((Nout + BN - 1) / BN) * Lg;
+        const int64_t g_kb = ((cvt ? K : spl ? Kseg : Kld) + BK - 1) / BK;
+        const SplitRound sr = plan_split_round(f32_epi, (int)g_tiles, (int)g_kb, units, s);
+        int packs = 0;
+
         // pack A and B
         for (int side = 0; side < 2; side++) {
             if (dir[side]) continue;
@@ -1897,11 +1970,13 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
                                            pp.type == T_BF16)) {
                 // the vector loads need every batch's base 16-byte aligned
                 const bool al = side == 0 ? a_vec_ok : b_vec_ok;
+                // B's pack right after A's (a single product) overlaps its tail
+                const bool pdl = G == 1 && packs == 1;
                 switch (pp.type) {
-                case T_F32: launch_pack_real<float>(pp, split, fmt, Lg, al, s); break;
-                case T_F64: launch_pack_real<double>(pp, split, fmt, Lg, al, s); break;
-                case T_F16: launch_pack_real<__half>(pp, split, fmt, Lg, al, s); break;
-                default: launch_pack_real<__nv_bfloat16>(pp, split, fmt, Lg, al, s); break;
+                case T_F32: launch_pack_real<float>(pp, split, fmt, Lg, al, s, pdl); break;
+                case T_F64: launch_pack_real<double>(pp, split, fmt, Lg, al, s, pdl); break;
+                case T_F16: launch_pack_real<__half>(pp, split, fmt, Lg, al, s, pdl); break;
+                default: launch_pack_real<__nv_bfloat16>(pp, split, fmt, Lg, al, s, pdl); break;
                 }
             } else {
                 dim3 grid((unsigned)((pp.R + PR - 1) / PR), (unsigned)((Kseg / (cplx ? 2 : 1) + PK - 1) / PK),
@@ -1910,9 +1985,13 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
             }
             count_launch();
             (*kernels)++;
+            packs++;
         }
         e = cudaGetLastError();
-        if (e != cudaSuccess) break;
+        if (e != cudaSuccess) {
+            if (sr.ws) cudaFreeAsync(sr.ws, s);
+            break;
+        }
 
         CUtensorMap tmA, tmB;
         if (cvt) {
@@ -1926,6 +2005,7 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
         } else if ((!dir[0] && !make_map(&tmA, pA, fmt, Kld, M, Lg, BM)) ||
             (!dir[1] && !make_map(&tmB, pB, fmt, Kld, Nout, Lg, cta2 ? Geo<true>::b_rows : BN))) {
             e = cudaErrorInvalidValue;
+            if (sr.ws) cudaFreeAsync(sr.ws, s);
             break;
         }
         GemmParams gp;
@@ -1974,7 +2054,6 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
         const uint32_t mma_m = cta2 ? 2 * BM : BM;
         const uint32_t idesc = (1u << 4) | (ab << 7) | (ab << 10) | ((uint32_t)gp.a_mn << 15) |
                                ((uint32_t)gp.b_mn << 16) | ((uint32_t)(BN >> 3) << 17) | ((mma_m >> 4) << 24);
-        const bool f32_epi = !cplx && P->tD == T_F32 && (P->beta_zero || P->tC == T_F32) && !P->conjD;
         CUtensorMap tmC = tmA, tmD = tmA;  // placeholders when the TMA epilogue is not used
         bool tma_epi = false;
         if (G == 1) {
@@ -1995,15 +2074,20 @@ cudaError_t launch_tc(const tb_plan* P, const tb_ptrs* d, int num, cudaStream_t 
             }
         }
         const int kind = tma_epi ? EPI_TMA : (f32_epi ? EPI_F32 : EPI_ANY);
-        const int units = cta2 ? num_sms() / 2 : num_sms();
-        void* split_ws = nullptr;
-        plan_split_round(gp, kind, units, &split_ws, s);
+        use_split_round(gp, sr);
         const int items = gp.num_tiles + gp.split_tiles;
         const int grid = (items < units ? items : units) * (cta2 ? 2 : 1);
-        if (main_timer && b0 == 0) tbk_timer_begin(s, main_timer);
-        e = launch_gemm(kind, cta2, grid, tmA, tmB, gp, idesc, tmC, tmD, s, cvt ? 1 : spl ? 2 : 0);
-        if (main_timer && b0 == 0) tbk_timer_end(s, *main_timer);
-        if (split_ws) cudaFreeAsync(split_ws, s);
+        const bool timed = main_timer && b0 == 0;
+        // the GEMM follows its last pack directly (a single product: no
+        // staging copy between them; no timer event) as a programmatic
+        // dependent launch: its CTAs start, set up their barriers and tensor
+        // memory while the pack drains, and wait for the pack's grid
+        // (griddepcontrol.wait) before their first global memory access
+        const bool pdl = packs > 0 && G == 1 && !timed;
+        if (timed) tbk_timer_begin(s, main_timer);
+        e = launch_gemm(kind, cta2, grid, tmA, tmB, gp, idesc, tmC, tmD, s, cvt ? 1 : spl ? 2 : 0, pdl);
+        if (timed) tbk_timer_end(s, *main_timer);
+        if (sr.ws) cudaFreeAsync(sr.ws, s);
         count_launch();
         (*kernels)++;
         if (e != cudaSuccess) break;
