@@ -951,7 +951,7 @@ def served_measure(lib, torch, n, seed=5, max_tensor_bytes=1 << 30, load=1.05):
     plain_lat, plain_span = run.run_plain_arrivals(ex, arrivals)
     lib.lib.TAPP_destroy_executor(ex)
     flops = float(run.flops.sum())
-    with Server(lib, 64 << 30, n_streams=4, max_in_flight=64) as srv:
+    with Server(lib, 64 << 30, n_streams=8, max_in_flight=64) as srv:
         run.run_served(srv, arrivals=None)               # warm-up of the served path
         burst = run.run_served(srv, arrivals=None)
         poisson = run.run_served(srv, arrivals=arrivals)
