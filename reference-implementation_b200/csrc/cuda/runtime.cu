@@ -343,6 +343,16 @@ int tbk_host_func(void* stream, void (*fn)(void*), void* arg)
     return (int)cudaLaunchHostFunc((cudaStream_t)stream, fn, arg);
 }
 
+int tbk_event_create(void** ev)
+{
+    cudaEvent_t e = nullptr;
+    cudaError_t r = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    *ev = e;
+    return (int)r;
+}
+
+int tbk_event_record(void* ev, void* stream) { return (int)cudaEventRecord((cudaEvent_t)ev, (cudaStream_t)stream); }
+
 int tbk_host_alloc(void** p, size_t bytes)
 {
     tb::count_allocation();

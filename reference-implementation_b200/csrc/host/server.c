@@ -23,15 +23,17 @@
  *              product is a unit of its own.
  *              Units are spread round-robin over the server's streams, each
  *              as: staging copies in, kernel(s), copy of D out, frees, and a
- *              stream callback;
- *   completion the callback (a CUDA driver thread, no CUDA calls) stamps the
- *              products' completion time, returns their budget and slots and
- *              wakes the scheduler and waiters.
+ *              completion event;
+ *   completion the completion thread polls the oldest pending unit of each
+ *              stream; once its event has passed it stamps the products'
+ *              completion time, returns their budget and slots and wakes the
+ *              scheduler and waiters.
  * Admission therefore runs whenever work completes or arrives, so products
  * join the device while others are still running (continuous batching).
  */
 #define _POSIX_C_SOURCE 200809L
 #include <pthread.h>
+#include <sched.h>
 #include <stdlib.h>
 #include <string.h>
 #include <time.h>
@@ -77,8 +79,15 @@ struct tb_server {
     pthread_mutex_t lock;
     pthread_cond_t cv_sched;  /* queue, budget or slots changed */
     pthread_cond_t cv_done;   /* a product completed */
+    pthread_cond_t cv_reap;   /* a unit was issued (the completion thread's wake-up) */
     pthread_t thread;
-    int stop;
+    pthread_t reaper;         /* completion thread: polls the issued units' events */
+    int stop, reap_stop;
+
+    /* issued units not yet complete, per stream in issue order (a stream
+     * completes its units in that order) */
+    struct srv_unit *pend_head[SRV_MAX_STREAMS], *pend_tail[SRV_MAX_STREAMS];
+    int64_t n_pend;
 
     srv_req *head, *tail;
 
@@ -102,6 +111,8 @@ typedef struct srv_unit {
     struct tb_server* srv;
     int n, slab, err;
     int tc_tile;     /* grouped tensor-core unit: its tile shape (1, 2); 0 otherwise */
+    void* ev;        /* recorded on the unit's stream after its work */
+    struct srv_unit* next_pend;
     srv_req* req[SRV_GROUP_MAX];
 } srv_unit;
 
@@ -155,7 +166,7 @@ static int cuda_code(int e) { return e == TBK_ERR_NOMEM ? TAPP_B200_ERR_NOMEM : 
 
 static int64_t round512(int64_t b) { return (b + 511) & ~(int64_t)511; }
 
-/* ---- completion (CUDA driver thread) ---- */
+/* ---- completion (completion thread) ---- */
 
 static void unit_done(void* arg)
 {
@@ -244,7 +255,8 @@ static int take_slab(struct tb_server* s)
 
 static void issue(struct tb_server* s, srv_unit* u)
 {
-    void* stream = s->streams[s->rr++ % s->n_streams];
+    const int si = s->rr++ % s->n_streams;
+    void* stream = s->streams[si];
     tb_ptrs dp[SRV_GROUP_MAX];
     int e = 0;
     for (int i = 0; i < u->n && !e; i++) e = stage_in(u->req[i], stream, &dp[i]);
@@ -278,11 +290,91 @@ static void issue(struct tb_server* s, srv_unit* u)
     for (int i = 0; i < u->n; i++)
         if (u->req[i]->P.path == TB_PATH_TC || u->req[i]->P.path == TB_PATH_SLICED) s->tc_ran = 1;
     pthread_mutex_unlock(&s->lock);
-    if (tbk_host_func(stream, unit_done, u)) {
+    void* ev = NULL;
+    if (!tbk_event_create(&ev) && !tbk_event_record(ev, stream)) {
+        u->ev = ev;
+        u->next_pend = NULL;
+        pthread_mutex_lock(&s->lock);
+        if (s->pend_tail[si]) s->pend_tail[si]->next_pend = u;
+        else s->pend_head[si] = u;
+        s->pend_tail[si] = u;
+        s->n_pend++;
+        pthread_cond_signal(&s->cv_reap);
+        pthread_mutex_unlock(&s->lock);
+    } else {
+        if (ev) tbk_event_destroy(ev);
         tbk_stream_sync(stream);
         if (!u->err) u->err = TAPP_B200_ERR_CUDA;
         unit_done(u);
     }
+}
+
+/* Completion thread: polls the issued units of every stream in issue order
+ * (a stream completes them in that order) and completes each run of units
+ * whose events have passed. Polling (a yield between sweeps, a 20 us sleep
+ * once sweeps have found nothing for a while) answers within microseconds
+ * of a unit's end, where a stream callback waits for the driver's callback
+ * thread and holds its stream until it returns; it keeps a host core busy
+ * while units are in flight and sleeps on cv_reap when none are. */
+#define SRV_REAP_MAX 32  /* units of one stream looked at per sweep */
+static void* reaper(void* arg)
+{
+    struct tb_server* s = (struct tb_server*)arg;
+    tbk_set_device(s->device);
+    int idle = 0;
+    srv_unit* seen[SRV_MAX_STREAMS][SRV_REAP_MAX];
+    int nseen[SRV_MAX_STREAMS], ndone[SRV_MAX_STREAMS];
+    pthread_mutex_lock(&s->lock);
+    for (;;) {
+        while (!s->n_pend && !s->reap_stop) {
+            idle = 0;
+            pthread_cond_wait(&s->cv_reap, &s->lock);
+        }
+        if (!s->n_pend) break;  /* stopping, nothing in flight */
+        const int ns = s->n_streams;
+        for (int i = 0; i < ns; i++) {
+            nseen[i] = 0;
+            for (srv_unit* u = s->pend_head[i]; u && nseen[i] < SRV_REAP_MAX; u = u->next_pend) seen[i][nseen[i]++] = u;
+        }
+        pthread_mutex_unlock(&s->lock);
+        /* only this thread removes units, so the ones seen stay valid unlocked */
+        int total = 0;
+        for (int i = 0; i < ns; i++) {
+            ndone[i] = 0;
+            for (int j = 0; j < nseen[i]; j++) {
+                srv_unit* u = seen[i][j];
+                const int q = tbk_event_done(u->ev);
+                if (q == 0) break;
+                if (q < 0 && !u->err) u->err = TAPP_B200_ERR_CUDA;
+                ndone[i]++;
+            }
+            total += ndone[i];
+        }
+        if (total) {
+            pthread_mutex_lock(&s->lock);
+            for (int i = 0; i < ns; i++) {
+                if (!ndone[i]) continue;
+                s->pend_head[i] = seen[i][ndone[i] - 1]->next_pend;
+                if (!s->pend_head[i]) s->pend_tail[i] = NULL;
+            }
+            s->n_pend -= total;
+            pthread_mutex_unlock(&s->lock);
+            for (int i = 0; i < ns; i++)
+                for (int j = 0; j < ndone[i]; j++) {
+                    tbk_event_destroy(seen[i][j]->ev);
+                    unit_done(seen[i][j]);
+                }
+            idle = 0;
+        } else if (++idle < 256) {
+            sched_yield();
+        } else {
+            const struct timespec ts = {0, 20000};
+            nanosleep(&ts, NULL);
+        }
+        pthread_mutex_lock(&s->lock);
+    }
+    pthread_mutex_unlock(&s->lock);
+    return NULL;
 }
 
 /* a tensor-core product that a grouped launch runs with the same result as
@@ -550,6 +642,7 @@ TAPP_error tapp_b200_server_create(TAPP_b200_server* server, TAPP_executor exec,
     pthread_mutex_init(&s->lock, NULL);
     pthread_cond_init(&s->cv_sched, NULL);
     pthread_cond_init(&s->cv_done, NULL);
+    pthread_cond_init(&s->cv_reap, NULL);
     int err = 0;
     for (int i = 0; i < n_streams && !err; i++)
         if ((e = tbk_stream_create(&s->streams[i]))) err = cuda_code(e);
@@ -560,6 +653,11 @@ TAPP_error tapp_b200_server_create(TAPP_b200_server* server, TAPP_executor exec,
         if ((e = tbk_host_alloc(&s->slab[i], s->slab_bytes))) err = cuda_code(e);
         s->slab_free[i] = 1;
     }
+    int reaper_on = 0;
+    if (!err) {
+        if (pthread_create(&s->reaper, NULL, reaper, s)) err = TAPP_B200_ERR_NOMEM;
+        else reaper_on = 1;
+    }
     if (!err && pthread_create(&s->thread, NULL, scheduler, s)) err = TAPP_B200_ERR_NOMEM;
     if (!err && !live_add(s)) {
         pthread_mutex_lock(&s->lock);
@@ -569,6 +667,13 @@ TAPP_error tapp_b200_server_create(TAPP_b200_server* server, TAPP_executor exec,
         pthread_join(s->thread, NULL);
         err = TAPP_B200_ERR_LIMIT;
     }
+    if (err && reaper_on) {
+        pthread_mutex_lock(&s->lock);
+        s->reap_stop = 1;
+        pthread_cond_broadcast(&s->cv_reap);
+        pthread_mutex_unlock(&s->lock);
+        pthread_join(s->reaper, NULL);
+    }
     if (err) {
         for (int i = 0; i < s->n_slabs; i++)
             if (s->slab[i]) tbk_host_free(s->slab[i]);
@@ -577,6 +682,7 @@ TAPP_error tapp_b200_server_create(TAPP_b200_server* server, TAPP_executor exec,
         pthread_mutex_destroy(&s->lock);
         pthread_cond_destroy(&s->cv_sched);
         pthread_cond_destroy(&s->cv_done);
+        pthread_cond_destroy(&s->cv_reap);
         free(s);
         return err;
     }
@@ -723,6 +829,11 @@ TAPP_error tapp_b200_server_destroy(TAPP_b200_server server)
     pthread_cond_broadcast(&s->cv_sched);
     pthread_mutex_unlock(&s->lock);
     pthread_join(s->thread, NULL);
+    pthread_mutex_lock(&s->lock);
+    s->reap_stop = 1;  /* the reaper ends once the issued units have completed */
+    pthread_cond_broadcast(&s->cv_reap);
+    pthread_mutex_unlock(&s->lock);
+    pthread_join(s->reaper, NULL);
     for (int i = 0; i < s->n_streams; i++) {
         tbk_stream_sync(s->streams[i]);
         tbk_stream_destroy(s->streams[i]);
@@ -733,6 +844,7 @@ TAPP_error tapp_b200_server_destroy(TAPP_b200_server server)
     pthread_mutex_destroy(&s->lock);
     pthread_cond_destroy(&s->cv_sched);
     pthread_cond_destroy(&s->cv_done);
+    pthread_cond_destroy(&s->cv_reap);
     s->magic = 0;
     free(s);
     return err;

@@ -56,6 +56,10 @@ int tbk_run_plan_batched(const tb_plan* plan, const tb_ptrs* ptrs, int num, void
 int tbk_stream_create(void** stream);
 int tbk_stream_destroy(void* stream);
 int tbk_host_func(void* stream, void (*fn)(void*), void* arg);
+/* Completion events (no timing): recorded on a stream, polled with
+ * tbk_event_done and freed with tbk_event_destroy (below). */
+int tbk_event_create(void** ev);
+int tbk_event_record(void* ev, void* stream);
 int tbk_host_alloc(void** p, size_t bytes);   /* page-locked host memory */
 int tbk_host_free(void* p);
 
