@@ -116,7 +116,7 @@ __device__ __forceinline__ double row_inverse(int code)
 // meet in p.expo (zeroed first) by atomicMax. RF: rows contiguous in the
 // source (threads along rows), otherwise one warp per row along k.
 template <bool RF>
-__global__ void __launch_bounds__(256) k_exponents(SliceParams p, int64_t kchunk)
+__global__ void __launch_bounds__(256, 4) k_exponents(SliceParams p, int64_t kchunk)
 {
     __shared__ int part[8][TR];
     const int t = threadIdx.x;
