@@ -657,7 +657,8 @@ def tiny_latency_measure(lib, torch, n=2000):
         burst_s = time.perf_counter() - t0
     out["server"] = {"p50_us": one["p50_us"], "p99_us": one["p99_us"], "burst_products_per_s": n / burst_s}
     # device loop
-    err, loop = lib.loop_create(0, blocks=32, slots=256, idle_ms=100.0)
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    err, loop = lib.loop_create(0, blocks=sms, slots=256, idle_ms=100.0)
     assert err == 0
     for d in order[:200]:
         lib.lib.tapp_b200_loop_wait(loop, lib.loop_submit(loop, d[3], *args(d))[1])

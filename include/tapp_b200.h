@@ -224,7 +224,7 @@ TAPP_EXPORT TAPP_error tapp_b200_load_tile_table(const char* path);
 /*
  * A device-resident request loop for small products (no counterpart in the
  * reference, whose handle and executor are placeholders): a persistent
- * kernel of `blocks` blocks (1..64; every block takes a share of each
+ * kernel of `blocks` blocks (1..256; every block takes a share of each
  * product's outputs) stays on the GPU and computes products as they are
  * submitted, with no kernel launch per product. Submission writes the
  * product's descriptor into a ring of `slots` entries in page-locked host

@@ -99,7 +99,7 @@ static int ensure_running(struct tb_loop* l)
 
 TAPP_error tapp_b200_loop_create(TAPP_b200_loop* loop, TAPP_executor exec, int blocks, int slots, double idle_ms)
 {
-    if (!loop || blocks < 1 || blocks > 64 || slots < blocks || slots > 4096 || !(idle_ms > 0.0) || idle_ms > 10000.0)
+    if (!loop || blocks < 1 || blocks > 256 || slots < blocks || slots > 4096 || !(idle_ms > 0.0) || idle_ms > 10000.0)
         return TAPP_B200_ERR_INVALID;
     *loop = 0;
     struct tb_loop* l = calloc(1, sizeof(*l));

@@ -75,13 +75,18 @@ def _plain(tapp, devs):
     return out
 
 
-def test_loop_matches_execute_product(tapp, gpu):
+@pytest.mark.parametrize("blocks", [4, "sms"])
+def test_loop_matches_execute_product(tapp, gpu, blocks):
     """Products of every compute domain, small enough for the element path,
-    submitted back to back (tickets in flight together over 4 blocks); each
-    D equals TAPP_execute_product's bit for bit."""
+    submitted back to back (tickets in flight together over 4 blocks, and
+    over one block per SM); each D equals TAPP_execute_product's bit for
+    bit."""
+    import torch
+    if blocks == "sms":
+        blocks = torch.cuda.get_device_properties(0).multi_processor_count
     devs = [_Dev(tapp, c) for c in _small_cases()]
     want = _plain(tapp, devs)
-    err, loop = tapp.loop_create(0, blocks=4, slots=16, idle_ms=200.0)
+    err, loop = tapp.loop_create(0, blocks=blocks, slots=max(16, blocks), idle_ms=200.0)
     assert err == 0
     for d in devs:
         d.bufs[3].copy_(d.D0)
